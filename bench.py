@@ -1,0 +1,393 @@
+"""Benchmark of the plain FP32 DEM step at 4M disks on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one DEM time step (sort, reorder, collide + integrate) of the
+4,194,304-disk "plain at scale" scene: log-normal radii (median 1 mm,
+sigma 0.15, clipped [0.6, 1.6] mm), seeded random sequential placement to
+area fraction 0.55 in a 4.1 m x 6.11 m walled box, 1024 x 1024 grid, dt 2e-6.
+With N > 1 (torchrun, one rank per GPU) every rank steps its own replica
+(seed = rank): the plain step of one box has a halo exchange that is not
+built, so this is weak scaling by replicas.
+
+`value` is whole-job particle-steps/s over K timed steps (device time, CUDA
+events, max over ranks).  `e2e` is the same workload through the C ABI with
+host buffers: the state uploaded from pinned host memory, K steps each
+followed by the reference's per-step followed-particle readback
+(writeOutputFile), and the state downloaded, all inside the timed region.
+`roofline` is for the dominant kernel, timed by events captured in the
+step's CUDA graph during the timed region.  `cpu_baseline` times the
+reference's own step functions built for the host (oracle/_ref) on a
+bounded sample of the same workload.
+
+`--impl reference` times only that CPU reference on the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s at 4M disks"
+UNIT = "particle-steps/s"
+N_DEFAULT = 4194304
+# Algorithmic bytes per particle of the fused collide+integrate+hash kernel:
+# read pos 8, vel 8, theta 4, omega 4, radius 4, mass 4; write pos 8, vel 8,
+# theta 4, omega 4, next hash 4, pressure 4 (neighbours are cache hits); plus
+# 8 bytes per cell (cellStart/cellEnd).
+STEP_KERNEL_BYTES_PER_PARTICLE = 68
+STEP_KERNEL_BYTES_PER_CELL = 8
+# Per-stage algorithmic bytes for the other stages: sort = 4 + 16 * passes
+# per particle (+ the per-tile histograms), reorder = key+index 8, gather 36,
+# write 36, loc 4 per particle + 12 per cell.
+WHOLE_STEP_BYTES = lambda n, c: 260.0 * n + 20.0 * c  # whole-step model, per step
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.isfile(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index),
+                                          "--query-gpu=" + q, "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU reference
+def cpu_reference_rate(target_s: float, n_hint: int = 262144, seed: int = 0):
+    """Particle-steps/s of the reference's step functions built for the host
+    (oracle/_ref), or of the CPU restatement when that build is absent, on a
+    bounded sample of the plain-at-scale workload."""
+    from demso_b200 import scenes
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    sc = scenes.plain_at_scale(n_hint, seed=seed + 1000)
+    if O.ref_available():
+        h = O.RefHarness(threads=threads)
+        h.setup(sc.sys, sc.radius, sc.mass, None)
+        b = h.make_buffers(sc.state())
+        h.run(b, 1)
+        t0 = time.perf_counter()
+        h.run(b, 1)
+        t1 = time.perf_counter() - t0
+        steps = max(1, min(1000, int(target_s / max(t1, 1e-6))))
+        t0 = time.perf_counter()
+        h.run(b, steps)
+        dt = time.perf_counter() - t0
+        kind, cores = "reference", h.threads
+    else:
+        po = O.PortOracle("f32")
+        st = sc.state()
+        t0 = time.perf_counter()
+        po.run(sc.sys, st, 1)
+        t1 = time.perf_counter() - t0
+        steps = max(1, min(1000, int(target_s / max(t1, 1e-6))))
+        t0 = time.perf_counter()
+        po.run(sc.sys, st, steps)
+        dt = time.perf_counter() - t0
+        kind, cores = "port", 1
+    rate = sc.n * steps / dt
+    sample = ("%d steps of a %d-disk instance of the plain-at-scale workload (same radii, "
+              "density and parameters; %dx%d grid) on %d host threads"
+              % (steps, sc.n, sc.sys.gx, sc.sys.gy, cores))
+    return dict(value=rate, unit=UNIT, cores=cores, kind=kind, sample=sample), dt
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    # each of the K + W steps is a bounded sample sized so the run ends in minutes
+    per_step = max(0.02, 150.0 / max(1, args.steps + args.warmup))
+    from demso_b200 import scenes
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    sc = scenes.plain_at_scale(65536, seed=1000)
+    if O.ref_available():
+        h = O.RefHarness(threads=threads)
+        h.setup(sc.sys, sc.radius, sc.mass, None)
+        b = h.make_buffers(sc.state())
+        h.run(b, 2)
+        t0 = time.perf_counter()
+        h.run(b, 2)
+        rate = sc.n * 2 / (time.perf_counter() - t0)
+        n_s = int(min(N_DEFAULT, max(4096, rate * per_step)))
+        sc = scenes.plain_at_scale(n_s, seed=1000)
+        h.setup(sc.sys, sc.radius, sc.mass, None)
+        b = h.make_buffers(sc.state())
+        h.run(b, args.warmup)
+        t0 = time.perf_counter()
+        h.run(b, args.steps)
+        dt = time.perf_counter() - t0
+        kind, cores = "reference", h.threads
+    else:
+        po = O.PortOracle("f32")
+        n_s = 16384
+        sc = scenes.plain_at_scale(n_s, seed=1000)
+        st = po.run(sc.sys, sc.state(), args.warmup)
+        t0 = time.perf_counter()
+        po.run(sc.sys, st, args.steps)
+        dt = time.perf_counter() - t0
+        kind, cores = "port", 1
+    value = sc.n * args.steps / dt
+    sample = ("each step is one step of a %d-disk instance of the plain-at-scale workload "
+              "(same radii, density and parameters, %dx%d grid) on %d host threads"
+              % (sc.n, sc.sys.gx, sc.sys.gy, cores))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_dict(args.n, None),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def config_dict(n, sc):
+    d = {"workload": "plain at scale: %d disks, log-normal radii (median 1 mm, sigma 0.15, "
+                     "clipped [0.6, 1.6] mm), seeded random sequential placement to area "
+                     "fraction 0.55 in a walled box (4.1 m wide at 4M), zero initial velocity, "
+                     "kn 1e5 N/m, kt 0.5 kn, damping ratio 0.3, friction 0.5, dt 2e-6 s, "
+                     "grid cell >= 2 rmax" % n,
+         "n_particles": n, "precision": "fp32 state and contact law (pressure sum in fp64)",
+         "l2": "inputs larger than L2: the state read each step is >= 150 MB at 4M disks"}
+    if sc is not None:
+        d.update(grid=[sc.sys.gx, sc.sys.gy], box_m=[round(sc.sys.Lx, 4), round(sc.sys.Ly, 4)],
+                 parallelism="replicas" if int(os.environ.get("WORLD_SIZE", "1")) > 1
+                 else "single")
+    return d
+
+
+# ------------------------------------------------------------------ our arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=500)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import demso_b200 as D
+    from demso_b200 import scenes
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    sc = scenes.plain_at_scale(args.n, seed=rank)
+    n = sc.n
+    sim = D.Simulation(sc.sys, capacity=n, flags=D.CTX_PRESSURE)
+    pin = lambda a: torch.from_numpy(a.view(np.int32) if a.dtype == np.uint32 else a).pin_memory()
+    host = {k: pin(getattr(sc, k)) for k in ("pos", "vel", "theta", "omega", "radius", "mass",
+                                              "id")}
+    stream = torch.cuda.current_stream()
+    sim.set_state(host["pos"], host["vel"], host["theta"], host["omega"], host["radius"],
+                  host["mass"], host["id"])
+    sim.step(args.warmup)
+    torch.cuda.synchronize()
+    sim.check()
+    kernels_per_step = sim.kernels_per_step()
+
+    # ---- timed region (device-resident state)
+    clocks = Clocks(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    D.check(D.load().dem_profile_begin(sim.handle, args.steps))
+    ev0.record(stream)
+    sim.step(args.steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    import ctypes as C
+    ms = (C.c_float * D._lib.NUM_STAGES)()
+    nprof = C.c_uint32(0)
+    D.check(D.load().dem_profile_end(sim.handle, ms, C.byref(nprof)))
+    elapsed = ev0.elapsed_time(ev1)
+    barrier()
+    if dist is not None:
+        t = torch.tensor([elapsed], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    sim.check()
+    value = n * world * args.steps / (elapsed * 1e-3)
+
+    stage_ms = [ms[i] / max(1, nprof.value) for i in range(3)]
+    stage_names = ["sort", "reorder", "collide_integrate"]
+    dom = int(np.argmax(stage_ms))
+    hbm, kind = peaks()
+    cells = sc.sys.num_cells
+    if dom == 2:
+        bytes_launch = STEP_KERNEL_BYTES_PER_PARTICLE * n + STEP_KERNEL_BYTES_PER_CELL * cells
+        kname = "step_kernel (collide + integrate + next hash)"
+    elif dom == 1:
+        bytes_launch = 84 * n + 12 * cells
+        kname = "reorder_kernel (+ cell reset)"
+    else:
+        bytes_launch = 36 * n
+        kname = "radix sort (2 passes)"
+    achieved = bytes_launch / (stage_ms[dom] * 1e-3) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.txt")
+    if os.path.isfile(tf):
+        for ln in open(tf):
+            f = ln.split()
+            if len(f) >= 3 and f[0] == stage_names[dom] and f[1] == "bytes_per_particle":
+                traffic = float(f[2]) * n
+    whole_bytes = WHOLE_STEP_BYTES(n, cells)
+    step_ms = elapsed / args.steps
+
+    # ---- CPU baseline (rank 0, N = 1 only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu, _ = cpu_reference_rate(12.0)
+        except Exception as e:  # the baseline is reported, never the target
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "unavailable",
+                   "sample": "failed: %s" % e}
+
+    # ---- end to end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        sim2 = D.Simulation(sc.sys, capacity=n, flags=D.CTX_PRESSURE | D.CTX_ACCEL)
+        out_host = {k: torch.empty_like(v).pin_memory() for k, v in host.items()}
+        follow = np.array([n // 3, (2 * n) // 3], dtype=np.uint32)
+        rows = np.zeros(12 * follow.size, np.float32)
+        L = D.load()
+        sim2.set_state(host["pos"], host["vel"], host["theta"], host["omega"], host["radius"],
+                       host["mass"], host["id"])
+        sim2.step(3)  # build graphs outside the timed region
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        sim2.set_state(host["pos"], host["vel"], host["theta"], host["omega"], host["radius"],
+                       host["mass"], host["id"])
+        for _ in range(args.steps):
+            sim2.step(1)
+            D.check(L.dem_get_followed(sim2.handle, follow.ctypes.data, follow.size,
+                                       rows.ctypes.data, D._stream()))
+        p = lambda k: out_host[k].data_ptr()
+        D.check(L.dem_get_state(sim2.handle, p("pos"), p("vel"), p("theta"), p("omega"),
+                                p("radius"), p("mass"), p("id"), None, None, None, None, None, 1,
+                                D._stream()))
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        if dist is not None:
+            t = torch.tensor([e2e_s], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        state_bytes = sum(v.numel() * v.element_size() for v in host.values())
+        e2e = {"value": n * world * args.steps / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": state_bytes / args.steps,
+               "d2h_bytes_per_step": state_bytes / args.steps + rows.nbytes}
+        sim2.close()
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic", "config": config_dict(n, sc),
+                "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved,
+                             "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                             "peak_kind": kind, "traffic": traffic,
+                             "bytes_per_launch": bytes_launch},
+                "stage_ms_per_step": dict(zip(stage_names, stage_ms)),
+                "whole_step": {"model_bytes_per_step": whole_bytes,
+                               "achieved_gbs": whole_bytes / (step_ms * 1e-3) / 1e9,
+                               "frac": whole_bytes / (step_ms * 1e-3) / 1e9 / hbm},
+                "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+                "gpu_launches": kernels_per_step * args.steps,
+                "kernels_per_step": kernels_per_step}
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,264 @@
+"""demso_b200 -- B200-native DEM step of DemSo (blumberg/DemSo).
+
+Python binding of the native library (include/demso_b200.h).  The compute
+path is the CUDA library only; this module converts arguments, passes torch
+device pointers and the current torch stream through the C ABI, and raises
+``DemError`` on any non-zero status.
+
+Two levels mirror the reference's host layer (src/functions.cuh):
+
+* per-stage functions with the reference's names and argument order --
+  ``calcHash``, ``sortParticles``, ``reorderDataAndFindCellStart``,
+  ``collide``, ``integrateSystem`` -- writing into caller-owned tensors;
+* ``Simulation``, the whole step loop of ``SimLooping`` (main.cu:396-507)
+  on library-owned buffers (fused kernels, CUDA-graph replay).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+from . import _lib
+from ._lib import CTX_ACCEL, CTX_PRESSURE, DEM_MAX_MATERIALS, DemError, check, load
+
+__all__ = ["Material", "System", "DemError", "calcHash", "sortParticles",
+           "reorderDataAndFindCellStart", "collide", "integrateSystem", "Simulation",
+           "sort_scratch_bytes", "load", "CTX_PRESSURE", "CTX_ACCEL"]
+
+
+@dataclass
+class Material:
+    """Contact coefficients of one particle type (main.cuh:39-54)."""
+    normalStiffness: float
+    shearStiffness: float
+    normalDamping: float
+    boundaryDamping: float
+    frictionCoefficient: float
+    attractCoefficient: float = 0.0
+
+    def row(self):
+        return [self.normalStiffness, self.shearStiffness, self.normalDamping,
+                self.boundaryDamping, self.frictionCoefficient, self.attractCoefficient]
+
+
+@dataclass
+class System:
+    """Scene-wide parameters (SystemProperties, main.cuh:108-122) + materials."""
+    Lx: float
+    Ly: float
+    gx: int
+    gy: int
+    dt: float
+    gravity: Sequence[float] = (0.0, -9.81)
+    knWall: float = 0.0
+    ktWall: float = 0.0
+    materials: list = field(default_factory=list)
+
+    @property
+    def num_cells(self) -> int:
+        return self.gx * self.gy
+
+    @property
+    def key_bits(self) -> int:
+        return max(0, (self.num_cells - 1).bit_length())
+
+    def to_c(self, n: int = 0) -> "_lib.DemSystem":
+        s = _lib.DemSystem()
+        s.numParticles = n
+        s.cubeDimension[0], s.cubeDimension[1] = self.Lx, self.Ly
+        s.gridSize[0], s.gridSize[1] = self.gx, self.gy
+        s.timeStep = self.dt
+        s.gravity[0], s.gravity[1] = float(self.gravity[0]), float(self.gravity[1])
+        s.boundaryNormalStiffness = self.knWall
+        s.boundaryShearStiffness = self.ktWall
+        if not 1 <= len(self.materials) <= DEM_MAX_MATERIALS:
+            raise ValueError("need 1..%d materials" % DEM_MAX_MATERIALS)
+        s.numMaterials = len(self.materials)
+        for i, m in enumerate(self.materials):
+            (s.materials[i].normalStiffness, s.materials[i].shearStiffness,
+             s.materials[i].normalDamping, s.materials[i].boundaryDamping,
+             s.materials[i].frictionCoefficient, s.materials[i].attractCoefficient) = m.row()
+        return s
+
+
+def _ptr(t) -> Optional[int]:
+    """Device pointer of a torch CUDA tensor (None passes NULL)."""
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError("expected a contiguous tensor")
+    return t.data_ptr()
+
+
+def _stream(stream=None) -> Optional[int]:
+    import torch
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return stream.cuda_stream or None
+
+
+# ---------------------------------------------------------------------------
+# per-stage entry points (functions.cuh:50-72)
+# ---------------------------------------------------------------------------
+def calcHash(sys: System, pos, gridParticleIndex, gridParticleHash, numParticles: int,
+             stream=None) -> None:
+    """calcHash (functions.cu:315-327)."""
+    s = sys.to_c(numParticles)
+    check(load().dem_calc_hash(s, _ptr(pos), _ptr(gridParticleIndex), _ptr(gridParticleHash),
+                               numParticles, _stream(stream)))
+
+
+def sort_scratch_bytes(numParticles: int, keyBits: int) -> int:
+    return int(load().dem_sort_scratch_bytes(numParticles, keyBits))
+
+
+def sortParticles(gridParticleHash, gridParticleIndex, numParticles: int, keyBits: int = 32,
+                  scratch=None, stream=None) -> None:
+    """sortParticles (functions.cu:336-341): stable in-place sort by hash.
+
+    ``scratch`` is a uint8 CUDA tensor of ``sort_scratch_bytes`` bytes; one
+    is allocated when omitted."""
+    import torch
+    need = sort_scratch_bytes(numParticles, keyBits)
+    if scratch is None:
+        scratch = torch.empty(max(need, 1), dtype=torch.uint8, device=gridParticleHash.device)
+    check(load().dem_sort_particles(_ptr(gridParticleHash), _ptr(gridParticleIndex), numParticles,
+                                    keyBits, _ptr(scratch), scratch.numel(), _stream(stream)))
+
+
+def reorderDataAndFindCellStart(sys: System, cellStart, cellEnd, sortedPos, sortedVel,
+                                sortedTheta, sortedOmega, sortedRadius, sortedMass, sortedID,
+                                sortedLoc, sortedType, gridParticleHash, gridParticleIndex,
+                                oldPos, oldVel, oldTheta, oldOmega, oldRadius, oldMass, oldID,
+                                oldType, numParticles: int, numCells: int, stream=None) -> None:
+    """reorderDataAndFindCellStart (functions.cu:347-393) + radius/mass."""
+    s = sys.to_c(numParticles)
+    check(load().dem_reorder_data_and_find_cell_start(
+        s, _ptr(cellStart), _ptr(cellEnd), _ptr(sortedPos), _ptr(sortedVel), _ptr(sortedTheta),
+        _ptr(sortedOmega), _ptr(sortedRadius), _ptr(sortedMass), _ptr(sortedID), _ptr(sortedLoc),
+        _ptr(sortedType), _ptr(gridParticleHash), _ptr(gridParticleIndex), _ptr(oldPos),
+        _ptr(oldVel), _ptr(oldTheta), _ptr(oldOmega), _ptr(oldRadius), _ptr(oldMass),
+        _ptr(oldID), _ptr(oldType), numParticles, numCells, _stream(stream)))
+
+
+def collide(sys: System, oldPos, oldVel, newAcc, oldOmega, newAlpha, oldType, oldRadius, oldMass,
+            cellStart, cellEnd, numParticles: int, numCells: int, pressure=None,
+            stream=None) -> None:
+    """collide (functions.cu:398-467), without the control particle."""
+    s = sys.to_c(numParticles)
+    check(load().dem_collide(s, _ptr(oldPos), _ptr(oldVel), _ptr(newAcc), _ptr(oldOmega),
+                             _ptr(newAlpha), _ptr(oldType), _ptr(oldRadius), _ptr(oldMass),
+                             _ptr(cellStart), _ptr(cellEnd), numParticles, numCells,
+                             _ptr(pressure), _stream(stream)))
+
+
+def integrateSystem(sys: System, pos, vel, acc, theta, omega, alpha, type_, radius, mass,
+                    pressure, numParticles: int, stream=None) -> None:
+    """integrateSystem (functions.cu:529-551), in place."""
+    s = sys.to_c(numParticles)
+    check(load().dem_integrate_system(s, _ptr(pos), _ptr(vel), _ptr(acc), _ptr(theta),
+                                      _ptr(omega), _ptr(alpha), _ptr(type_), _ptr(radius),
+                                      _ptr(mass), _ptr(pressure), numParticles, _stream(stream)))
+
+
+# ---------------------------------------------------------------------------
+# context
+# ---------------------------------------------------------------------------
+class Simulation:
+    """Library-owned state and the fused, graph-captured step (dem_step)."""
+
+    def __init__(self, sys: System, capacity: int, flags: int = CTX_PRESSURE):
+        import ctypes as C
+        self.sys = sys
+        self.capacity = int(capacity)
+        self.flags = flags
+        self._h = C.c_void_p()
+        check(load().dem_create(sys.to_c(0), self.capacity, flags, C.byref(self._h)))
+        self.n = 0
+
+    def close(self) -> None:
+        if self._h:
+            load().dem_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_system(self, sys: System) -> None:
+        check(load().dem_set_system(self._h, sys.to_c(self.n)))
+        self.sys = sys
+
+    def set_state(self, pos, vel, theta, omega, radius, mass, ids, type_=None, stream=None):
+        """Tensors on the GPU (device copy) or on the CPU (host copy)."""
+        host = not pos.is_cuda
+        ptr = (lambda t: None if t is None else t.data_ptr())
+        n = pos.shape[0]
+        for t in (pos, vel, theta, omega, radius, mass, ids):
+            if not t.is_contiguous() or t.is_cuda == host:
+                raise ValueError("state tensors must be contiguous and on one device")
+        check(load().dem_set_state(self._h, n, ptr(pos), ptr(vel), ptr(theta), ptr(omega),
+                                   ptr(radius), ptr(mass), ptr(ids), ptr(type_), int(host),
+                                   _stream(stream)))
+        self.n = n
+
+    def get_state(self, device="cuda", stream=None) -> dict:
+        """Current state (cell-sorted order) as a dict of tensors."""
+        import torch
+        n = self.n
+        host = str(device) == "cpu"
+        kw = dict(device=device, pin_memory=host) if host else dict(device=device)
+        out = dict(pos=torch.empty((n, 2), dtype=torch.float32, **kw),
+                   vel=torch.empty((n, 2), dtype=torch.float32, **kw),
+                   theta=torch.empty(n, dtype=torch.float32, **kw),
+                   omega=torch.empty(n, dtype=torch.float32, **kw),
+                   radius=torch.empty(n, dtype=torch.float32, **kw),
+                   mass=torch.empty(n, dtype=torch.float32, **kw),
+                   id=torch.empty(n, dtype=torch.int32, **kw),
+                   loc=torch.empty(n, dtype=torch.int32, **kw),
+                   pressure=torch.empty(n, dtype=torch.float32, **kw),
+                   acc=torch.empty((n, 2), dtype=torch.float32, **kw),
+                   alpha=torch.empty(n, dtype=torch.float32, **kw))
+        typed = len(self.sys.materials) > 1
+        out["type"] = torch.empty(n, dtype=torch.int32, **kw) if typed else None
+        p = (lambda k: None if out[k] is None else out[k].data_ptr())
+        st = _stream(stream)
+        check(load().dem_get_state(self._h, p("pos"), p("vel"), p("theta"), p("omega"),
+                                   p("radius"), p("mass"), p("id"), p("type"), p("loc"),
+                                   p("pressure") if self.flags & CTX_PRESSURE else None,
+                                   p("acc") if self.flags & CTX_ACCEL else None,
+                                   p("alpha") if self.flags & CTX_ACCEL else None,
+                                   int(host), st))
+        if host:
+            torch.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
+        return out
+
+    def step(self, nsteps: int = 1, stream=None) -> None:
+        check(load().dem_step(self._h, int(nsteps), _stream(stream)))
+
+    def check(self, stream=None) -> None:
+        check(load().dem_check(self._h, _stream(stream)))
+
+    def kernels_per_step(self) -> int:
+        return int(load().dem_kernels_per_step(self._h))
+
+    def cells(self):
+        """(cellStart, cellEnd) device pointers of the last reorder."""
+        import ctypes as C
+        a, b = C.c_void_p(), C.c_void_p()
+        check(load().dem_get_cells(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value

@@ -1,0 +1,683 @@
+// C ABI of the DEM step (include/demso_b200.h): argument checking, the
+// per-stage entry points, and the context that runs the fused, graph-captured
+// step on library-owned buffers.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "dem_common.cuh"
+#include "dem_kernels.cuh"
+#include "dem_sort.cuh"
+
+using namespace dem;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    return fail(e == cudaErrorMemoryAllocation ? DEM_ERR_NO_MEMORY : DEM_ERR_CUDA, "%s: %s", what,
+                cudaGetErrorString(e));
+}
+
+#define DEM_TRY_CUDA(expr, what)                          \
+    do {                                                  \
+        cudaError_t _e = (expr);                          \
+        if (_e != cudaSuccess) return cuda_fail(_e, what); \
+    } while (0)
+
+inline bool is_pow2(uint32_t v) { return v != 0 && (v & (v - 1u)) == 0; }
+
+uint32_t log2_u32(uint32_t v) {
+    uint32_t b = 0;
+    while ((1ull << b) < (uint64_t)v) ++b;
+    return b;
+}
+
+int validate(const DemSystem* s) {
+    if (!s) return fail(DEM_ERR_INVALID_ARG, "system is NULL");
+    if (!is_pow2(s->gridSize[0]) || !is_pow2(s->gridSize[1]))
+        return fail(DEM_ERR_INVALID_ARG, "gridSize (%u, %u) must be powers of two",
+                    s->gridSize[0], s->gridSize[1]);
+    if ((uint64_t)s->gridSize[0] * s->gridSize[1] > (1ull << 31))
+        return fail(DEM_ERR_INVALID_ARG, "too many cells");
+    if (!(s->cubeDimension[0] > 0.0f) || !(s->cubeDimension[1] > 0.0f))
+        return fail(DEM_ERR_INVALID_ARG, "cubeDimension must be positive");
+    if (s->numMaterials < 1 || s->numMaterials > DEM_MAX_MATERIALS)
+        return fail(DEM_ERR_INVALID_ARG, "numMaterials %u outside 1..%d", s->numMaterials,
+                    DEM_MAX_MATERIALS);
+    return DEM_OK;
+}
+
+// Host-side evaluation of the per-pair coefficients, with the reference's
+// float expressions (particles_kernel.cuh:269-275, :417-421).
+KParams make_kparams(const DemSystem* s, uint32_t n) {
+    KParams P;
+    memset(&P, 0, sizeof(P));
+    P.n = n;
+    P.gx = s->gridSize[0];
+    P.gy = s->gridSize[1];
+    P.gxf = (float)s->gridSize[0];
+    P.gyf = (float)s->gridSize[1];
+    P.Lx = s->cubeDimension[0];
+    P.Ly = s->cubeDimension[1];
+    P.dt = s->timeStep;
+    P.gravx = s->gravity[0];
+    P.gravy = s->gravity[1];
+    P.ktWall = s->boundaryShearStiffness;
+    P.nmat = s->numMaterials;
+    for (uint32_t a = 0; a < P.nmat; ++a) {
+        const DemMaterial& A = s->materials[a];
+        P.cn[a] = A.normalDamping;
+        P.eb[a] = A.boundaryDamping;
+        P.mu[a] = A.frictionCoefficient;
+        P.at[a] = A.attractCoefficient;
+        P.ktw[a] = series_assoc(A.shearStiffness, s->boundaryShearStiffness);
+        for (uint32_t b = 0; b < P.nmat; ++b) {
+            const DemMaterial& B = s->materials[b];
+            P.pair[a * P.nmat + b] = make_float4(
+                series_assoc(A.normalStiffness, B.normalStiffness),
+                series_assoc(A.shearStiffness, B.shearStiffness),
+                series_assoc(A.normalDamping, B.normalDamping),
+                (A.frictionCoefficient + B.frictionCoefficient) / 2.0f);
+        }
+    }
+    return P;
+}
+
+template <typename T>
+bool misaligned(const T* p, size_t a) { return ((uintptr_t)p % a) != 0; }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// library
+// ---------------------------------------------------------------------------
+extern "C" int dem_abi_version(void) { return DEM_ABI_VERSION; }
+
+extern "C" const char* dem_last_error_string(void) { return g_last_error.c_str(); }
+
+extern "C" int dem_validate_system(const DemSystem* sys) { return validate(sys); }
+
+// ---------------------------------------------------------------------------
+// per-stage entry points
+// ---------------------------------------------------------------------------
+extern "C" int dem_calc_hash(const DemSystem* sys, const float* pos, uint32_t* gridParticleIndex,
+                             uint32_t* gridParticleHash, uint32_t numParticles, void* stream) {
+    int rc = validate(sys);
+    if (rc) return rc;
+    if (numParticles && (!pos || !gridParticleHash || !gridParticleIndex))
+        return fail(DEM_ERR_INVALID_ARG, "dem_calc_hash: NULL buffer");
+    if (misaligned(pos, 8)) return fail(DEM_ERR_INVALID_ARG, "pos must be 8-byte aligned");
+    const KParams P = make_kparams(sys, numParticles);
+    DEM_TRY_CUDA(launch_calc_hash(P, reinterpret_cast<const float2*>(pos), gridParticleHash,
+                                  gridParticleIndex, numParticles, (cudaStream_t)stream),
+                 "calc_hash launch");
+    return DEM_OK;
+}
+
+extern "C" size_t dem_sort_scratch_bytes(uint32_t numParticles, uint32_t keyBits) {
+    return sort_scratch_bytes(numParticles, keyBits);
+}
+
+extern "C" int dem_sort_particles(uint32_t* hash, uint32_t* index, uint32_t n, uint32_t keyBits,
+                                  void* scratch, size_t scratchBytes, void* stream) {
+    if (keyBits > 32) return fail(DEM_ERR_INVALID_ARG, "keyBits %u > 32", keyBits);
+    if (n == 0) return DEM_OK;
+    if (!hash || !index) return fail(DEM_ERR_INVALID_ARG, "dem_sort_particles: NULL buffer");
+    const size_t need = sort_scratch_bytes(n, keyBits);
+    if (!scratch || scratchBytes < need)
+        return fail(DEM_ERR_INVALID_ARG, "dem_sort_particles: scratch %zu bytes < %zu needed",
+                    scratchBytes, need);
+    if (misaligned((const char*)scratch, 256))
+        return fail(DEM_ERR_INVALID_ARG, "scratch must be 256-byte aligned");
+    const SortScratch s = carve_sort_scratch(scratch, n, keyBits);
+    cudaStream_t st = (cudaStream_t)stream;
+    uint32_t *ko, *vo;
+    DEM_TRY_CUDA(radix_sort_pairs(hash, index, n, keyBits, false, s, st, &ko, &vo, nullptr),
+                 "radix sort");
+    if (ko != hash) {
+        DEM_TRY_CUDA(cudaMemcpyAsync(hash, ko, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st),
+                     "sort copy-back");
+        DEM_TRY_CUDA(cudaMemcpyAsync(index, vo, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st),
+                     "sort copy-back");
+    }
+    return DEM_OK;
+}
+
+extern "C" int dem_reorder_data_and_find_cell_start(
+    const DemSystem* sys, uint32_t* cellStart, uint32_t* cellEnd, float* sortedPos,
+    float* sortedVel, float* sortedTheta, float* sortedOmega, float* sortedRadius,
+    float* sortedMass, uint32_t* sortedID, uint32_t* sortedLoc, uint32_t* sortedType,
+    const uint32_t* hash, const uint32_t* index, const float* oldPos, const float* oldVel,
+    const float* oldTheta, const float* oldOmega, const float* oldRadius, const float* oldMass,
+    const uint32_t* oldID, const uint32_t* oldType, uint32_t numParticles, uint32_t numCells,
+    void* stream) {
+    int rc = validate(sys);
+    if (rc) return rc;
+    if (numCells != sys->gridSize[0] * sys->gridSize[1])
+        return fail(DEM_ERR_INVALID_ARG, "numCells %u != gridSize product", numCells);
+    if (!cellStart || !cellEnd) return fail(DEM_ERR_INVALID_ARG, "NULL cell arrays");
+    if (numParticles &&
+        (!sortedPos || !sortedVel || !sortedTheta || !sortedOmega || !sortedRadius ||
+         !sortedMass || !sortedID || !sortedLoc || !hash || !index || !oldPos || !oldVel ||
+         !oldTheta || !oldOmega || !oldRadius || !oldMass || !oldID))
+        return fail(DEM_ERR_INVALID_ARG, "dem_reorder: NULL buffer");
+    if ((sortedType == nullptr) != (oldType == nullptr))
+        return fail(DEM_ERR_INVALID_ARG, "sortedType and oldType must both be set or both NULL");
+    if (misaligned(sortedPos, 8) || misaligned(sortedVel, 8) || misaligned(oldPos, 8) ||
+        misaligned(oldVel, 8))
+        return fail(DEM_ERR_INVALID_ARG, "float2 arrays must be 8-byte aligned");
+    const KParams P = make_kparams(sys, numParticles);
+    DynSet s{reinterpret_cast<float2*>(sortedPos), reinterpret_cast<float2*>(sortedVel),
+             sortedTheta, sortedOmega};
+    StatSet sS{sortedRadius, sortedMass, sortedID, sortedType};
+    DynSet o{const_cast<float2*>(reinterpret_cast<const float2*>(oldPos)),
+             const_cast<float2*>(reinterpret_cast<const float2*>(oldVel)),
+             const_cast<float*>(oldTheta), const_cast<float*>(oldOmega)};
+    StatSet oS{const_cast<float*>(oldRadius), const_cast<float*>(oldMass),
+               const_cast<uint32_t*>(oldID), const_cast<uint32_t*>(oldType)};
+    DEM_TRY_CUDA(launch_reorder(P, cellStart, cellEnd, s, sS, sortedLoc, hash, index, o, oS,
+                                numParticles, numCells, true, (cudaStream_t)stream, nullptr),
+                 "reorder launch");
+    return DEM_OK;
+}
+
+extern "C" int dem_collide(const DemSystem* sys, const float* pos, const float* vel, float* acc,
+                           const float* omega, float* alpha, const uint32_t* type,
+                           const float* radius, const float* mass, const uint32_t* cellStart,
+                           const uint32_t* cellEnd, uint32_t numParticles, uint32_t numCells,
+                           float* pressure, void* stream) {
+    int rc = validate(sys);
+    if (rc) return rc;
+    if (numCells != sys->gridSize[0] * sys->gridSize[1])
+        return fail(DEM_ERR_INVALID_ARG, "numCells %u != gridSize product", numCells);
+    if (numParticles &&
+        (!pos || !vel || !acc || !omega || !alpha || !radius || !mass || !cellStart || !cellEnd))
+        return fail(DEM_ERR_INVALID_ARG, "dem_collide: NULL buffer");
+    if (sys->numMaterials > 1 && !type)
+        return fail(DEM_ERR_INVALID_ARG, "type array required with more than one material");
+    if (misaligned(pos, 8) || misaligned(vel, 8) || misaligned(acc, 8))
+        return fail(DEM_ERR_INVALID_ARG, "float2 arrays must be 8-byte aligned");
+    const KParams P = make_kparams(sys, numParticles);
+    DEM_TRY_CUDA(launch_collide(P, reinterpret_cast<const float2*>(pos),
+                                reinterpret_cast<const float2*>(vel), omega, radius, mass, type,
+                                cellStart, cellEnd, reinterpret_cast<float2*>(acc), alpha,
+                                pressure, numParticles, (cudaStream_t)stream),
+                 "collide launch");
+    return DEM_OK;
+}
+
+extern "C" int dem_integrate_system(const DemSystem* sys, float* pos, float* vel,
+                                    const float* acc, float* theta, float* omega,
+                                    const float* alpha, const uint32_t* type, const float* radius,
+                                    const float* mass, float* pressure, uint32_t numParticles,
+                                    void* stream) {
+    int rc = validate(sys);
+    if (rc) return rc;
+    if (numParticles && (!pos || !vel || !acc || !theta || !omega || !alpha || !radius || !mass))
+        return fail(DEM_ERR_INVALID_ARG, "dem_integrate_system: NULL buffer");
+    if (sys->numMaterials > 1 && !type)
+        return fail(DEM_ERR_INVALID_ARG, "type array required with more than one material");
+    if (misaligned(pos, 8) || misaligned(vel, 8) || misaligned(acc, 8))
+        return fail(DEM_ERR_INVALID_ARG, "float2 arrays must be 8-byte aligned");
+    const KParams P = make_kparams(sys, numParticles);
+    DEM_TRY_CUDA(launch_integrate(P, reinterpret_cast<float2*>(pos), reinterpret_cast<float2*>(vel),
+                                  reinterpret_cast<const float2*>(acc), theta, omega, alpha, type,
+                                  radius, mass, pressure, numParticles, (cudaStream_t)stream),
+                 "integrate launch");
+    return DEM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+struct DemContext {
+    DemSystem sys;
+    KParams P;
+    uint32_t capacity = 0, n = 0, flags = 0, numCells = 0, keyBits = 0;
+    int device = 0;
+    bool typed = false;
+    // dynamic fields: dyn[0] holds the integrated state, dyn[1] the sorted copy
+    DynSet dyn[2];
+    // static fields ping-pong between the two sets on every reorder
+    StatSet stat[2];
+    int cur = 0;               // static set holding the current state
+    uint32_t* loc = nullptr;   // indexed by id
+    uint32_t* keys = nullptr;  // cell of each particle of the current state
+    uint32_t* perm = nullptr;  // sort values (source index of each sorted slot)
+    uint32_t *cellStart = nullptr, *cellEnd = nullptr;
+    float* pressure = nullptr;
+    float2* acc = nullptr;
+    float* alpha = nullptr;
+    uint32_t* errFlag = nullptr;
+    void* sortScratch = nullptr;
+    SortScratch ss;
+    bool keysValid = false;
+    cudaStream_t capStream = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int launchesPerStep = 0;
+    void* block = nullptr;  // one allocation for every per-particle/per-cell array
+    // followed-particle staging (device), see dem_get_followed
+    float* followRows = nullptr;
+    // stage profiling: graphs with event-record nodes at the stage boundaries
+    bool profiling = false;
+    cudaEvent_t marker[DEM_NUM_STAGES + 1] = {};
+    cudaGraphExec_t pgraph[2] = {nullptr, nullptr};
+    cudaGraphNode_t pnode[2][DEM_NUM_STAGES + 1] = {};
+    cudaEvent_t* evPool = nullptr;
+    uint32_t evCap = 0, evUsed = 0, stepsProfiled = 0;
+};
+
+namespace {
+
+void drop_graphs(DemContext* c) {
+    for (auto& g : c->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    for (auto& g : c->pgraph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+// One step from (dyn[0], stat[cur]) into (dyn[0], stat[cur^1]).  With
+// `markers`, an event is recorded before the sort, between the stages and
+// after the last kernel (captured as event-record nodes).
+cudaError_t enqueue_step(DemContext* c, cudaStream_t st, int* launches,
+                         const cudaEvent_t* markers) {
+    const int a = c->cur, b = c->cur ^ 1;
+    cudaError_t e;
+    if (markers && (e = cudaEventRecordWithFlags(markers[0], st, cudaEventRecordExternal)) != cudaSuccess)
+        return e;
+    uint32_t *ko, *vo;
+    e = radix_sort_pairs(c->keys, c->perm, c->n, c->keyBits, true, c->ss, st, &ko, &vo, launches);
+    if (e != cudaSuccess) return e;
+    if (markers && (e = cudaEventRecordWithFlags(markers[1], st, cudaEventRecordExternal)) != cudaSuccess)
+        return e;
+    e = launch_reorder(c->P, c->cellStart, c->cellEnd, c->dyn[1], c->stat[b], c->loc, ko, vo,
+                       c->dyn[0], c->stat[a], c->n, c->numCells, true, st, launches);
+    if (e != cudaSuccess) return e;
+    if (markers && (e = cudaEventRecordWithFlags(markers[2], st, cudaEventRecordExternal)) != cudaSuccess)
+        return e;
+    e = launch_step(c->P, c->dyn[1], c->stat[b], c->cellStart, c->cellEnd, c->dyn[0], c->keys,
+                    (c->flags & DEM_CTX_PRESSURE) ? c->pressure : nullptr,
+                    (c->flags & DEM_CTX_ACCEL) ? c->acc : nullptr,
+                    (c->flags & DEM_CTX_ACCEL) ? c->alpha : nullptr, c->errFlag, c->n, st);
+    if (launches) ++*launches;
+    if (e != cudaSuccess) return e;
+    if (markers && (e = cudaEventRecordWithFlags(markers[3], st, cudaEventRecordExternal)) != cudaSuccess)
+        return e;
+    return cudaSuccess;
+}
+
+int build_graph(DemContext* c, int parity, bool profiled) {
+    cudaGraph_t g = nullptr;
+    const int saved = c->cur;
+    c->cur = parity;
+    DEM_TRY_CUDA(cudaStreamBeginCapture(c->capStream, cudaStreamCaptureModeThreadLocal),
+                 "begin capture");
+    int launches = 0;
+    cudaError_t e = enqueue_step(c, c->capStream, &launches, profiled ? c->marker : nullptr);
+    cudaError_t e2 = cudaStreamEndCapture(c->capStream, &g);
+    c->cur = saved;
+    if (e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return cuda_fail(e, "step capture");
+    }
+    if (e2 != cudaSuccess) return cuda_fail(e2, "end capture");
+    if (profiled) {
+        // find the event-record nodes by the marker they record
+        size_t nn = 0;
+        cudaGraphGetNodes(g, nullptr, &nn);
+        cudaGraphNode_t* nodes = new cudaGraphNode_t[nn ? nn : 1];
+        cudaGraphGetNodes(g, nodes, &nn);
+        for (size_t i = 0; i < nn; ++i) {
+            cudaGraphNodeType t;
+            cudaGraphNodeGetType(nodes[i], &t);
+            if (t != cudaGraphNodeTypeEventRecord) continue;
+            cudaEvent_t ev;
+            cudaGraphEventRecordNodeGetEvent(nodes[i], &ev);
+            for (int k = 0; k <= DEM_NUM_STAGES; ++k)
+                if (ev == c->marker[k]) c->pnode[parity][k] = nodes[i];
+        }
+        delete[] nodes;
+    }
+    cudaGraphExec_t* slot = profiled ? &c->pgraph[parity] : &c->graph[parity];
+    e = cudaGraphInstantiate(slot, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "graph instantiate");
+    c->launchesPerStep = launches;
+    return DEM_OK;
+}
+
+void drop_profile(DemContext* c) {
+    for (auto& g : c->pgraph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    if (c->evPool) {
+        for (uint32_t i = 0; i < c->evCap; ++i) cudaEventDestroy(c->evPool[i]);
+        delete[] c->evPool;
+        c->evPool = nullptr;
+    }
+    for (auto& m : c->marker)
+        if (m) {
+            cudaEventDestroy(m);
+            m = nullptr;
+        }
+    c->evCap = c->evUsed = 0;
+    c->profiling = false;
+}
+
+size_t al256(size_t b) { return (b + 255u) & ~(size_t)255u; }
+
+}  // namespace
+
+extern "C" int dem_create(const DemSystem* sys, uint32_t capacity, uint32_t flags,
+                          DemContext** out) {
+    if (!out) return fail(DEM_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    int rc = validate(sys);
+    if (rc) return rc;
+    if (capacity == 0) return fail(DEM_ERR_INVALID_ARG, "capacity must be > 0");
+    DemContext* c = new (std::nothrow) DemContext();
+    if (!c) return fail(DEM_ERR_NO_MEMORY, "host allocation failed");
+    c->sys = *sys;
+    c->capacity = capacity;
+    c->flags = flags;
+    c->numCells = sys->gridSize[0] * sys->gridSize[1];
+    c->keyBits = log2_u32(c->numCells);
+    c->typed = sys->numMaterials > 1;
+    c->P = make_kparams(sys, 0);
+    cudaGetDevice(&c->device);
+
+    const size_t N = capacity, f4 = al256(4 * N), f8 = al256(8 * N), cells = al256(4 * (size_t)c->numCells);
+    size_t total = 0;
+    total += 2 * (2 * f8 + 2 * f4);             // dyn sets
+    total += 2 * (3 * f4 + (c->typed ? f4 : 0)); // static sets
+    total += 3 * f4;                            // loc, keys, perm
+    total += 2 * cells;                         // cellStart/End
+    total += f4 + f8 + f4;                      // pressure, acc, alpha
+    total += 256;                               // error flag
+    const size_t sortBytes = sort_scratch_bytes(capacity, c->keyBits);
+    cudaError_t e = cudaMalloc(&c->block, total);
+    if (e != cudaSuccess) {
+        delete c;
+        return cuda_fail(e, "cudaMalloc state");
+    }
+    e = cudaMalloc(&c->sortScratch, sortBytes);
+    if (e != cudaSuccess) {
+        cudaFree(c->block);
+        delete c;
+        return cuda_fail(e, "cudaMalloc sort scratch");
+    }
+    char* p = static_cast<char*>(c->block);
+    auto take = [&p](size_t b) { char* q = p; p += b; return q; };
+    for (int s = 0; s < 2; ++s) {
+        c->dyn[s].pos = reinterpret_cast<float2*>(take(f8));
+        c->dyn[s].vel = reinterpret_cast<float2*>(take(f8));
+        c->dyn[s].theta = reinterpret_cast<float*>(take(f4));
+        c->dyn[s].omega = reinterpret_cast<float*>(take(f4));
+        c->stat[s].radius = reinterpret_cast<float*>(take(f4));
+        c->stat[s].mass = reinterpret_cast<float*>(take(f4));
+        c->stat[s].id = reinterpret_cast<uint32_t*>(take(f4));
+        c->stat[s].type = c->typed ? reinterpret_cast<uint32_t*>(take(f4)) : nullptr;
+    }
+    c->loc = reinterpret_cast<uint32_t*>(take(f4));
+    c->keys = reinterpret_cast<uint32_t*>(take(f4));
+    c->perm = reinterpret_cast<uint32_t*>(take(f4));
+    c->cellStart = reinterpret_cast<uint32_t*>(take(cells));
+    c->cellEnd = reinterpret_cast<uint32_t*>(take(cells));
+    c->pressure = reinterpret_cast<float*>(take(f4));
+    c->acc = reinterpret_cast<float2*>(take(f8));
+    c->alpha = reinterpret_cast<float*>(take(f4));
+    c->errFlag = reinterpret_cast<uint32_t*>(take(256));
+    c->ss = carve_sort_scratch(c->sortScratch, capacity, c->keyBits);
+    e = cudaMemset(c->block, 0, total);
+    if (e == cudaSuccess) e = cudaMemset(c->cellStart, 0xff, 4 * (size_t)c->numCells);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->capStream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        cudaFree(c->sortScratch);
+        cudaFree(c->block);
+        delete c;
+        return cuda_fail(e, "context init");
+    }
+    *out = c;
+    return DEM_OK;
+}
+
+extern "C" int dem_destroy(DemContext* c) {
+    if (!c) return DEM_OK;
+    drop_graphs(c);
+    drop_profile(c);
+    if (c->capStream) cudaStreamDestroy(c->capStream);
+    cudaFree(c->followRows);
+    cudaFree(c->sortScratch);
+    cudaFree(c->block);
+    delete c;
+    return DEM_OK;
+}
+
+extern "C" int dem_set_system(DemContext* c, const DemSystem* sys) {
+    if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    int rc = validate(sys);
+    if (rc) return rc;
+    if (sys->gridSize[0] != c->sys.gridSize[0] || sys->gridSize[1] != c->sys.gridSize[1])
+        return fail(DEM_ERR_INVALID_ARG, "grid size is fixed at dem_create");
+    if ((sys->numMaterials > 1) != c->typed)
+        return fail(DEM_ERR_INVALID_ARG, "single/multi-material layout is fixed at dem_create");
+    c->sys = *sys;
+    c->P = make_kparams(sys, c->n);
+    drop_graphs(c);
+    // keys depend on the box size; recompute before the next step
+    c->keysValid = false;
+    return DEM_OK;
+}
+
+extern "C" int dem_set_state(DemContext* c, uint32_t n, const float* pos, const float* vel,
+                             const float* theta, const float* omega, const float* radius,
+                             const float* mass, const uint32_t* id, const uint32_t* type, int host,
+                             void* stream) {
+    if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    if (n > c->capacity) return fail(DEM_ERR_CAPACITY, "n %u > capacity %u", n, c->capacity);
+    if (n && (!pos || !vel || !theta || !omega || !radius || !mass || !id))
+        return fail(DEM_ERR_INVALID_ARG, "dem_set_state: NULL buffer");
+    if (c->typed && n && !type)
+        return fail(DEM_ERR_INVALID_ARG, "type array required with more than one material");
+    cudaStream_t st = (cudaStream_t)stream;
+    const cudaMemcpyKind k = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    const int a = c->cur;
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[0].pos, pos, 8ull * n, k, st), "set pos");
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[0].vel, vel, 8ull * n, k, st), "set vel");
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[0].theta, theta, 4ull * n, k, st), "set theta");
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[0].omega, omega, 4ull * n, k, st), "set omega");
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->stat[a].radius, radius, 4ull * n, k, st), "set radius");
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->stat[a].mass, mass, 4ull * n, k, st), "set mass");
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->stat[a].id, id, 4ull * n, k, st), "set id");
+    if (c->typed)
+        DEM_TRY_CUDA(cudaMemcpyAsync(c->stat[a].type, type, 4ull * n, k, st), "set type");
+    if (n != c->n) {
+        c->n = n;
+        c->P = make_kparams(&c->sys, n);
+        drop_graphs(c);
+    }
+    c->keysValid = false;
+    return DEM_OK;
+}
+
+extern "C" int dem_get_state(DemContext* c, float* pos, float* vel, float* theta, float* omega,
+                             float* radius, float* mass, uint32_t* id, uint32_t* type,
+                             uint32_t* loc, float* pressure, float* acc, float* alpha, int host,
+                             void* stream) {
+    if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    cudaStream_t st = (cudaStream_t)stream;
+    const cudaMemcpyKind k = host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    const uint32_t n = c->n;
+    const int a = c->cur;
+    if (pos) DEM_TRY_CUDA(cudaMemcpyAsync(pos, c->dyn[0].pos, 8ull * n, k, st), "get pos");
+    if (vel) DEM_TRY_CUDA(cudaMemcpyAsync(vel, c->dyn[0].vel, 8ull * n, k, st), "get vel");
+    if (theta) DEM_TRY_CUDA(cudaMemcpyAsync(theta, c->dyn[0].theta, 4ull * n, k, st), "get theta");
+    if (omega) DEM_TRY_CUDA(cudaMemcpyAsync(omega, c->dyn[0].omega, 4ull * n, k, st), "get omega");
+    if (radius) DEM_TRY_CUDA(cudaMemcpyAsync(radius, c->stat[a].radius, 4ull * n, k, st), "get radius");
+    if (mass) DEM_TRY_CUDA(cudaMemcpyAsync(mass, c->stat[a].mass, 4ull * n, k, st), "get mass");
+    if (id) DEM_TRY_CUDA(cudaMemcpyAsync(id, c->stat[a].id, 4ull * n, k, st), "get id");
+    if (type && c->typed)
+        DEM_TRY_CUDA(cudaMemcpyAsync(type, c->stat[a].type, 4ull * n, k, st), "get type");
+    if (loc) DEM_TRY_CUDA(cudaMemcpyAsync(loc, c->loc, 4ull * n, k, st), "get loc");
+    if (pressure) DEM_TRY_CUDA(cudaMemcpyAsync(pressure, c->pressure, 4ull * n, k, st), "get pressure");
+    if (acc) DEM_TRY_CUDA(cudaMemcpyAsync(acc, c->acc, 8ull * n, k, st), "get acc");
+    if (alpha) DEM_TRY_CUDA(cudaMemcpyAsync(alpha, c->alpha, 4ull * n, k, st), "get alpha");
+    return DEM_OK;
+}
+
+extern "C" int dem_step(DemContext* c, uint32_t nsteps, void* stream) {
+    if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    if (nsteps == 0 || c->n == 0) return DEM_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!c->keysValid) {
+        DEM_TRY_CUDA(launch_calc_hash(c->P, c->dyn[0].pos, c->keys, nullptr, c->n, st), "hash");
+        c->keysValid = true;
+    }
+    for (int p = 0; p < 2; ++p) {
+        if (!c->graph[p]) {
+            int rc = build_graph(c, p, false);
+            if (rc) return rc;
+        }
+        if (c->profiling && !c->pgraph[p]) {
+            int rc = build_graph(c, p, true);
+            if (rc) return rc;
+        }
+    }
+    for (uint32_t s = 0; s < nsteps; ++s) {
+        const int p = c->cur;
+        if (c->profiling && c->evUsed + DEM_NUM_STAGES + 1 <= c->evCap) {
+            for (int k = 0; k <= DEM_NUM_STAGES; ++k)
+                DEM_TRY_CUDA(cudaGraphExecEventRecordNodeSetEvent(c->pgraph[p], c->pnode[p][k],
+                                                                  c->evPool[c->evUsed + k]),
+                             "set profile event");
+            c->evUsed += DEM_NUM_STAGES + 1;
+            ++c->stepsProfiled;
+            DEM_TRY_CUDA(cudaGraphLaunch(c->pgraph[p], st), "graph launch");
+        } else {
+            DEM_TRY_CUDA(cudaGraphLaunch(c->graph[p], st), "graph launch");
+        }
+        c->cur ^= 1;
+    }
+    return DEM_OK;
+}
+
+extern "C" int dem_get_cells(DemContext* c, const uint32_t** cellStart, const uint32_t** cellEnd) {
+    if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    if (cellStart) *cellStart = c->cellStart;
+    if (cellEnd) *cellEnd = c->cellEnd;
+    return DEM_OK;
+}
+
+extern "C" int dem_check(DemContext* c, void* stream) {
+    if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    uint32_t flag = 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    DEM_TRY_CUDA(cudaMemcpyAsync(&flag, c->errFlag, 4, cudaMemcpyDeviceToHost, st), "read flag");
+    DEM_TRY_CUDA(cudaStreamSynchronize(st), "sync");
+    if (flag) return fail(DEM_ERR_OOB, "a particle position became NaN or infinite");
+    return DEM_OK;
+}
+
+extern "C" int dem_kernels_per_step(DemContext* c) {
+    if (!c) return -1;
+    if (!c->graph[0] && c->n > 0) {
+        if (build_graph(c, 0, false) != DEM_OK) return -1;
+    }
+    return c->launchesPerStep;
+}
+
+extern "C" int dem_get_followed(DemContext* c, const uint32_t* ids, uint32_t count, float* rows,
+                                void* stream) {
+    if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    if (count == 0) return DEM_OK;
+    if (!ids || !rows) return fail(DEM_ERR_INVALID_ARG, "dem_get_followed: NULL buffer");
+    for (uint32_t i = 0; i < count; ++i)
+        if (ids[i] >= c->n) return fail(DEM_ERR_INVALID_ARG, "followed id %u >= n %u", ids[i], c->n);
+    if (!c->followRows) {
+        DEM_TRY_CUDA(cudaMalloc(&c->followRows, sizeof(float) * 12 * kFollowBatch),
+                     "cudaMalloc followed rows");
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const int a = c->cur;
+    for (uint32_t base = 0; base < count; base += kFollowBatch) {
+        FollowIds f;
+        f.count = count - base < kFollowBatch ? count - base : kFollowBatch;
+        for (uint32_t i = 0; i < f.count; ++i) f.id[i] = ids[base + i];
+        DEM_TRY_CUDA(launch_followed(f, c->loc, c->dyn[0], c->stat[a],
+                                     (c->flags & DEM_CTX_ACCEL) ? c->acc : nullptr,
+                                     (c->flags & DEM_CTX_ACCEL) ? c->alpha : nullptr,
+                                     (c->flags & DEM_CTX_PRESSURE) ? c->pressure : nullptr,
+                                     c->followRows, st),
+                     "followed gather");
+        DEM_TRY_CUDA(cudaMemcpyAsync(rows + 12ull * base, c->followRows,
+                                     sizeof(float) * 12 * f.count, cudaMemcpyDeviceToHost, st),
+                     "followed copy");
+        DEM_TRY_CUDA(cudaStreamSynchronize(st), "followed sync");
+    }
+    return DEM_OK;
+}
+
+extern "C" int dem_profile_begin(DemContext* c, uint32_t maxSteps) {
+    if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    if (maxSteps == 0) return fail(DEM_ERR_INVALID_ARG, "maxSteps must be > 0");
+    drop_profile(c);
+    const uint32_t cap = maxSteps * (DEM_NUM_STAGES + 1);
+    c->evPool = new (std::nothrow) cudaEvent_t[cap];
+    if (!c->evPool) return fail(DEM_ERR_NO_MEMORY, "host allocation failed");
+    for (uint32_t i = 0; i < cap; ++i) {
+        cudaError_t e = cudaEventCreate(&c->evPool[i]);
+        if (e != cudaSuccess) {
+            c->evCap = i;
+            drop_profile(c);
+            return cuda_fail(e, "cudaEventCreate");
+        }
+    }
+    c->evCap = cap;
+    for (auto& m : c->marker) DEM_TRY_CUDA(cudaEventCreate(&m), "cudaEventCreate");
+    c->evUsed = 0;
+    c->stepsProfiled = 0;
+    c->profiling = true;
+    return DEM_OK;
+}
+
+extern "C" int dem_profile_end(DemContext* c, float* ms, uint32_t* steps) {
+    if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    if (!c->profiling) return fail(DEM_ERR_INVALID_ARG, "profiling was not started");
+    float acc[DEM_NUM_STAGES] = {0.0f, 0.0f, 0.0f};
+    if (c->evUsed) DEM_TRY_CUDA(cudaEventSynchronize(c->evPool[c->evUsed - 1]), "event sync");
+    for (uint32_t s = 0; s < c->stepsProfiled; ++s) {
+        cudaEvent_t* e = c->evPool + s * (DEM_NUM_STAGES + 1);
+        for (int k = 0; k < DEM_NUM_STAGES; ++k) {
+            float t = 0.0f;
+            DEM_TRY_CUDA(cudaEventElapsedTime(&t, e[k], e[k + 1]), "event elapsed");
+            acc[k] += t;
+        }
+    }
+    if (ms)
+        for (int k = 0; k < DEM_NUM_STAGES; ++k) ms[k] = acc[k];
+    if (steps) *steps = c->stepsProfiled;
+    drop_profile(c);
+    return DEM_OK;
+}

@@ -1,0 +1,62 @@
+// Kernel launchers for the DEM step (definitions in dem_kernels.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "dem_common.cuh"
+
+namespace dem {
+
+// Pointers of one state set in the reference SoA layout.
+struct DynSet {
+    float2* pos;
+    float2* vel;
+    float* theta;
+    float* omega;
+};
+struct StatSet {
+    float* radius;
+    float* mass;
+    uint32_t* id;
+    uint32_t* type;  // may be null (single material)
+};
+
+constexpr uint32_t kFollowBatch = 64;
+struct FollowIds {
+    uint32_t count;
+    uint32_t id[kFollowBatch];
+};
+cudaError_t launch_followed(const FollowIds& f, const uint32_t* loc, DynSet d, StatSet s,
+                            const float2* acc, const float* alpha, const float* pressure,
+                            float* rows, cudaStream_t st);
+
+cudaError_t launch_calc_hash(const KParams& P, const float2* pos, uint32_t* hash, uint32_t* index,
+                             uint32_t n, cudaStream_t st);
+
+cudaError_t launch_reorder(const KParams& P, uint32_t* cellStart, uint32_t* cellEnd,
+                           DynSet sorted, StatSet sortedS, uint32_t* sortedLoc,
+                           const uint32_t* hash, const uint32_t* index, DynSet old, StatSet oldS,
+                           uint32_t n, uint32_t numCells, bool clearCells, cudaStream_t st,
+                           int* launches);
+
+cudaError_t launch_collide(const KParams& P, const float2* pos, const float2* vel,
+                           const float* omega, const float* radius, const float* mass,
+                           const uint32_t* type, const uint32_t* cellStart,
+                           const uint32_t* cellEnd, float2* acc, float* alpha, float* pressure,
+                           uint32_t n, cudaStream_t st);
+
+cudaError_t launch_integrate(const KParams& P, float2* pos, float2* vel, const float2* acc,
+                             float* theta, float* omega, const float* alpha, const uint32_t* type,
+                             const float* radius, const float* mass, float* pressure, uint32_t n,
+                             cudaStream_t st);
+
+// Fused collide + integrate + next-step hash: reads the sorted set `in`,
+// writes the integrated state to `out` (same order) and the cell key of each
+// new position to `nextHash`.  acc/alpha/pressure may be null.
+cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t* cellStart,
+                        const uint32_t* cellEnd, DynSet out, uint32_t* nextHash, float* pressure,
+                        float2* acc, float* alpha, uint32_t* errFlag, uint32_t n,
+                        cudaStream_t st);
+
+}  // namespace dem

@@ -1,0 +1,229 @@
+/*
+ * demso_b200 -- C ABI of the B200-native DEM step.
+ *
+ * Drop-in for the per-timestep pipeline of DemSo (blumberg/DemSo): the host
+ * launch layer src/functions.cu / src/functions.cuh and the step loop of
+ * src/main.cu (SimLooping, main.cu:396-507).  Every entry point takes plain
+ * pointers and sizes, returns an int status (DEM_OK = 0) instead of the
+ * reference's silent `void`, never exits the process, and takes the CUDA
+ * stream to run on as `void*` (a cudaStream_t; NULL = legacy default stream,
+ * the reference's only stream).
+ *
+ * Data layout is the reference's SoA layout (functions.cu:68-99):
+ *   pos, vel, acc : float[2*n] (float2 per particle)
+ *   theta, omega, alpha, pressure : float[n]
+ *   id, loc, type : uint32[n]          (loc is indexed by id)
+ *   hash, index   : uint32[n]
+ *   cellStart, cellEnd : uint32[gridSize[0]*gridSize[1]]; empty cells have
+ *                        cellStart = 0xFFFFFFFF (cellEnd of an empty cell is
+ *                        left unspecified, as in the reference)
+ * plus two per-particle arrays the reference keeps per type:
+ *   radius, mass  : float[n]
+ * The reference stores radius/mass/inertia/coefficients per particle *type*
+ * in constant memory (main.cuh:39-54, particles_kernel.cuh:31-33, at most 10
+ * types).  Here radius and mass are per particle, inertia is 2/5 m r^2
+ * evaluated as main.cu:193 does, and the contact coefficients come from a
+ * material table of up to DEM_MAX_MATERIALS entries indexed by `type`
+ * (`type` may be NULL when there is one material).
+ *
+ * All device pointers must be device-accessible and 8-byte aligned for the
+ * float2 arrays.  Functions named *_host take host pointers.
+ */
+#ifndef DEMSO_B200_H
+#define DEMSO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DEM_ABI_VERSION 1
+
+#define DEM_OK 0
+#define DEM_ERR_INVALID_ARG 1 /* bad pointer, size, grid (not a power of two) */
+#define DEM_ERR_CUDA 2        /* a CUDA call failed; see dem_last_error_string */
+#define DEM_ERR_OOB 3         /* a particle position became NaN/Inf */
+#define DEM_ERR_TIMEOUT 4     /* a bounded device-side wait gave up */
+#define DEM_ERR_NO_MEMORY 5   /* device allocation failed */
+#define DEM_ERR_CAPACITY 6    /* more particles/cells than the context holds */
+
+#define DEM_MAX_MATERIALS 8
+
+/* Per-material contact coefficients: the reference's ParticleProperties
+ * (main.cuh:39-54) minus radius/mass/inertia/colour.  Pair values follow the
+ * reference: stiffness and damping combine in series, a*b/(a+b) (0 if either
+ * is 0; particles_kernel.cuh:36-41, :269-274), friction by the mean (:275). */
+typedef struct DemMaterial {
+    float normalStiffness;     /* <stiffness dir="normal"> */
+    float shearStiffness;      /* <stiffness dir="shear"> */
+    float normalDamping;       /* <damping>, a dashpot coefficient [N s/m] */
+    float boundaryDamping;     /* <damping type="boundary">: wall velocity factor */
+    float frictionCoefficient; /* <friction> */
+    float attractCoefficient;  /* <attraction>; 0 disables attractSpheres */
+} DemMaterial;
+
+/* Scene-wide parameters: the reference's SystemProperties (main.cuh:108-122)
+ * plus the material table. */
+typedef struct DemSystem {
+    uint32_t numParticles;
+    float cubeDimension[2];      /* box size Lx, Ly */
+    uint32_t gridSize[2];        /* cells per axis; powers of two (hash wraps with a mask) */
+    float timeStep;
+    float gravity[2];
+    float boundaryNormalStiffness; /* carried for completeness; the reference's
+                                      floor law does not use it (particles_kernel.cuh:423-427) */
+    float boundaryShearStiffness;
+    uint32_t numMaterials;       /* 1..DEM_MAX_MATERIALS */
+    DemMaterial materials[DEM_MAX_MATERIALS];
+} DemSystem;
+
+/* ---------------------------------------------------------------------------
+ * Library
+ * ------------------------------------------------------------------------- */
+int dem_abi_version(void);
+/* Text of the last error on the calling host thread ("" if none). */
+const char* dem_last_error_string(void);
+/* Validates a DemSystem (powers of two, material count, positive sizes). */
+int dem_validate_system(const DemSystem* sys);
+
+/* ---------------------------------------------------------------------------
+ * Per-stage entry points: one per host wrapper of the reference's step.
+ * Caller owns every buffer; outputs match the reference's per stage.
+ * ------------------------------------------------------------------------- */
+
+/* Replaces calcHash (functions.cu:315-327 -> calcHashD, particles_kernel.cuh:133-151):
+ * gridParticleHash[i] = cell of pos[i], gridParticleIndex[i] = i. */
+int dem_calc_hash(const DemSystem* sys, const float* pos, uint32_t* gridParticleIndex,
+                  uint32_t* gridParticleHash, uint32_t numParticles, void* stream);
+
+/* Scratch bytes dem_sort_particles needs for n pairs of `keyBits`-bit keys. */
+size_t dem_sort_scratch_bytes(uint32_t numParticles, uint32_t keyBits);
+
+/* Replaces sortParticles (functions.cu:336-341, thrust::sort_by_key): stable
+ * ascending sort of (hash, index) pairs in place.  Only the low `keyBits`
+ * bits of the keys are examined (keys must be < 2^keyBits; 32 = any key).
+ * `scratch` is device memory of dem_sort_scratch_bytes() bytes. */
+int dem_sort_particles(uint32_t* gridParticleHash, uint32_t* gridParticleIndex,
+                       uint32_t numParticles, uint32_t keyBits, void* scratch,
+                       size_t scratchBytes, void* stream);
+
+/* Replaces reorderDataAndFindCellStart (functions.cu:347-393 ->
+ * reorderDataAndFindCellStartD, particles_kernel.cuh:156-233): marks every
+ * cell empty, records [cellStart, cellEnd) of each occupied cell, gathers the
+ * state into sorted order and scatters sortedLoc[id] = sorted position.
+ * sortedType/oldType may be NULL (single material). */
+int dem_reorder_data_and_find_cell_start(
+    const DemSystem* sys, uint32_t* cellStart, uint32_t* cellEnd,
+    float* sortedPos, float* sortedVel, float* sortedTheta, float* sortedOmega,
+    float* sortedRadius, float* sortedMass, uint32_t* sortedID, uint32_t* sortedLoc,
+    uint32_t* sortedType, const uint32_t* gridParticleHash, const uint32_t* gridParticleIndex,
+    const float* oldPos, const float* oldVel, const float* oldTheta, const float* oldOmega,
+    const float* oldRadius, const float* oldMass, const uint32_t* oldID, const uint32_t* oldType,
+    uint32_t numParticles, uint32_t numCells, void* stream);
+
+/* Replaces collide (functions.cu:398-467 -> collideD, particles_kernel.cuh:459-549,
+ * without the control particle): gather-only 3x3-cell contact forces.
+ * newAcc = F/m, newAlpha = M/I, pressure = the reference's diagnostic
+ * (pressure may be NULL to skip it).  No atomics: results are deterministic. */
+int dem_collide(const DemSystem* sys, const float* sortedPos, const float* sortedVel,
+                float* newAcc, const float* sortedOmega, float* newAlpha,
+                const uint32_t* sortedType, const float* sortedRadius, const float* sortedMass,
+                const uint32_t* cellStart, const uint32_t* cellEnd, uint32_t numParticles,
+                uint32_t numCells, float* pressure, void* stream);
+
+/* Replaces integrateSystem (functions.cu:529-551 -> integrateSystemD,
+ * particles_kernel.cuh:580-627): symplectic Euler, theta wrap, wall clamps
+ * and floor contact, in place.  pressure may be NULL. */
+int dem_integrate_system(const DemSystem* sys, float* pos, float* vel, const float* acc,
+                         float* theta, float* omega, const float* alpha, const uint32_t* type,
+                         const float* radius, const float* mass, float* pressure,
+                         uint32_t numParticles, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Context API: the whole step (SimLooping's inner loop, main.cu:396-507)
+ * on library-owned device buffers, with the five stages fused into four
+ * kernels and graph-captured.
+ * ------------------------------------------------------------------------- */
+typedef struct DemContext DemContext;
+
+/* Flags for dem_create. */
+#define DEM_CTX_PRESSURE 1u   /* maintain the pressure diagnostic (as the reference does) */
+#define DEM_CTX_ACCEL 2u      /* also store acc/alpha of the last step (output rows) */
+
+int dem_create(const DemSystem* sys, uint32_t capacity, uint32_t flags, DemContext** out);
+int dem_destroy(DemContext* ctx);
+/* Runtime parameter change (gravity, dt, materials; grid size and particle
+ * count fixed): the reference's set_gravity (functions.cu:663-668) generalised. */
+int dem_set_system(DemContext* ctx, const DemSystem* sys);
+
+/* State transfer in the reference layout, any order of particles; ids must
+ * be a permutation of 0..n-1 (loc is indexed by id).  `host` != 0: the
+ * pointers are host memory (pinned or pageable), else device memory.
+ * type may be NULL. */
+int dem_set_state(DemContext* ctx, uint32_t n, const float* pos, const float* vel,
+                  const float* theta, const float* omega, const float* radius,
+                  const float* mass, const uint32_t* id, const uint32_t* type, int host,
+                  void* stream);
+/* Copies out the current state in its current (cell-sorted) order, plus loc
+ * (indexed by id) and, when requested at create time, pressure/acc/alpha of
+ * the last step.  NULL outputs are skipped. */
+int dem_get_state(DemContext* ctx, float* pos, float* vel, float* theta, float* omega,
+                  float* radius, float* mass, uint32_t* id, uint32_t* type, uint32_t* loc,
+                  float* pressure, float* acc, float* alpha, int host, void* stream);
+
+/* Advances `nsteps` full steps (hash, sort, reorder, collide, integrate). */
+int dem_step(DemContext* ctx, uint32_t nsteps, void* stream);
+
+/* Cell arrays of the last step's reorder (device pointers owned by ctx). */
+int dem_get_cells(DemContext* ctx, const uint32_t** cellStart, const uint32_t** cellEnd);
+
+/* Reads the device error flag (synchronises `stream`): DEM_OK or DEM_ERR_OOB. */
+int dem_check(DemContext* ctx, void* stream);
+
+/* Number of kernels one dem_step(ctx, 1, ...) launches (library kernels
+ * only; the cellStart memset is not counted). */
+int dem_kernels_per_step(DemContext* ctx);
+
+/* Followed-particle rows, the reference's per-step output (writeOutputFile,
+ * functions.cu:608-661): for each id in `ids` (host array), 12 words
+ *   id, type (uint32 bits), x, y, vx, vy, ax, ay, theta, omega, alpha, pressure
+ * are gathered on the device by loc[id] and copied to `rows` (host memory,
+ * 12*count words) with one transfer; acc/alpha/pressure need the matching
+ * DEM_CTX_* flags (zeros otherwise).  Synchronises `stream`. */
+int dem_get_followed(DemContext* ctx, const uint32_t* ids, uint32_t count, float* rows,
+                     void* stream);
+
+/* Stage timing inside dem_step (CUDA events recorded by the step's graph):
+ * after dem_profile_begin(ctx, maxSteps) the next dem_step calls (up to
+ * maxSteps steps in total) bracket each stage with events; dem_profile_end
+ * synchronises and returns the summed milliseconds per stage
+ *   ms[0] = sort (all passes), ms[1] = reorder (cell reset + gather),
+ *   ms[2] = collide + integrate + next hash
+ * and the number of steps profiled. */
+#define DEM_NUM_STAGES 3
+int dem_profile_begin(DemContext* ctx, uint32_t maxSteps);
+int dem_profile_end(DemContext* ctx, float* ms, uint32_t* steps);
+
+/* ---------------------------------------------------------------------------
+ * Scene generation (host only, no GPU needed)
+ * ------------------------------------------------------------------------- */
+
+/* Seeded random sequential placement of n non-overlapping disks of the given
+ * radii in [0,Lx]x[0,Ly] (host arrays; pos receives 2n floats in the order of
+ * `radius`).  Replaces the reference's wall-clock-seeded block generators
+ * (createRectanglesD, particles_kernel.cuh:43-74; seed time(NULL), main.cu:291)
+ * for scenes that must be reproducible.  Disks are placed largest first into
+ * `strips` horizontal strips filled in parallel; each disk gets up to
+ * `trials` uniform random trials, then a search over jittered lattice points
+ * of random cells.  The result depends only on the arguments.  Returns
+ * DEM_ERR_CAPACITY (with *placed < n, unplaced positions NaN) when the box
+ * is too full. */
+int dem_scene_rsa(uint32_t n, const float* radius, float Lx, float Ly, uint64_t seed,
+                  uint32_t strips, uint32_t trials, float* pos, uint32_t* placed);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DEMSO_B200_H */

@@ -1,0 +1,398 @@
+"""Test infrastructure (oracle only): ctypes wrappers for the CPU oracles.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline and
+reference arms import this module, and only as the checker or the timed CPU
+baseline.  The product path (the ``demso_b200`` package and its CUDA
+library) never imports or calls anything here.
+
+Two oracles are wrapped:
+
+* ``PortOracle`` -- ``dem_oracle.c``, our CPU restatement of the reference's
+  step (particles_kernel.cuh / functions.cu / main.cu), in float
+  (``libdem_oracle_f32.so``) or double (``libdem_oracle_f64.so``).
+* ``RefHarness`` -- ``_ref/libdemso_ref.so``, the reference's own
+  ``src/particles_kernel.cuh`` compiled for the host by oracle/Makefile (only
+  when the reference tree was present at build time).
+
+Both take arrays in the reference layout: ``pos``/``vel``/``acc`` are
+(n, 2) float arrays, everything else (n,).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(HERE, "_ref")
+MAX_MATERIALS = 8
+
+_u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+
+
+@dataclass
+class Material:
+    """Per-type contact coefficients (reference ParticleProperties, main.cuh:39-54)."""
+    normalStiffness: float
+    shearStiffness: float
+    normalDamping: float
+    boundaryDamping: float
+    frictionCoefficient: float
+    attractCoefficient: float = 0.0
+
+    def row(self):
+        return [self.normalStiffness, self.shearStiffness, self.normalDamping,
+                self.boundaryDamping, self.frictionCoefficient, self.attractCoefficient]
+
+
+@dataclass
+class System:
+    """Scene-wide parameters (reference SystemProperties, main.cuh:108-122)."""
+    Lx: float
+    Ly: float
+    gx: int
+    gy: int
+    dt: float
+    gravity: Sequence[float] = (0.0, -9.81)
+    knWall: float = 0.0
+    ktWall: float = 0.0
+    materials: list = field(default_factory=list)
+
+    @property
+    def num_cells(self) -> int:
+        return self.gx * self.gy
+
+
+class _OrcSystem(C.Structure):
+    _fields_ = [("Lx", C.c_double), ("Ly", C.c_double), ("gx", C.c_uint32), ("gy", C.c_uint32),
+                ("dt", C.c_double), ("gravx", C.c_double), ("gravy", C.c_double),
+                ("knWall", C.c_double), ("ktWall", C.c_double), ("nmat", C.c_uint32),
+                ("reserved", C.c_uint32), ("mat", (C.c_double * 6) * MAX_MATERIALS)]
+
+
+def _orc_system(s: System) -> _OrcSystem:
+    o = _OrcSystem()
+    o.Lx, o.Ly, o.gx, o.gy, o.dt = s.Lx, s.Ly, s.gx, s.gy, s.dt
+    o.gravx, o.gravy = float(s.gravity[0]), float(s.gravity[1])
+    o.knWall, o.ktWall = s.knWall, s.ktWall
+    if not 1 <= len(s.materials) <= MAX_MATERIALS:
+        raise ValueError("need 1..%d materials" % MAX_MATERIALS)
+    o.nmat = len(s.materials)
+    for m, mat in enumerate(s.materials):
+        for k, v in enumerate(mat.row()):
+            o.mat[m][k] = v
+    return o
+
+
+def build(ref_root: Optional[str] = None, quiet: bool = True) -> None:
+    """Compile the oracles (and the reference host build when its tree exists)."""
+    targets = ["all"]
+    root = ref_root or "/root/reference"
+    if os.path.isfile(os.path.join(root, "src", "particles_kernel.cuh")):
+        targets.append("ref")
+    subprocess.run(["make", "-C", HERE, "REF_ROOT=" + root] + targets, check=True,
+                   stdout=subprocess.DEVNULL if quiet else None)
+
+
+def ref_available() -> bool:
+    return os.path.isfile(os.path.join(OUT, "libdemso_ref.so"))
+
+
+# ---------------------------------------------------------------------------
+# CPU restatement
+# ---------------------------------------------------------------------------
+class PortOracle:
+    """The C restatement (dem_oracle.c) at float or double precision."""
+
+    def __init__(self, precision: str = "f32"):
+        if precision not in ("f32", "f64"):
+            raise ValueError(precision)
+        path = os.path.join(OUT, "libdem_oracle_%s.so" % precision)
+        if not os.path.isfile(path):
+            build()
+        self.lib = C.CDLL(path)
+        self.dt = np.float32 if precision == "f32" else np.float64
+        rp = _f32p if precision == "f32" else _f64p
+        L = self.lib
+        sp = C.POINTER(_OrcSystem)
+        u32 = C.c_uint32
+        L.orc_calc_hash.argtypes = [sp, u32, rp, _u32p, _u32p]
+        L.orc_sort.argtypes = [u32, _u32p, _u32p]
+        L.orc_reorder.argtypes = [sp, u32, _u32p, _u32p] + [rp] * 6 + [_u32p, _u32p, C.c_void_p] + \
+            [_u32p, _u32p] + [rp] * 6 + [_u32p, C.c_void_p]
+        L.orc_collide.argtypes = [sp, u32, rp, rp, rp, rp, rp, C.c_void_p, _u32p, _u32p,
+                                  rp, rp, _f32p]
+        L.orc_integrate.argtypes = [sp, u32, rp, rp, rp, rp, rp, rp, rp, rp, C.c_void_p, _f32p]
+        L.orc_step.argtypes = [sp, u32] + [rp] * 6 + [_u32p, C.c_void_p] + [rp] * 6 + \
+            [_u32p, _u32p, C.c_void_p] + [rp, rp, _f32p, _u32p, _u32p, _u32p, _u32p]
+
+    def _r(self, a, shape=None):
+        a = np.ascontiguousarray(a, dtype=self.dt)
+        return a if shape is None else a.reshape(shape)
+
+    @staticmethod
+    def _tp(t):
+        if t is None:
+            return None
+        t = np.ascontiguousarray(t, dtype=np.uint32)
+        return t
+
+    def calc_hash(self, sys: System, pos):
+        pos = self._r(pos)
+        n = pos.shape[0]
+        h = np.empty(n, np.uint32)
+        ix = np.empty(n, np.uint32)
+        self.lib.orc_calc_hash(C.byref(_orc_system(sys)), n, pos.reshape(-1), h, ix)
+        return h, ix
+
+    def sort(self, hash_, index):
+        h = np.ascontiguousarray(hash_, dtype=np.uint32).copy()
+        ix = np.ascontiguousarray(index, dtype=np.uint32).copy()
+        self.lib.orc_sort(h.shape[0], h, ix)
+        return h, ix
+
+    def reorder(self, sys: System, hash_, index, st: dict, cell_end_init=None):
+        n = len(hash_)
+        cs = np.empty(sys.num_cells, np.uint32)
+        ce = (np.zeros(sys.num_cells, np.uint32) if cell_end_init is None
+              else np.array(cell_end_init, dtype=np.uint32))
+        out = {k: np.empty_like(self._r(st[k])) for k in ("pos", "vel", "theta", "omega",
+                                                          "radius", "mass")}
+        out["id"] = np.empty(n, np.uint32)
+        out["loc"] = np.zeros(n, np.uint32)
+        typ = self._tp(st.get("type"))
+        out["type"] = np.empty(n, np.uint32) if typ is not None else None
+        src = {k: self._r(st[k]) for k in ("pos", "vel", "theta", "omega", "radius", "mass")}
+        self.lib.orc_reorder(
+            C.byref(_orc_system(sys)), n, cs, ce,
+            out["pos"].reshape(-1), out["vel"].reshape(-1), out["theta"], out["omega"],
+            out["radius"], out["mass"], out["id"], out["loc"],
+            out["type"].ctypes.data if typ is not None else None,
+            np.ascontiguousarray(hash_, dtype=np.uint32), np.ascontiguousarray(index, dtype=np.uint32),
+            src["pos"].reshape(-1), src["vel"].reshape(-1), src["theta"], src["omega"],
+            src["radius"], src["mass"], np.ascontiguousarray(st["id"], dtype=np.uint32),
+            typ.ctypes.data if typ is not None else None)
+        if typ is None:
+            out["type"] = None
+        return cs, ce, out
+
+    def collide(self, sys: System, st: dict, cell_start, cell_end):
+        pos = self._r(st["pos"])
+        n = pos.shape[0]
+        acc = np.empty((n, 2), self.dt)
+        alpha = np.empty(n, self.dt)
+        pr = np.empty(n, np.float32)
+        typ = self._tp(st.get("type"))
+        self.lib.orc_collide(C.byref(_orc_system(sys)), n, pos.reshape(-1),
+                             self._r(st["vel"]).reshape(-1), self._r(st["omega"]),
+                             self._r(st["radius"]), self._r(st["mass"]),
+                             typ.ctypes.data if typ is not None else None,
+                             np.ascontiguousarray(cell_start, dtype=np.uint32),
+                             np.ascontiguousarray(cell_end, dtype=np.uint32),
+                             acc.reshape(-1), alpha, pr)
+        return acc, alpha, pr
+
+    def integrate(self, sys: System, st: dict, acc, alpha, pressure):
+        """Returns new (pos, vel, theta, omega, pressure); inputs are not modified."""
+        pos = self._r(st["pos"]).copy()
+        vel = self._r(st["vel"]).copy()
+        th = self._r(st["theta"]).copy()
+        om = self._r(st["omega"]).copy()
+        pr = np.array(pressure, dtype=np.float32)
+        typ = self._tp(st.get("type"))
+        n = pos.shape[0]
+        self.lib.orc_integrate(C.byref(_orc_system(sys)), n, pos.reshape(-1), vel.reshape(-1),
+                               self._r(acc).reshape(-1), th, om, self._r(alpha),
+                               self._r(st["radius"]), self._r(st["mass"]),
+                               typ.ctypes.data if typ is not None else None, pr)
+        return pos, vel, th, om, pr
+
+    def run(self, sys: System, st: dict, nsteps: int):
+        """`nsteps` full steps; returns the final sorted state dict plus
+        acc/alpha/pressure/cellStart/cellEnd/hash/index of the last step."""
+        a = {k: self._r(st[k]).copy() for k in ("pos", "vel", "theta", "omega", "radius", "mass")}
+        n = a["pos"].shape[0]
+        a["id"] = np.ascontiguousarray(st["id"], dtype=np.uint32).copy()
+        typ = self._tp(st.get("type"))
+        a["type"] = typ.copy() if typ is not None else None
+        b = {k: np.empty_like(v) for k, v in a.items() if v is not None}
+        b["type"] = np.empty(n, np.uint32) if typ is not None else None
+        b["loc"] = np.zeros(n, np.uint32)
+        a["loc"] = np.zeros(n, np.uint32)
+        acc = np.zeros((n, 2), self.dt)
+        alpha = np.zeros(n, self.dt)
+        pr = np.zeros(n, np.float32)
+        h = np.zeros(n, np.uint32)
+        ix = np.zeros(n, np.uint32)
+        cs = np.zeros(sys.num_cells, np.uint32)
+        ce = np.zeros(sys.num_cells, np.uint32)
+        osys = _orc_system(sys)
+        for _ in range(nsteps):
+            self.lib.orc_step(
+                C.byref(osys), n, a["pos"].reshape(-1), a["vel"].reshape(-1), a["theta"],
+                a["omega"], a["radius"], a["mass"], a["id"],
+                a["type"].ctypes.data if a["type"] is not None else None,
+                b["pos"].reshape(-1), b["vel"].reshape(-1), b["theta"], b["omega"], b["radius"],
+                b["mass"], b["id"], b["loc"],
+                b["type"].ctypes.data if b["type"] is not None else None,
+                acc.reshape(-1), alpha, pr, h, ix, cs, ce)
+            a, b = b, a
+        out = dict(a)
+        out.update(acc=acc, alpha=alpha, pressure=pr, cellStart=cs, cellEnd=ce, hash=h, index=ix)
+        return out
+
+
+# ---------------------------------------------------------------------------
+# Reference host build
+# ---------------------------------------------------------------------------
+class RefHarness:
+    """The reference's own kernels (src/particles_kernel.cuh) run on host cores.
+
+    Particle i is given its own reference "type" i carrying radius[i],
+    mass[i] and the coefficients of material[i]; the reference's ``type``
+    arrays therefore hold particle ids.  Global state lives in the library
+    (the reference's constant-memory symbols), so one harness per process.
+    """
+
+    def __init__(self, threads: Optional[int] = None):
+        path = os.path.join(OUT, "libdemso_ref.so")
+        if not os.path.isfile(path):
+            raise FileNotFoundError("reference host build missing: " + path)
+        self.lib = C.CDLL(path)
+        L = self.lib
+        u32 = C.c_uint32
+        f = C.c_float
+        L.ref_setup.argtypes = [u32, f, f, u32, u32, f, f, f, f, f, _f32p, _f32p, C.c_void_p,
+                                _f32p, u32]
+        L.ref_setup.restype = C.c_int
+        L.ref_set_threads.argtypes = [C.c_int]
+        L.ref_set_threads.restype = C.c_int
+        L.ref_calc_hash.argtypes = [_f32p, _u32p, _u32p]
+        L.ref_sort.argtypes = [_u32p, _u32p]
+        L.ref_reorder.argtypes = [_u32p, _u32p, _f32p, _f32p, _f32p, _f32p, _u32p, _u32p, _u32p,
+                                  _u32p, _u32p, _f32p, _f32p, _f32p, _f32p, _u32p, _u32p]
+        L.ref_collide.argtypes = [_f32p, _f32p, _f32p, _f32p, _f32p, _u32p, _u32p, _u32p, _f32p]
+        L.ref_integrate.argtypes = [_f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _u32p, _f32p]
+        L.ref_run.argtypes = [u32] + [_f32p] * 4 + [_u32p] * 3 + [_f32p] * 4 + [_u32p] * 3 + \
+            [_f32p, _f32p, _f32p, _u32p, _u32p, _u32p, _u32p]
+        L.ref_max_particles.restype = C.c_int
+        self.threads = L.ref_set_threads(int(threads or 0))
+        self.sys = None
+        self.n = 0
+
+    def setup(self, sys: System, radius, mass, material=None):
+        radius = np.ascontiguousarray(radius, dtype=np.float32)
+        mass = np.ascontiguousarray(mass, dtype=np.float32)
+        n = radius.shape[0]
+        tab = np.zeros((MAX_MATERIALS, 6), np.float32)
+        for m, mat in enumerate(sys.materials):
+            tab[m] = mat.row()
+        mt = None if material is None else np.ascontiguousarray(material, dtype=np.uint32)
+        rc = self.lib.ref_setup(n, sys.Lx, sys.Ly, sys.gx, sys.gy, sys.dt, float(sys.gravity[0]),
+                                float(sys.gravity[1]), sys.knWall, sys.ktWall, radius, mass,
+                                mt.ctypes.data if mt is not None else None, tab.reshape(-1),
+                                len(sys.materials))
+        if rc != 0:
+            raise ValueError("ref_setup failed: %d" % rc)
+        self.sys, self.n = sys, n
+
+    def calc_hash(self, pos):
+        pos = np.ascontiguousarray(pos, dtype=np.float32)
+        h = np.empty(self.n, np.uint32)
+        ix = np.empty(self.n, np.uint32)
+        self.lib.ref_calc_hash(pos.reshape(-1), h, ix)
+        return h, ix
+
+    def sort(self, hash_, index):
+        h = np.array(hash_, dtype=np.uint32)
+        ix = np.array(index, dtype=np.uint32)
+        self.lib.ref_sort(h, ix)
+        return h, ix
+
+    def reorder(self, hash_, index, pos, vel, theta, omega, ids, cell_end_init=None):
+        n = self.n
+        cs = np.empty(self.sys.num_cells, np.uint32)
+        ce = (np.zeros(self.sys.num_cells, np.uint32) if cell_end_init is None
+              else np.array(cell_end_init, dtype=np.uint32))
+        sp = np.empty((n, 2), np.float32)
+        sv = np.empty((n, 2), np.float32)
+        sth = np.empty(n, np.float32)
+        som = np.empty(n, np.float32)
+        sid = np.empty(n, np.uint32)
+        sloc = np.zeros(n, np.uint32)
+        styp = np.empty(n, np.uint32)
+        ids = np.ascontiguousarray(ids, dtype=np.uint32)
+        self.lib.ref_reorder(cs, ce, sp.reshape(-1), sv.reshape(-1), sth, som, sid, sloc, styp,
+                             np.ascontiguousarray(hash_, dtype=np.uint32),
+                             np.ascontiguousarray(index, dtype=np.uint32),
+                             np.ascontiguousarray(pos, dtype=np.float32).reshape(-1),
+                             np.ascontiguousarray(vel, dtype=np.float32).reshape(-1),
+                             np.ascontiguousarray(theta, dtype=np.float32),
+                             np.ascontiguousarray(omega, dtype=np.float32), ids, ids.copy())
+        return cs, ce, dict(pos=sp, vel=sv, theta=sth, omega=som, id=sid, loc=sloc, type=styp)
+
+    def collide(self, pos, vel, omega, ids, cell_start, cell_end):
+        n = self.n
+        acc = np.empty((n, 2), np.float32)
+        alpha = np.empty(n, np.float32)
+        pr = np.empty(n, np.float32)
+        self.lib.ref_collide(np.ascontiguousarray(pos, dtype=np.float32).reshape(-1),
+                             np.ascontiguousarray(vel, dtype=np.float32).reshape(-1),
+                             acc.reshape(-1), np.ascontiguousarray(omega, dtype=np.float32), alpha,
+                             np.ascontiguousarray(ids, dtype=np.uint32),
+                             np.ascontiguousarray(cell_start, dtype=np.uint32),
+                             np.ascontiguousarray(cell_end, dtype=np.uint32), pr)
+        return acc, alpha, pr
+
+    def integrate(self, pos, vel, acc, theta, omega, alpha, ids, pressure):
+        pos = np.array(pos, dtype=np.float32)
+        vel = np.array(vel, dtype=np.float32)
+        th = np.array(theta, dtype=np.float32)
+        om = np.array(omega, dtype=np.float32)
+        pr = np.array(pressure, dtype=np.float32)
+        self.lib.ref_integrate(pos.reshape(-1), vel.reshape(-1),
+                               np.ascontiguousarray(acc, dtype=np.float32).reshape(-1), th, om,
+                               np.ascontiguousarray(alpha, dtype=np.float32),
+                               np.ascontiguousarray(ids, dtype=np.uint32), pr)
+        return pos, vel, th, om, pr
+
+    def make_buffers(self, st: dict):
+        """Allocate the two state sets and scratch for ``run`` (kept out of timing)."""
+        n = self.n
+        b = {}
+        b["pos1"] = np.ascontiguousarray(st["pos"], dtype=np.float32).copy()
+        b["vel1"] = np.ascontiguousarray(st["vel"], dtype=np.float32).copy()
+        b["theta1"] = np.ascontiguousarray(st["theta"], dtype=np.float32).copy()
+        b["omega1"] = np.ascontiguousarray(st["omega"], dtype=np.float32).copy()
+        b["id1"] = np.ascontiguousarray(st["id"], dtype=np.uint32).copy()
+        b["type1"] = b["id1"].copy()
+        b["loc1"] = np.zeros(n, np.uint32)
+        for k in ("pos", "vel"):
+            b[k + "2"] = np.zeros((n, 2), np.float32)
+        for k in ("theta", "omega"):
+            b[k + "2"] = np.zeros(n, np.float32)
+        for k in ("id", "type", "loc"):
+            b[k + "2"] = np.zeros(n, np.uint32)
+        b["acc"] = np.zeros((n, 2), np.float32)
+        b["alpha"] = np.zeros(n, np.float32)
+        b["pressure"] = np.zeros(n, np.float32)
+        b["hash"] = np.zeros(n, np.uint32)
+        b["index"] = np.zeros(n, np.uint32)
+        b["cellStart"] = np.zeros(self.sys.num_cells, np.uint32)
+        b["cellEnd"] = np.zeros(self.sys.num_cells, np.uint32)
+        return b
+
+    def run(self, b: dict, nsteps: int):
+        """`nsteps` full reference steps in place on buffers from ``make_buffers``."""
+        self.lib.ref_run(nsteps, b["pos1"].reshape(-1), b["vel1"].reshape(-1), b["theta1"],
+                         b["omega1"], b["id1"], b["type1"], b["loc1"], b["pos2"].reshape(-1),
+                         b["vel2"].reshape(-1), b["theta2"], b["omega2"], b["id2"], b["type2"],
+                         b["loc2"], b["acc"].reshape(-1), b["alpha"], b["pressure"], b["hash"],
+                         b["index"], b["cellStart"], b["cellEnd"])
+        return b

@@ -1,0 +1,105 @@
+"""The C-ABI library builds for sm_100a, loads without a GPU, exports every
+entry point its header declares, and rejects bad arguments with status codes
+(host-side checks only; no kernel is launched here)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+import demso_b200 as D
+from demso_b200 import _lib, scenes
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADERS = [os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include"))
+           if f.endswith(".h")]
+
+
+def declared_functions():
+    names = set()
+    for h in HEADERS:
+        txt = open(h).read()
+        txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+        for m in re.finditer(r"\b(dem_[a-z0-9_]+)\s*\(", txt):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    lib = _lib.load()
+    names = declared_functions()
+    assert len(names) >= 15
+    for n in names:
+        assert hasattr(lib, n), n
+
+
+def test_binding_covers_header():
+    bound = {s[0] for s in _lib.SIGNATURES}
+    assert set(declared_functions()) <= bound
+
+
+def test_abi_version_and_struct_sizes():
+    lib = _lib.load()
+    assert lib.dem_abi_version() == 1
+    # DemSystem: 4 + 8 + 8 + 4 + 8 + 4 + 4 + 4 + 8 * 24 bytes
+    assert C.sizeof(_lib.DemSystem) == 44 + 8 * 24
+    assert C.sizeof(_lib.DemMaterial) == 24
+
+
+def _sys(**kw):
+    s = scenes.settling_pile(side=8, box=0.02).sys
+    for k, v in kw.items():
+        setattr(s, k, v)
+    return s
+
+
+def test_validate_system():
+    lib = _lib.load()
+    assert lib.dem_validate_system(_sys().to_c()) == 0
+    assert lib.dem_validate_system(_sys(gx=24).to_c()) == 1
+    assert b"power" in lib.dem_last_error_string()
+    assert lib.dem_validate_system(_sys(gy=0).to_c()) == 1
+    s = _sys().to_c()
+    s.numMaterials = 0
+    assert lib.dem_validate_system(s) == 1
+    s.numMaterials = 9
+    assert lib.dem_validate_system(s) == 1
+    s = _sys().to_c()
+    s.cubeDimension[0] = 0.0
+    assert lib.dem_validate_system(s) == 1
+
+
+def test_sort_scratch_sizes():
+    lib = _lib.load()
+    for n in (1, 1000, 4096, 1 << 20):
+        for bits in (0, 1, 10, 20, 32):
+            b = lib.dem_sort_scratch_bytes(n, bits)
+            assert b >= 8 * n
+    assert lib.dem_sort_scratch_bytes(1 << 22, 20) > lib.dem_sort_scratch_bytes(1 << 20, 20)
+
+
+def test_bad_arguments_are_status_codes_not_crashes():
+    lib = _lib.load()
+    s = _sys().to_c()
+    # NULL buffers with n > 0 are rejected before any CUDA call
+    assert lib.dem_calc_hash(s, None, None, None, 10, None) == 1
+    assert lib.dem_sort_particles(None, None, 10, 20, None, 0, None) == 1
+    assert lib.dem_sort_particles(None, None, 10, 33, None, 0, None) == 1
+    assert lib.dem_collide(s, None, None, None, None, None, None, None, None, None, None, 10,
+                           64, None, None) == 1
+    assert lib.dem_collide(s, None, None, None, None, None, None, None, None, None, None, 10,
+                           63, None, None) == 1  # numCells mismatch
+    assert lib.dem_integrate_system(s, None, None, None, None, None, None, None, None, None,
+                                    None, 10, None) == 1
+    h = C.c_void_p()
+    assert lib.dem_create(None, 10, 0, C.byref(h)) == 1
+    assert lib.dem_create(s, 0, 0, C.byref(h)) == 1
+    assert lib.dem_step(None, 1, None) == 1
+    assert lib.dem_destroy(None) == 0
+    # n = 0 is a no-op
+    assert lib.dem_calc_hash(s, None, None, None, 0, None) == 0
+
+
+def test_python_errors_raise():
+    with pytest.raises(D.DemError):
+        _lib.check(1)
