@@ -1,6 +1,7 @@
 // C ABI of the DEM step (include/demso_b200.h): argument checking, the
 // per-stage entry points, and the context that runs the fused, graph-captured
 // step on library-owned buffers.
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -78,6 +79,10 @@ KParams make_kparams(const DemSystem* s, uint32_t n) {
     P.gravy = s->gravity[1];
     P.ktWall = s->boundaryShearStiffness;
     P.nmat = s->numMaterials;
+    P.rmax = INFINITY;
+    P.cellW = P.Lx / P.gxf;
+    P.cellH = P.Ly / P.gyf;
+    P.cullMargin = 4e-6f * (P.Lx > P.Ly ? P.Lx : P.Ly);
     for (uint32_t a = 0; a < P.nmat; ++a) {
         const DemMaterial& A = s->materials[a];
         P.cn[a] = A.normalDamping;
@@ -264,8 +269,9 @@ struct DemContext {
     float* alpha = nullptr;
     uint32_t* errFlag = nullptr;
     void* sortScratch = nullptr;
-    SortScratch ss;
+    OnesweepScratch ss;
     bool keysValid = false;
+    float rmax = INFINITY;   // largest radius of the current state (culling bound)
     cudaStream_t capStream = nullptr;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int launchesPerStep = 0;
@@ -276,6 +282,7 @@ struct DemContext {
     bool profiling = false;
     cudaEvent_t marker[DEM_NUM_STAGES + 1] = {};
     cudaGraphExec_t pgraph[2] = {nullptr, nullptr};
+    cudaGraph_t pgraphSrc[2] = {nullptr, nullptr};  // kept: its nodes address the exec's nodes
     cudaGraphNode_t pnode[2][DEM_NUM_STAGES + 1] = {};
     cudaEvent_t* evPool = nullptr;
     uint32_t evCap = 0, evUsed = 0, stepsProfiled = 0;
@@ -294,6 +301,11 @@ void drop_graphs(DemContext* c) {
             cudaGraphExecDestroy(g);
             g = nullptr;
         }
+    for (auto& g : c->pgraphSrc)
+        if (g) {
+            cudaGraphDestroy(g);
+            g = nullptr;
+        }
 }
 
 // One step from (dyn[0], stat[cur]) into (dyn[0], stat[cur^1]).  With
@@ -306,7 +318,8 @@ cudaError_t enqueue_step(DemContext* c, cudaStream_t st, int* launches,
     if (markers && (e = cudaEventRecordWithFlags(markers[0], st, cudaEventRecordExternal)) != cudaSuccess)
         return e;
     uint32_t *ko, *vo;
-    e = radix_sort_pairs(c->keys, c->perm, c->n, c->keyBits, true, c->ss, st, &ko, &vo, launches);
+    e = onesweep_sort_pairs(c->keys, c->perm, c->n, c->keyBits, true, c->ss, c->errFlag, st, &ko,
+                            &vo, launches);
     if (e != cudaSuccess) return e;
     if (markers && (e = cudaEventRecordWithFlags(markers[1], st, cudaEventRecordExternal)) != cudaSuccess)
         return e;
@@ -360,7 +373,10 @@ int build_graph(DemContext* c, int parity, bool profiled) {
     }
     cudaGraphExec_t* slot = profiled ? &c->pgraph[parity] : &c->graph[parity];
     e = cudaGraphInstantiate(slot, g, 0);
-    cudaGraphDestroy(g);
+    if (profiled && e == cudaSuccess)
+        c->pgraphSrc[parity] = g;  // node handles stay valid while the graph lives
+    else
+        cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(e, "graph instantiate");
     c->launchesPerStep = launches;
     return DEM_OK;
@@ -370,6 +386,11 @@ void drop_profile(DemContext* c) {
     for (auto& g : c->pgraph)
         if (g) {
             cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    for (auto& g : c->pgraphSrc)
+        if (g) {
+            cudaGraphDestroy(g);
             g = nullptr;
         }
     if (c->evPool) {
@@ -416,7 +437,7 @@ extern "C" int dem_create(const DemSystem* sys, uint32_t capacity, uint32_t flag
     total += 2 * cells;                         // cellStart/End
     total += f4 + f8 + f4;                      // pressure, acc, alpha
     total += 256;                               // error flag
-    const size_t sortBytes = sort_scratch_bytes(capacity, c->keyBits);
+    const size_t sortBytes = onesweep_scratch_bytes(capacity, c->keyBits);
     cudaError_t e = cudaMalloc(&c->block, total);
     if (e != cudaSuccess) {
         delete c;
@@ -449,7 +470,7 @@ extern "C" int dem_create(const DemSystem* sys, uint32_t capacity, uint32_t flag
     c->acc = reinterpret_cast<float2*>(take(f8));
     c->alpha = reinterpret_cast<float*>(take(f4));
     c->errFlag = reinterpret_cast<uint32_t*>(take(256));
-    c->ss = carve_sort_scratch(c->sortScratch, capacity, c->keyBits);
+    c->ss = carve_onesweep_scratch(c->sortScratch, capacity, c->keyBits);
     e = cudaMemset(c->block, 0, total);
     if (e == cudaSuccess) e = cudaMemset(c->cellStart, 0xff, 4 * (size_t)c->numCells);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->capStream, cudaStreamNonBlocking);
@@ -485,6 +506,7 @@ extern "C" int dem_set_system(DemContext* c, const DemSystem* sys) {
         return fail(DEM_ERR_INVALID_ARG, "single/multi-material layout is fixed at dem_create");
     c->sys = *sys;
     c->P = make_kparams(sys, c->n);
+    c->P.rmax = c->rmax;
     drop_graphs(c);
     // keys depend on the box size; recompute before the next step
     c->keysValid = false;
@@ -513,11 +535,19 @@ extern "C" int dem_set_state(DemContext* c, uint32_t n, const float* pos, const 
     DEM_TRY_CUDA(cudaMemcpyAsync(c->stat[a].id, id, 4ull * n, k, st), "set id");
     if (c->typed)
         DEM_TRY_CUDA(cudaMemcpyAsync(c->stat[a].type, type, 4ull * n, k, st), "set type");
-    if (n != c->n) {
-        c->n = n;
-        c->P = make_kparams(&c->sys, n);
-        drop_graphs(c);
-    }
+    // the largest radius bounds every contact distance (neighbour culling)
+    uint32_t rbits = 0;
+    DEM_TRY_CUDA(launch_max_radius(c->stat[a].radius, n, c->errFlag + 1, st), "max radius");
+    DEM_TRY_CUDA(cudaMemcpyAsync(&rbits, c->errFlag + 1, 4, cudaMemcpyDeviceToHost, st),
+                 "max radius copy");
+    DEM_TRY_CUDA(cudaStreamSynchronize(st), "set_state sync");
+    float rmax;
+    memcpy(&rmax, &rbits, 4);
+    c->n = n;
+    c->rmax = (n > 0 && std::isfinite(rmax)) ? rmax : INFINITY;
+    c->P = make_kparams(&c->sys, n);
+    c->P.rmax = c->rmax;
+    drop_graphs(c);
     c->keysValid = false;
     return DEM_OK;
 }
@@ -596,6 +626,8 @@ extern "C" int dem_check(DemContext* c, void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
     DEM_TRY_CUDA(cudaMemcpyAsync(&flag, c->errFlag, 4, cudaMemcpyDeviceToHost, st), "read flag");
     DEM_TRY_CUDA(cudaStreamSynchronize(st), "sync");
+    if (flag & kSortTimeoutBit)
+        return fail(DEM_ERR_TIMEOUT, "a bounded wait in the sort gave up; the state is invalid");
     if (flag) return fail(DEM_ERR_OOB, "a particle position became NaN or infinite");
     return DEM_OK;
 }

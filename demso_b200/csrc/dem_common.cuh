@@ -38,6 +38,12 @@ struct KParams {
     float at[kMaxMat];    // attractCoefficient
     // per material pair (a * nmat + b): series kn, series kt, series cn, mean mu
     float4 pair[kMaxMat * kMaxMat];
+    // Neighbour culling (context step only): an upper bound on every radius
+    // (INFINITY disables culling), the cell size, and an absolute margin that
+    // covers float rounding of positions and cell bounds.
+    float rmax;
+    float cellW, cellH;
+    float cullMargin;
 };
 
 // particles_kernel.cuh:36-41, evaluated on the host when KParams is built.

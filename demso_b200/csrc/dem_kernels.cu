@@ -29,19 +29,23 @@ template <bool TYPED>
 __global__ void __launch_bounds__(kThreads)
 reorder_kernel(uint32_t* __restrict__ cellStart, uint32_t* __restrict__ cellEnd, DynSet s,
                StatSet sS, uint32_t* __restrict__ sLoc, const uint32_t* __restrict__ hash,
-               const uint32_t* __restrict__ index, DynSet o, StatSet oS, uint32_t n) {
+               const uint32_t* __restrict__ index, DynSet o, StatSet oS, uint32_t n,
+               uint32_t numCells) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = i < n;
     const uint32_t h = valid ? hash[i] : 0u;
     uint32_t hp = __shfl_up_sync(0xffffffffu, h, 1);
     if ((threadIdx.x & 31) == 0 && valid && i > 0) hp = hash[i - 1];
     if (!valid) return;
+    // keys outside the grid or indices outside the arrays can only come from a
+    // caller's own buffers; such entries are skipped rather than written
     if (i == 0 || h != hp) {
-        cellStart[h] = i;
-        if (i > 0) cellEnd[hp] = i;
+        if (h < numCells) cellStart[h] = i;
+        if (i > 0 && hp < numCells) cellEnd[hp] = i;
     }
-    if (i == n - 1) cellEnd[h] = i + 1;
+    if (i == n - 1 && h < numCells) cellEnd[h] = i + 1;
     const uint32_t src = index[i];
+    if (src >= n) return;
     s.pos[i] = o.pos[src];
     s.vel[i] = o.vel[src];
     s.theta[i] = o.theta[src];
@@ -50,7 +54,7 @@ reorder_kernel(uint32_t* __restrict__ cellStart, uint32_t* __restrict__ cellEnd,
     sS.mass[i] = oS.mass[src];
     const uint32_t id = oS.id[src];
     sS.id[i] = id;
-    sLoc[id] = i;
+    if (id < n) sLoc[id] = i;
     if (TYPED) sS.type[i] = oS.type[src];
 }
 
@@ -59,7 +63,21 @@ reorder_kernel(uint32_t* __restrict__ cellStart, uint32_t* __restrict__ cellEnd,
 // y-outer, x-inner, particles in ascending sorted index, each cell's
 // subtotal added to the running force.  Wrapping makes a 1- or 2-wide grid
 // visit the same cell more than once, exactly as the reference does.
-template <bool TYPED, bool ATTRACT>
+//
+// Work the reference spends on pairs that are not in contact is skipped
+// without changing any result, because such a pair adds nothing (its force
+// is +0 and it touches neither moment nor pressure):
+//  * a candidate is dropped before the square root when its squared distance
+//    exceeds (rA + rB)^2 by a relative 2e-6; then sqrtf(d2) >= rA + rB after
+//    rounding, which is the reference's no-contact branch;
+//  * with CULL (the context step, which knows an upper bound rmax on all
+//    radii), a neighbour column/row is not visited when the particle is
+//    farther than rA + rmax (plus a rounding margin) from that side of its
+//    own cell, and candidates are first tested against rA + rmax so that
+//    the neighbour's radius is loaded only for near pairs.  Culling needs at
+//    least 3 cells per axis (then the three columns/rows are distinct cells)
+//    and a particle inside the box.
+template <bool TYPED, bool ATTRACT, bool CULL>
 __device__ __forceinline__ void collide_one(const KParams& P, uint32_t i, float2 p, float2 v,
                                             float w, float r, uint32_t mat,
                                             const float2* __restrict__ pos,
@@ -75,10 +93,22 @@ __device__ __forceinline__ void collide_one(const KParams& P, uint32_t i, float2
     moment = 0.0f;
     pr = 0.0f;
     const float4 pc0 = P.pair[0];
+    int y0 = -1, y1 = 1, x0 = -1, x1 = 1;
+    float reach2 = INFINITY;
+    if (CULL && p.x >= 0.0f && p.x < P.Lx && p.y >= 0.0f && p.y < P.Ly) {
+        const float reach = (r + P.rmax) * 1.0001f + P.cullMargin;
+        const float X0 = (float)g.x * P.cellW, Y0 = (float)g.y * P.cellH;
+        if (p.x - X0 > reach) x0 = 0;
+        if (X0 + P.cellW - p.x > reach) x1 = 0;
+        if (p.y - Y0 > reach) y0 = 0;
+        if (Y0 + P.cellH - p.y > reach) y1 = 0;
+        const float rr = (r + P.rmax) * 1.0001f;
+        reach2 = rr * rr;
+    }
 #pragma unroll 1
-    for (int dy = -1; dy <= 1; ++dy) {
+    for (int dy = y0; dy <= y1; ++dy) {
 #pragma unroll 1
-        for (int dx = -1; dx <= 1; ++dx) {
+        for (int dx = x0; dx <= x1; ++dx) {
             const uint32_t h = grid_hash(P, g.x + dx, g.y + dy);
             const uint32_t start = __ldg(cellStart + h);
             float2 fc = make_float2(0.0f, 0.0f);
@@ -88,6 +118,9 @@ __device__ __forceinline__ void collide_one(const KParams& P, uint32_t i, float2
                 for (uint32_t j = start; j < end; ++j) {
                     if (j == i) continue;
                     const float2 pj = __ldg(pos + j);
+                    const float relx = pj.x - p.x, rely = pj.y - p.y;
+                    const float d2 = relx * relx + rely * rely;
+                    if (!ATTRACT && CULL && d2 > reach2) continue;
                     const float rj = __ldg(radius + j);
                     uint32_t mj = 0;
                     float4 pc = pc0;
@@ -95,10 +128,8 @@ __device__ __forceinline__ void collide_one(const KParams& P, uint32_t i, float2
                         mj = __ldg(type + j);
                         pc = P.pair[mat * P.nmat + mj];
                     }
-                    // contact test first; velocity/omega of j only for contacts
-                    const float relx = pj.x - p.x, rely = pj.y - p.y;
-                    const float dist = len2(relx, rely);
-                    if (dist < r + rj) {
+                    const float cd = r + rj;
+                    if (d2 <= cd * cd * 1.000002f && sqrtf(d2) < cd) {
                         const float2 f = pair_force(p, pj, v, __ldg(vel + j), w, __ldg(omega + j),
                                                     r, rj, pc, P.dt, moment, pr);
                         fc.x += f.x;
@@ -134,8 +165,8 @@ collide_kernel(KParams P, const float2* __restrict__ pos, const float2* __restri
     const uint32_t mat = TYPED ? type[i] : 0u;
     float2 f;
     float moment, pr;
-    collide_one<TYPED, ATTRACT>(P, i, p, v, w, r, mat, pos, vel, omega, radius, type, cellStart,
-                                cellEnd, f, moment, pr);
+    collide_one<TYPED, ATTRACT, false>(P, i, p, v, w, r, mat, pos, vel, omega, radius, type,
+                                       cellStart, cellEnd, f, moment, pr);
     const float m = mass[i];
     acc[i] = make_float2(f.x / m, f.y / m);
     alpha[i] = moment / inertia_of(m, r);
@@ -169,7 +200,7 @@ integrate_kernel(KParams P, float2* __restrict__ pos, float2* __restrict__ vel,
 // collideD + integrateSystemD + calcHashD of the next step for one particle.
 // The acceleration stays in registers instead of a round trip through HBM;
 // the arithmetic is the same expressions in the same order.
-template <bool TYPED, bool ATTRACT>
+template <bool TYPED, bool ATTRACT, bool CULL>
 __global__ void __launch_bounds__(kCollideThreads)
 step_kernel(KParams P, DynSet in, StatSet inS, const uint32_t* __restrict__ cellStart,
             const uint32_t* __restrict__ cellEnd, DynSet out, uint32_t* __restrict__ nextHash,
@@ -185,8 +216,8 @@ step_kernel(KParams P, DynSet in, StatSet inS, const uint32_t* __restrict__ cell
     const uint32_t mat = TYPED ? inS.type[i] : 0u;
     float2 f;
     float moment, pr;
-    collide_one<TYPED, ATTRACT>(P, i, s.p, s.v, s.w, r, mat, in.pos, in.vel, in.omega, inS.radius,
-                                inS.type, cellStart, cellEnd, f, moment, pr);
+    collide_one<TYPED, ATTRACT, CULL>(P, i, s.p, s.v, s.w, r, mat, in.pos, in.vel, in.omega,
+                                      inS.radius, inS.type, cellStart, cellEnd, f, moment, pr);
     const float m = inS.mass[i];
     const float2 a = make_float2(f.x / m, f.y / m);
     const float al = moment / inertia_of(m, r);
@@ -229,6 +260,17 @@ __global__ void followed_kernel(FollowIds f, const uint32_t* __restrict__ loc, D
     r[11] = pressure ? pressure[i] : 0.0f;
 }
 
+// Largest radius (positive floats order like their bit patterns).
+__global__ void max_radius_kernel(const float* __restrict__ radius, uint32_t n,
+                                  uint32_t* __restrict__ out) {
+    float m = 0.0f;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        m = fmaxf(m, radius[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+}
+
 bool has_attraction(const KParams& P) {
     for (uint32_t m = 0; m < P.nmat; ++m)
         if (P.at[m] != 0.0f) return true;
@@ -241,6 +283,14 @@ cudaError_t launch_followed(const FollowIds& f, const uint32_t* loc, DynSet d, S
                             const float2* acc, const float* alpha, const float* pressure,
                             float* rows, cudaStream_t st) {
     followed_kernel<<<1, kFollowBatch, 0, st>>>(f, loc, d, s, acc, alpha, pressure, rows);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_max_radius(const float* radius, uint32_t n, uint32_t* out, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(uint32_t), st);
+    if (e != cudaSuccess || n == 0) return e;
+    const unsigned b = blocks_for(n, kThreads) < 1184 ? blocks_for(n, kThreads) : 1184;
+    max_radius_kernel<<<b, kThreads, 0, st>>>(radius, n, out);
     return cudaGetLastError();
 }
 
@@ -264,10 +314,10 @@ cudaError_t launch_reorder(const KParams& P, uint32_t* cellStart, uint32_t* cell
     if (n == 0) return cudaSuccess;
     if (sortedS.type && oldS.type)
         reorder_kernel<true><<<blocks_for(n, kThreads), kThreads, 0, st>>>(
-            cellStart, cellEnd, sorted, sortedS, sortedLoc, hash, index, old, oldS, n);
+            cellStart, cellEnd, sorted, sortedS, sortedLoc, hash, index, old, oldS, n, numCells);
     else
         reorder_kernel<false><<<blocks_for(n, kThreads), kThreads, 0, st>>>(
-            cellStart, cellEnd, sorted, sortedS, sortedLoc, hash, index, old, oldS, n);
+            cellStart, cellEnd, sorted, sortedS, sortedLoc, hash, index, old, oldS, n, numCells);
     if (launches) ++*launches;
     return cudaGetLastError();
 }
@@ -317,14 +367,22 @@ cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t
     const bool typed = inS.type != nullptr && P.nmat > 1;
     const bool attract = has_attraction(P);
     const unsigned b = blocks_for(n, kCollideThreads);
-#define DEM_STEP(T, A)                                                                      \
-    step_kernel<T, A><<<b, kCollideThreads, 0, st>>>(P, in, inS, cellStart, cellEnd, out,    \
-                                                     nextHash, pressure, acc, alpha, errFlag, \
-                                                     n)
+#define DEM_STEP(T, A, C)                                                                   \
+    step_kernel<T, A, C><<<b, kCollideThreads, 0, st>>>(P, in, inS, cellStart, cellEnd, out,  \
+                                                        nextHash, pressure, acc, alpha,       \
+                                                        errFlag, n)
+    // culling also needs cells wider than any contact distance, so that a
+    // wrapped neighbour column/row is never within reach
+    const bool cull = isfinite(P.rmax) && P.gx >= 3 && P.gy >= 3 &&
+                      P.cellW > 2.002f * P.rmax && P.cellH > 2.002f * P.rmax;
     if (typed) {
-        if (attract) DEM_STEP(true, true); else DEM_STEP(true, false);
+        if (attract) DEM_STEP(true, true, false);
+        else if (cull) DEM_STEP(true, false, true);
+        else DEM_STEP(true, false, false);
     } else {
-        if (attract) DEM_STEP(false, true); else DEM_STEP(false, false);
+        if (attract) DEM_STEP(false, true, false);
+        else if (cull) DEM_STEP(false, false, true);
+        else DEM_STEP(false, false, false);
     }
 #undef DEM_STEP
     return cudaGetLastError();

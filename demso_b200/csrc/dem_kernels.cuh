@@ -31,6 +31,9 @@ cudaError_t launch_followed(const FollowIds& f, const uint32_t* loc, DynSet d, S
                             const float2* acc, const float* alpha, const float* pressure,
                             float* rows, cudaStream_t st);
 
+// Upper bound of the radii: writes the largest radius's bit pattern to *out.
+cudaError_t launch_max_radius(const float* radius, uint32_t n, uint32_t* out, cudaStream_t st);
+
 cudaError_t launch_calc_hash(const KParams& P, const float2* pos, uint32_t* hash, uint32_t* index,
                              uint32_t n, cudaStream_t st);
 

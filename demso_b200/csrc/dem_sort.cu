@@ -196,6 +196,174 @@ downsweep_kernel(const uint32_t* __restrict__ keysIn, const uint32_t* __restrict
     }
 }
 
+// ---------------------------------------------------------------- onesweep
+constexpr uint32_t kFlagAgg = 1u << 30;   // tile aggregate published
+constexpr uint32_t kFlagIncl = 2u << 30;  // inclusive prefix published
+constexpr uint32_t kValueMask = (1u << 30) - 1u;
+constexpr uint32_t kSpinLimit = 1u << 22;
+constexpr int kHistBlocksPerSM = 2;
+
+// Global digit histograms of every pass.  Each thread walks a run of
+// consecutive keys and adds one count per run of equal digits, so nearly
+// sorted input (the step's common case) needs few shared-memory atomics.
+template <int BITS>
+__global__ void __launch_bounds__(kSortThreads)
+global_hist_kernel(const uint32_t* __restrict__ keys, uint32_t n, int passes, int4 shifts,
+                   int4 rowsv, uint32_t* __restrict__ gh) {
+    constexpr int R = 1 << BITS;
+    __shared__ uint32_t h[4][R];
+    const int sh[4] = {shifts.x, shifts.y, shifts.z, shifts.w};
+    const int rw[4] = {rowsv.x, rowsv.y, rowsv.z, rowsv.w};
+    for (int i = threadIdx.x; i < 4 * R; i += kSortThreads) (&h[0][0])[i] = 0;
+    __syncthreads();
+    const uint32_t per = 16;
+    const size_t stride = (size_t)gridDim.x * kSortThreads * per;
+    for (size_t base = ((size_t)blockIdx.x * kSortThreads + threadIdx.x) * per; base < n;
+         base += stride) {
+        const uint32_t cnt = (uint32_t)min((size_t)per, (size_t)n - base);
+        for (int p = 0; p < passes; ++p) {
+            const uint32_t mask = (uint32_t)rw[p] - 1u;
+            uint32_t cur = (__ldg(keys + base) >> sh[p]) & mask, run = 1;
+            for (uint32_t k = 1; k < cnt; ++k) {
+                const uint32_t d = (__ldg(keys + base + k) >> sh[p]) & mask;
+                if (d == cur) {
+                    ++run;
+                } else {
+                    atomicAdd(&h[p][cur], run);
+                    cur = d;
+                    run = 1;
+                }
+            }
+            atomicAdd(&h[p][cur], run);
+        }
+    }
+    __syncthreads();
+    for (int p = 0; p < passes; ++p)
+        for (int d = threadIdx.x; d < rw[p]; d += kSortThreads)
+            if (h[p][d]) atomicAdd(gh + (size_t)p * R + d, h[p][d]);
+}
+
+// Exclusive scan of each pass's row of the global histogram (one block per pass).
+template <int BITS>
+__global__ void __launch_bounds__(1024) global_hist_scan_kernel(uint32_t* __restrict__ gh) {
+    constexpr int R = 1 << BITS;
+    constexpr int PER = (R + 1023) / 1024;
+    __shared__ uint32_t warpTot[32];
+    uint32_t* row = gh + (size_t)blockIdx.x * R;
+    uint32_t v[PER];
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int d = threadIdx.x * PER + k;
+        v[k] = d < R ? row[d] : 0u;
+        s += v[k];
+    }
+    uint32_t total;
+    uint32_t run = block_exclusive_scan<1024>(s, warpTot, total);
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int d = threadIdx.x * PER + k;
+        if (d < R) row[d] = run;
+        run += v[k];
+    }
+}
+
+template <int BITS, bool IDENT>
+__global__ void __launch_bounds__(kSortThreads, 3)
+onesweep_kernel(const uint32_t* __restrict__ keysIn, const uint32_t* __restrict__ valsIn,
+                uint32_t* __restrict__ keysOut, uint32_t* __restrict__ valsOut, uint32_t n,
+                int shift, uint32_t rows, const uint32_t* __restrict__ gOffset,
+                uint32_t* __restrict__ lookback, uint32_t* __restrict__ errFlag) {
+    constexpr int R = 1 << BITS;
+    __shared__ uint16_t cnt[kSortWarps][R];
+    __shared__ uint32_t dbase[R];
+    __shared__ uint32_t tileS;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t mask = rows - 1u;
+    if (threadIdx.x == 0) tileS = atomicAdd(lookback, 1u);
+    uint16_t* flat = &cnt[0][0];
+    for (int i = threadIdx.x; i < kSortWarps * R; i += kSortThreads) flat[i] = 0;
+    __syncthreads();
+    const uint32_t tile = tileS;
+    volatile uint32_t* lb = lookback + 64;
+
+    const size_t wbase = (size_t)tile * kSortTile + (size_t)warp * (kSortItems * 32);
+    uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+        const size_t idx = wbase + (size_t)k * 32 + lane;
+        const bool valid = idx < n;
+        key[k] = valid ? __ldg(keysIn + idx) : 0u;
+        if (IDENT) val[k] = (uint32_t)idx;
+        else val[k] = valid ? __ldg(valsIn + idx) : 0u;
+    }
+    const uint32_t lt = lanemask_lt();
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+        const size_t idx = wbase + (size_t)k * 32 + lane;
+        const bool valid = idx < n;
+        const uint32_t d = valid ? ((key[k] >> shift) & mask) : 0xffffffffu;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t c = valid ? (uint32_t)cnt[warp][d] : 0u;
+        __syncwarp();
+        if (valid && (peers & lt) == 0u) cnt[warp][d] = (uint16_t)(c + (uint32_t)__popc(peers));
+        __syncwarp();
+        rank[k] = c + (uint32_t)__popc(peers & lt);
+    }
+    __syncthreads();
+    // per digit: exclusive offsets of the warps and the tile's count, which is
+    // published at once (inclusive for tile 0) before any look-back starts
+    for (uint32_t d = threadIdx.x; d < rows; d += kSortThreads) {
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w) {
+            const uint32_t c = cnt[w][d];
+            cnt[w][d] = (uint16_t)run;
+            run += c;
+        }
+        lb[(size_t)tile * rows + d] = (tile == 0 ? kFlagIncl : kFlagAgg) | run;
+        dbase[d] = run;
+    }
+    // decoupled look-back: the tile's exclusive prefix of each digit
+    for (uint32_t d = threadIdx.x; d < rows; d += kSortThreads) {
+        const uint32_t run = dbase[d];
+        uint32_t excl = 0;
+        if (tile > 0) {
+            uint32_t spins = 0;
+            int t = (int)tile - 1;
+            while (true) {
+                const uint32_t v = lb[(size_t)t * rows + d];
+                if ((v & ~kValueMask) == 0u) {
+                    if (++spins > kSpinLimit) {
+                        atomicOr(errFlag, kSortTimeoutBit);
+                        break;
+                    }
+                    if (spins > 64) __nanosleep(64);
+                    continue;
+                }
+                excl += v & kValueMask;
+                if ((v & kFlagIncl) || t == 0) break;
+                --t;
+            }
+            lb[(size_t)tile * rows + d] = kFlagIncl | (excl + run);
+        }
+        dbase[d] = gOffset[d] + excl;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+        const size_t idx = wbase + (size_t)k * 32 + lane;
+        if (idx < n) {
+            const uint32_t d = (key[k] >> shift) & mask;
+            const uint32_t dst = dbase[d] + (uint32_t)cnt[warp][d] + rank[k];
+            if (dst < n) {
+                keysOut[dst] = key[k];
+                valsOut[dst] = val[k];
+            }
+        }
+    }
+}
+
 __global__ void iota_kernel(uint32_t* __restrict__ v, uint32_t n) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) v[i] = i;
@@ -273,6 +441,109 @@ SortScratch carve_sort_scratch(void* base, uint32_t n, uint32_t keyBits) {
     p += align256(sizeof(uint32_t) * std::max<size_t>(hw, 1));
     s.partials = reinterpret_cast<uint32_t*>(p);
     return s;
+}
+
+size_t onesweep_scratch_bytes(uint32_t n, uint32_t keyBits) {
+    const SortPlan plan = make_sort_plan(keyBits);
+    const size_t numTiles = (n + kSortTile - 1) / kSortTile;
+    const size_t R = (size_t)1 << (plan.radixBits ? plan.radixBits : 6);
+    return 2 * align256(sizeof(uint32_t) * std::max<size_t>(n, 1)) +
+           align256(sizeof(uint32_t) * 4 * R) +
+           align256(sizeof(uint32_t) * (64 + numTiles * R));
+}
+
+OnesweepScratch carve_onesweep_scratch(void* base, uint32_t n, uint32_t keyBits) {
+    const SortPlan plan = make_sort_plan(keyBits);
+    const size_t R = (size_t)1 << (plan.radixBits ? plan.radixBits : 6);
+    char* p = static_cast<char*>(base);
+    OnesweepScratch s;
+    s.altKeys = reinterpret_cast<uint32_t*>(p);
+    p += align256(sizeof(uint32_t) * std::max<size_t>(n, 1));
+    s.altVals = reinterpret_cast<uint32_t*>(p);
+    p += align256(sizeof(uint32_t) * std::max<size_t>(n, 1));
+    s.globalHist = reinterpret_cast<uint32_t*>(p);
+    p += align256(sizeof(uint32_t) * 4 * R);
+    s.lookback = reinterpret_cast<uint32_t*>(p);
+    return s;
+}
+
+namespace {
+template <int BITS>
+cudaError_t onesweep_impl(uint32_t* keys, uint32_t* vals, uint32_t n, const SortPlan& plan,
+                          bool identityVals, const OnesweepScratch& s, uint32_t* errFlag,
+                          cudaStream_t st, uint32_t** keysOut, uint32_t** valsOut,
+                          int* launches) {
+    constexpr int R = 1 << BITS;
+    const uint32_t numTiles = (n + kSortTile - 1) / kSortTile;
+    cudaError_t e = cudaMemsetAsync(s.globalHist, 0, sizeof(uint32_t) * 4 * R, st);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t perBlock = (size_t)kSortThreads * 16;
+    const unsigned hb = (unsigned)std::max<size_t>(
+        1, std::min<size_t>((size_t)sms * kHistBlocksPerSM, (n + perBlock - 1) / perBlock));
+    const int4 shifts = make_int4(plan.shift[0], plan.shift[1], plan.shift[2], plan.shift[3]);
+    const int4 rowsv = make_int4(1 << plan.bits[0], 1 << plan.bits[1], 1 << plan.bits[2],
+                                 1 << plan.bits[3]);
+    global_hist_kernel<BITS><<<hb, kSortThreads, 0, st>>>(keys, n, plan.passes, shifts, rowsv,
+                                                          s.globalHist);
+    global_hist_scan_kernel<BITS><<<plan.passes, 1024, 0, st>>>(s.globalHist);
+    if (launches) *launches += 2;
+    uint32_t *ki = keys, *vi = vals, *ko = s.altKeys, *vo = s.altVals;
+    for (int p = 0; p < plan.passes; ++p) {
+        const uint32_t rows = 1u << plan.bits[p];
+        e = cudaMemsetAsync(s.lookback, 0, sizeof(uint32_t) * (64 + (size_t)numTiles * rows), st);
+        if (e != cudaSuccess) return e;
+        const uint32_t* go = s.globalHist + (size_t)p * R;
+        if (identityVals && p == 0)
+            onesweep_kernel<BITS, true><<<numTiles, kSortThreads, 0, st>>>(
+                ki, vi, ko, vo, n, plan.shift[p], rows, go, s.lookback, errFlag);
+        else
+            onesweep_kernel<BITS, false><<<numTiles, kSortThreads, 0, st>>>(
+                ki, vi, ko, vo, n, plan.shift[p], rows, go, s.lookback, errFlag);
+        if (launches) ++*launches;
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        std::swap(ki, ko);
+        std::swap(vi, vo);
+    }
+    *keysOut = ki;
+    *valsOut = vi;
+    return cudaSuccess;
+}
+}  // namespace
+
+cudaError_t onesweep_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t keyBits,
+                                bool identityVals, const OnesweepScratch& s, uint32_t* errFlag,
+                                cudaStream_t st, uint32_t** keysOut, uint32_t** valsOut,
+                                int* launches) {
+    *keysOut = keys;
+    *valsOut = vals;
+    if (n == 0) return cudaSuccess;
+    if (n >= (1u << 30)) return cudaErrorInvalidValue;
+    const SortPlan plan = make_sort_plan(keyBits);
+    if (plan.passes == 0) {
+        if (identityVals) {
+            iota_kernel<<<(n + 255) / 256, 256, 0, st>>>(vals, n);
+            if (launches) ++*launches;
+        }
+        return cudaGetLastError();
+    }
+    switch (plan.radixBits) {
+        case 6:
+            return onesweep_impl<6>(keys, vals, n, plan, identityVals, s, errFlag, st, keysOut,
+                                    valsOut, launches);
+        case 8:
+            return onesweep_impl<8>(keys, vals, n, plan, identityVals, s, errFlag, st, keysOut,
+                                    valsOut, launches);
+        case 10:
+            return onesweep_impl<10>(keys, vals, n, plan, identityVals, s, errFlag, st, keysOut,
+                                     valsOut, launches);
+        default:
+            return onesweep_impl<11>(keys, vals, n, plan, identityVals, s, errFlag, st, keysOut,
+                                     valsOut, launches);
+    }
 }
 
 cudaError_t exclusive_scan_u32(uint32_t* data, size_t len, uint32_t* partials, cudaStream_t st,

@@ -51,6 +51,28 @@ cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_
                              bool identityVals, const SortScratch& s, cudaStream_t stream,
                              uint32_t** keysOut, uint32_t** valsOut, int* launches);
 
+// Single-pass-per-digit variant ("onesweep"): one kernel computes the global
+// digit histograms of every pass from the input keys, then each pass is one
+// kernel whose tiles take their digit offsets from their predecessors by
+// decoupled look-back.  Tiles are numbered in launch order by an atomic
+// counter, so a tile only ever waits on tiles that are already running;
+// every wait is bounded and, if it gives up, sets kSortTimeoutBit in
+// *errFlag and carries on (the result is then invalid, never a hang).
+constexpr uint32_t kSortTimeoutBit = 2u;
+
+struct OnesweepScratch {
+    uint32_t* altKeys;    // n
+    uint32_t* altVals;    // n
+    uint32_t* globalHist; // passes * 2^maxBits (exclusive offsets after the scan)
+    uint32_t* lookback;   // 1 counter word padded to 64, then numTiles * 2^maxBits
+};
+size_t onesweep_scratch_bytes(uint32_t n, uint32_t keyBits);
+OnesweepScratch carve_onesweep_scratch(void* base, uint32_t n, uint32_t keyBits);
+cudaError_t onesweep_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t keyBits,
+                                bool identityVals, const OnesweepScratch& s, uint32_t* errFlag,
+                                cudaStream_t stream, uint32_t** keysOut, uint32_t** valsOut,
+                                int* launches);
+
 // Exclusive scan of `len` words in place; partials holds sort_scan_partials(len).
 cudaError_t exclusive_scan_u32(uint32_t* data, size_t len, uint32_t* partials,
                                cudaStream_t stream, int* launches);

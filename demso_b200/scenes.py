@@ -205,4 +205,21 @@ def plain_at_scale(n=4194304, seed=0, grid="2r", dt=2e-6, phi=0.55) -> Scene:
     mat = pair_material()
     sys = System(Lx=W, Ly=H, gx=gx, gy=gy, dt=dt, gravity=(0.0, -9.81),
                  knWall=mat.normalStiffness, ktWall=mat.shearStiffness, materials=[mat])
-    return _finish(sys, pos, np.zeros((n, 2)), radius, name="plain_at_scale_%d" % n)
+    # number the disks in cell order, as the reference's block generators
+    # number theirs lattice row by lattice row (createRectanglesD,
+    # particles_kernel.cuh:61-71)
+    order = np.argsort(cell_hash(pos, sys), kind="stable")
+    return _finish(sys, pos[order], np.zeros((n, 2)), radius[order],
+                   name="plain_at_scale_%d" % n)
+
+
+def cell_hash(pos, sys: System) -> np.ndarray:
+    """The reference's cell index of each position (particles_kernel.cuh:114-130),
+    with the same float32 operations."""
+    p = np.asarray(pos, dtype=np.float32)
+    gxf, gyf = np.float32(sys.gx), np.float32(sys.gy)
+    cx = np.floor((p[:, 0] * gxf) / np.float32(sys.Lx)).astype(np.int64)
+    cy = np.floor((p[:, 1] * gyf) / np.float32(sys.Ly)).astype(np.int64)
+    cx &= sys.gx - 1
+    cy &= sys.gy - 1
+    return (cy * sys.gx + cx).astype(np.uint32)

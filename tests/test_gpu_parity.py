@@ -175,3 +175,39 @@ def test_trajectory_within_tolerance_of_fp64_oracle():
     pa = out["pos"][np.argsort(out["id"])].astype(np.float64)
     pb = ref["pos"][np.argsort(ref["id"])]
     assert np.abs(pa - pb).max() < 1e-6
+
+
+def _permuted(sc, seed):
+    """The same scene with its particles stored in a random order (ids kept)."""
+    perm = np.random.default_rng(seed).permutation(sc.n)
+    st = sc.state()
+    return {k: (None if v is None else np.ascontiguousarray(v[perm])) for k, v in st.items()}
+
+
+def test_step_from_random_order_matches_oracle(f32):
+    """First sort of the context step on a fully shuffled state (the look-back
+    sort then sees random keys, not the nearly sorted keys of later steps)."""
+    sc = scenes.agitated_gas(n=50000, seed=17)
+    st = _permuted(sc, 3)
+    out = gpu_run(sc.sys, st, 3)
+    ref = f32.run(sc.sys, st, 3)
+    for k in FINAL_KEYS:
+        assert same(out[k], ref[k]), k
+
+
+def test_step_scale_scene_matches_oracle(f32):
+    """The plain-at-scale workload at 262,144 disks (log-normal radii, random
+    sequential placement, neighbour culling active) for 50 steps."""
+    sc = scenes.plain_at_scale(262144, seed=5)
+    out = gpu_run(sc.sys, sc.state(), 50, chunks=[7, 43])
+    ref = f32.run(sc.sys, sc.state(), 50)
+    for k in FINAL_KEYS:
+        assert same(out[k], ref[k]), k
+
+
+def test_step_one_million_matches_oracle(f32):
+    sc = scenes.agitated_gas(n=1 << 20, seed=41)
+    out = gpu_run(sc.sys, sc.state(), 4)
+    ref = f32.run(sc.sys, sc.state(), 4)
+    for k in FINAL_KEYS:
+        assert same(out[k], ref[k]), k
