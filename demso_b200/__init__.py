@@ -256,9 +256,11 @@ class Simulation:
     def kernels_per_step(self) -> int:
         return int(load().dem_kernels_per_step(self._h))
 
-    def cells(self):
-        """(cellStart, cellEnd) device pointers of the last reorder."""
-        import ctypes as C
-        a, b = C.c_void_p(), C.c_void_p()
-        check(load().dem_get_cells(self._h, C.byref(a), C.byref(b)))
-        return a.value, b.value
+    def cells(self, stream=None):
+        """(cellStart, cellEnd) of the last step's reorder as int32 CUDA tensors."""
+        import torch
+        nc = self.sys.num_cells
+        cs = torch.empty(nc, dtype=torch.int32, device="cuda")
+        ce = torch.empty(nc, dtype=torch.int32, device="cuda")
+        check(load().dem_get_cells(self._h, cs.data_ptr(), ce.data_ptr(), _stream(stream)))
+        return cs, ce

@@ -60,7 +60,7 @@ SIGNATURES = [
     ("dem_set_state", C.c_int, [_P, _U] + [_P] * 8 + [C.c_int, _P]),
     ("dem_get_state", C.c_int, [_P] + [_P] * 12 + [C.c_int, _P]),
     ("dem_step", C.c_int, [_P, _U, _P]),
-    ("dem_get_cells", C.c_int, [_P, C.POINTER(_P), C.POINTER(_P)]),
+    ("dem_get_cells", C.c_int, [_P, _P, _P, _P]),
     ("dem_check", C.c_int, [_P, _P]),
     ("dem_kernels_per_step", C.c_int, [_P]),
     ("dem_get_followed", C.c_int, [_P, _P, _U, _P, _P]),

@@ -263,7 +263,7 @@ struct DemContext {
     uint32_t* loc = nullptr;   // indexed by id
     uint32_t* keys = nullptr;  // cell of each particle of the current state
     uint32_t* perm = nullptr;  // sort values (source index of each sorted slot)
-    uint32_t *cellStart = nullptr, *cellEnd = nullptr;
+    uint2* cellRange = nullptr;  // interleaved (cellStart, cellEnd) per cell
     float* pressure = nullptr;
     float2* acc = nullptr;
     float* alpha = nullptr;
@@ -323,12 +323,12 @@ cudaError_t enqueue_step(DemContext* c, cudaStream_t st, int* launches,
     if (e != cudaSuccess) return e;
     if (markers && (e = cudaEventRecordWithFlags(markers[1], st, cudaEventRecordExternal)) != cudaSuccess)
         return e;
-    e = launch_reorder(c->P, c->cellStart, c->cellEnd, c->dyn[1], c->stat[b], c->loc, ko, vo,
-                       c->dyn[0], c->stat[a], c->n, c->numCells, true, st, launches);
+    e = launch_reorder_packed(c->cellRange, c->dyn[1], c->stat[b], c->loc, ko, vo, c->dyn[0],
+                              c->stat[a], c->n, c->numCells, st, launches);
     if (e != cudaSuccess) return e;
     if (markers && (e = cudaEventRecordWithFlags(markers[2], st, cudaEventRecordExternal)) != cudaSuccess)
         return e;
-    e = launch_step(c->P, c->dyn[1], c->stat[b], c->cellStart, c->cellEnd, c->dyn[0], c->keys,
+    e = launch_step(c->P, c->dyn[1], c->stat[b], ko, c->cellRange, c->dyn[0], c->keys,
                     (c->flags & DEM_CTX_PRESSURE) ? c->pressure : nullptr,
                     (c->flags & DEM_CTX_ACCEL) ? c->acc : nullptr,
                     (c->flags & DEM_CTX_ACCEL) ? c->alpha : nullptr, c->errFlag, c->n, st);
@@ -434,7 +434,7 @@ extern "C" int dem_create(const DemSystem* sys, uint32_t capacity, uint32_t flag
     total += 2 * (2 * f8 + 2 * f4);             // dyn sets
     total += 2 * (3 * f4 + (c->typed ? f4 : 0)); // static sets
     total += 3 * f4;                            // loc, keys, perm
-    total += 2 * cells;                         // cellStart/End
+    total += 2 * cells;                         // interleaved cell ranges
     total += f4 + f8 + f4;                      // pressure, acc, alpha
     total += 256;                               // error flag
     const size_t sortBytes = onesweep_scratch_bytes(capacity, c->keyBits);
@@ -464,15 +464,14 @@ extern "C" int dem_create(const DemSystem* sys, uint32_t capacity, uint32_t flag
     c->loc = reinterpret_cast<uint32_t*>(take(f4));
     c->keys = reinterpret_cast<uint32_t*>(take(f4));
     c->perm = reinterpret_cast<uint32_t*>(take(f4));
-    c->cellStart = reinterpret_cast<uint32_t*>(take(cells));
-    c->cellEnd = reinterpret_cast<uint32_t*>(take(cells));
+    c->cellRange = reinterpret_cast<uint2*>(take(2 * cells));
     c->pressure = reinterpret_cast<float*>(take(f4));
     c->acc = reinterpret_cast<float2*>(take(f8));
     c->alpha = reinterpret_cast<float*>(take(f4));
     c->errFlag = reinterpret_cast<uint32_t*>(take(256));
     c->ss = carve_onesweep_scratch(c->sortScratch, capacity, c->keyBits);
     e = cudaMemset(c->block, 0, total);
-    if (e == cudaSuccess) e = cudaMemset(c->cellStart, 0xff, 4 * (size_t)c->numCells);
+    if (e == cudaSuccess) e = cudaMemset(c->cellRange, 0xff, 8 * (size_t)c->numCells);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->capStream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         cudaFree(c->sortScratch);
@@ -613,10 +612,12 @@ extern "C" int dem_step(DemContext* c, uint32_t nsteps, void* stream) {
     return DEM_OK;
 }
 
-extern "C" int dem_get_cells(DemContext* c, const uint32_t** cellStart, const uint32_t** cellEnd) {
+extern "C" int dem_get_cells(DemContext* c, uint32_t* cellStart, uint32_t* cellEnd,
+                             void* stream) {
     if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
-    if (cellStart) *cellStart = c->cellStart;
-    if (cellEnd) *cellEnd = c->cellEnd;
+    DEM_TRY_CUDA(launch_unpack_cells(c->cellRange, c->numCells, cellStart, cellEnd,
+                                     (cudaStream_t)stream),
+                 "unpack cells");
     return DEM_OK;
 }
 

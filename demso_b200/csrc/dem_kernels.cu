@@ -58,15 +58,67 @@ reorder_kernel(uint32_t* __restrict__ cellStart, uint32_t* __restrict__ cellEnd,
     if (TYPED) sS.type[i] = oS.type[src];
 }
 
+// Cell ranges, read either from the reference's two arrays (cellStart with
+// 0xFFFFFFFF for empty cells, cellEnd) or from the context's interleaved
+// (start, end) pairs.  An empty cell yields start >= end, so its particle
+// loop runs zero times, as the reference's `startIndex != -1` test does.
+struct SplitCells {
+    const uint32_t* __restrict__ start;
+    const uint32_t* __restrict__ end;
+    __device__ __forceinline__ uint2 get(uint32_t h) const {
+        const uint32_t a = __ldg(start + h);
+        return make_uint2(a, a == kEmptyCell ? 0u : __ldg(end + h));
+    }
+};
+struct PackedCells {
+    const uint2* __restrict__ range;
+    __device__ __forceinline__ uint2 get(uint32_t h) const { return __ldg(range + h); }
+};
+
+// Contact test and force of one candidate j (the reference's collideSpheres
+// and, with ATTRACT, attractSpheres) added to the cell subtotal fc.
+template <bool TYPED, bool ATTRACT>
+__device__ __forceinline__ void candidate(const KParams& P, uint32_t j, float2 p, float2 v, float w,
+                                          float r, uint32_t mat, float2 pj, float d2,
+                                          const float2* __restrict__ vel,
+                                          const float* __restrict__ omega,
+                                          const float* __restrict__ radius,
+                                          const uint32_t* __restrict__ type, float2& fc,
+                                          float& moment, float& pr) {
+    const float rj = __ldg(radius + j);
+    uint32_t mj = 0;
+    float4 pc = P.pair[0];
+    if (TYPED) {
+        mj = __ldg(type + j);
+        pc = P.pair[mat * P.nmat + mj];
+    }
+    const float cd = r + rj;
+    // d2 > cd^2 (1 + 2e-6) implies sqrtf(d2) >= cd after rounding: no contact
+    if (d2 <= cd * cd * 1.000002f && sqrtf(d2) < cd) {
+        const float2 f = pair_force(p, pj, v, __ldg(vel + j), w, __ldg(omega + j), r, rj, pc,
+                                    P.dt, moment, pr);
+        fc.x += f.x;
+        fc.y += f.y;
+    }
+    if (ATTRACT) {
+        const float2 f = pair_attract(p, pj, r, rj, P.at[mat], P.at[mj], pr);
+        fc.x += f.x;
+        fc.y += f.y;
+    }
+}
+
 // Sum of the forces on particle i from its 3x3 cell neighbourhood,
 // particles_kernel.cuh:459-549 (collideD) with collideCell (:346-385): cells
 // y-outer, x-inner, particles in ascending sorted index, each cell's
-// subtotal added to the running force.  Wrapping makes a 1- or 2-wide grid
-// visit the same cell more than once, exactly as the reference does.
+// subtotal added to the running force.  `g` is the particle's grid position
+// (calcGridPos, or the wrapped cell of its sort key: the same neighbour
+// cells).  Wrapping makes a 1- or 2-wide grid visit the same cell more than
+// once, exactly as the reference does.
 //
 // Work the reference spends on pairs that are not in contact is skipped
 // without changing any result, because such a pair adds nothing (its force
-// is +0 and it touches neither moment nor pressure):
+// is +0 -- and a running sum that starts at +0 can never be -0 -- and it
+// touches neither moment nor pressure):
 //  * a candidate is dropped before the square root when its squared distance
 //    exceeds (rA + rB)^2 by a relative 2e-6; then sqrtf(d2) >= rA + rB after
 //    rounding, which is the reference's no-contact branch;
@@ -75,27 +127,25 @@ reorder_kernel(uint32_t* __restrict__ cellStart, uint32_t* __restrict__ cellEnd,
 //    farther than rA + rmax (plus a rounding margin) from that side of its
 //    own cell, and candidates are first tested against rA + rmax so that
 //    the neighbour's radius is loaded only for near pairs.  Culling needs at
-//    least 3 cells per axis (then the three columns/rows are distinct cells)
-//    and a particle inside the box.
-template <bool TYPED, bool ATTRACT, bool CULL>
-__device__ __forceinline__ void collide_one(const KParams& P, uint32_t i, float2 p, float2 v,
-                                            float w, float r, uint32_t mat,
+//    least 3 cells per axis and cells wider than 2 rmax (then the three
+//    columns/rows are distinct cells and a wrapped neighbour is out of
+//    reach) and a particle inside the box by more than the margin.
+template <bool TYPED, bool ATTRACT, bool CULL, typename Cells>
+__device__ __forceinline__ void collide_one(const KParams& P, uint32_t i, int2 g, float2 p,
+                                            float2 v, float w, float r, uint32_t mat,
                                             const float2* __restrict__ pos,
                                             const float2* __restrict__ vel,
                                             const float* __restrict__ omega,
                                             const float* __restrict__ radius,
-                                            const uint32_t* __restrict__ type,
-                                            const uint32_t* __restrict__ cellStart,
-                                            const uint32_t* __restrict__ cellEnd, float2& force,
-                                            float& moment, float& pr) {
-    const int2 g = grid_pos(P, p);
+                                            const uint32_t* __restrict__ type, Cells cells,
+                                            float2& force, float& moment, float& pr) {
     force = make_float2(0.0f, 0.0f);
     moment = 0.0f;
     pr = 0.0f;
-    const float4 pc0 = P.pair[0];
     int y0 = -1, y1 = 1, x0 = -1, x1 = 1;
     float reach2 = INFINITY;
-    if (CULL && p.x >= 0.0f && p.x < P.Lx && p.y >= 0.0f && p.y < P.Ly) {
+    if (CULL && p.x > P.cullMargin && p.x < P.Lx - P.cullMargin && p.y > P.cullMargin &&
+        p.y < P.Ly - P.cullMargin) {
         const float reach = (r + P.rmax) * 1.0001f + P.cullMargin;
         const float X0 = (float)g.x * P.cellW, Y0 = (float)g.y * P.cellH;
         if (p.x - X0 > reach) x0 = 0;
@@ -109,38 +159,35 @@ __device__ __forceinline__ void collide_one(const KParams& P, uint32_t i, float2
     for (int dy = y0; dy <= y1; ++dy) {
 #pragma unroll 1
         for (int dx = x0; dx <= x1; ++dx) {
-            const uint32_t h = grid_hash(P, g.x + dx, g.y + dy);
-            const uint32_t start = __ldg(cellStart + h);
+            const uint2 se = cells.get(grid_hash(P, g.x + dx, g.y + dy));
             float2 fc = make_float2(0.0f, 0.0f);
-            if (start != kEmptyCell) {
-                const uint32_t end = __ldg(cellEnd + h);
+            // empty cells have start >= end (start 0xFFFFFFFF): no iterations
+            const uint32_t count = se.y > se.x ? se.y - se.x : 0u;
+            const uint32_t stop = se.x + (count & ~1u);
+            uint32_t j = se.x;
+            // two candidates per iteration: two loads in flight
 #pragma unroll 1
-                for (uint32_t j = start; j < end; ++j) {
-                    if (j == i) continue;
-                    const float2 pj = __ldg(pos + j);
-                    const float relx = pj.x - p.x, rely = pj.y - p.y;
-                    const float d2 = relx * relx + rely * rely;
-                    if (!ATTRACT && CULL && d2 > reach2) continue;
-                    const float rj = __ldg(radius + j);
-                    uint32_t mj = 0;
-                    float4 pc = pc0;
-                    if (TYPED) {
-                        mj = __ldg(type + j);
-                        pc = P.pair[mat * P.nmat + mj];
-                    }
-                    const float cd = r + rj;
-                    if (d2 <= cd * cd * 1.000002f && sqrtf(d2) < cd) {
-                        const float2 f = pair_force(p, pj, v, __ldg(vel + j), w, __ldg(omega + j),
-                                                    r, rj, pc, P.dt, moment, pr);
-                        fc.x += f.x;
-                        fc.y += f.y;
-                    }
-                    if (ATTRACT) {
-                        const float2 f = pair_attract(p, pj, r, rj, P.at[mat], P.at[mj], pr);
-                        fc.x += f.x;
-                        fc.y += f.y;
-                    }
-                }
+            for (; j < stop; j += 2) {
+                const float2 pa = __ldg(pos + j);
+                const float2 pb = __ldg(pos + j + 1);
+                const float ax = pa.x - p.x, ay = pa.y - p.y;
+                const float bx = pb.x - p.x, by = pb.y - p.y;
+                const float da = ax * ax + ay * ay;
+                const float db = bx * bx + by * by;
+                if (j != i && (ATTRACT || !CULL || da <= reach2))
+                    candidate<TYPED, ATTRACT>(P, j, p, v, w, r, mat, pa, da, vel, omega, radius,
+                                              type, fc, moment, pr);
+                if (j + 1 != i && (ATTRACT || !CULL || db <= reach2))
+                    candidate<TYPED, ATTRACT>(P, j + 1, p, v, w, r, mat, pb, db, vel, omega,
+                                              radius, type, fc, moment, pr);
+            }
+            if ((count & 1u) && j != i) {
+                const float2 pa = __ldg(pos + j);
+                const float ax = pa.x - p.x, ay = pa.y - p.y;
+                const float da = ax * ax + ay * ay;
+                if (ATTRACT || !CULL || da <= reach2)
+                    candidate<TYPED, ATTRACT>(P, j, p, v, w, r, mat, pa, da, vel, omega, radius,
+                                              type, fc, moment, pr);
             }
             force.x += fc.x;
             force.y += fc.y;
@@ -165,8 +212,9 @@ collide_kernel(KParams P, const float2* __restrict__ pos, const float2* __restri
     const uint32_t mat = TYPED ? type[i] : 0u;
     float2 f;
     float moment, pr;
-    collide_one<TYPED, ATTRACT, false>(P, i, p, v, w, r, mat, pos, vel, omega, radius, type,
-                                       cellStart, cellEnd, f, moment, pr);
+    collide_one<TYPED, ATTRACT, false>(P, i, grid_pos(P, p), p, v, w, r, mat, pos, vel, omega,
+                                       radius, type, SplitCells{cellStart, cellEnd}, f, moment,
+                                       pr);
     const float m = mass[i];
     acc[i] = make_float2(f.x / m, f.y / m);
     alpha[i] = moment / inertia_of(m, r);
@@ -202,10 +250,10 @@ integrate_kernel(KParams P, float2* __restrict__ pos, float2* __restrict__ vel,
 // the arithmetic is the same expressions in the same order.
 template <bool TYPED, bool ATTRACT, bool CULL>
 __global__ void __launch_bounds__(kCollideThreads)
-step_kernel(KParams P, DynSet in, StatSet inS, const uint32_t* __restrict__ cellStart,
-            const uint32_t* __restrict__ cellEnd, DynSet out, uint32_t* __restrict__ nextHash,
+step_kernel(KParams P, DynSet in, StatSet inS, const uint32_t* __restrict__ sortedKey,
+            const uint2* __restrict__ cellRange, DynSet out, uint32_t* __restrict__ nextHash,
             float* __restrict__ pressure, float2* __restrict__ acc, float* __restrict__ alpha,
-            uint32_t* __restrict__ errFlag, uint32_t n) {
+            uint32_t* __restrict__ errFlag, uint32_t n, uint32_t log2gx) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     Dyn s;
@@ -214,10 +262,14 @@ step_kernel(KParams P, DynSet in, StatSet inS, const uint32_t* __restrict__ cell
     s.w = in.omega[i];
     const float r = inS.radius[i];
     const uint32_t mat = TYPED ? inS.type[i] : 0u;
+    // the sort key of particle i is calcGridPos of this very position, wrapped
+    const uint32_t key = sortedKey[i];
+    const int2 g = make_int2((int)(key & (P.gx - 1u)), (int)(key >> log2gx));
     float2 f;
     float moment, pr;
-    collide_one<TYPED, ATTRACT, CULL>(P, i, s.p, s.v, s.w, r, mat, in.pos, in.vel, in.omega,
-                                      inS.radius, inS.type, cellStart, cellEnd, f, moment, pr);
+    collide_one<TYPED, ATTRACT, CULL>(P, i, g, s.p, s.v, s.w, r, mat, in.pos, in.vel, in.omega,
+                                      inS.radius, inS.type, PackedCells{cellRange}, f, moment,
+                                      pr);
     const float m = inS.mass[i];
     const float2 a = make_float2(f.x / m, f.y / m);
     const float al = moment / inertia_of(m, r);
@@ -230,9 +282,50 @@ step_kernel(KParams P, DynSet in, StatSet inS, const uint32_t* __restrict__ cell
     out.theta[i] = s.th;
     out.omega[i] = s.w;
     if (pressure) pressure[i] = pr;
-    const int2 g = grid_pos(P, s.p);
-    nextHash[i] = grid_hash(P, g.x, g.y);
+    const int2 gn = grid_pos(P, s.p);
+    nextHash[i] = grid_hash(P, gn.x, gn.y);
     if (!(isfinite(s.p.x) && isfinite(s.p.y))) atomicOr(errFlag, 1u);
+}
+
+// Reorder for the context step: as reorder_kernel, but the cell ranges are
+// written as interleaved (start, end) pairs (empty cells hold 0xFFFFFFFF).
+template <bool TYPED>
+__global__ void __launch_bounds__(kThreads)
+reorder_packed_kernel(uint2* __restrict__ cellRange, DynSet s, StatSet sS,
+                      uint32_t* __restrict__ sLoc, const uint32_t* __restrict__ hash,
+                      const uint32_t* __restrict__ index, DynSet o, StatSet oS, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < n;
+    const uint32_t h = valid ? hash[i] : 0u;
+    uint32_t hp = __shfl_up_sync(0xffffffffu, h, 1);
+    if ((threadIdx.x & 31) == 0 && valid && i > 0) hp = hash[i - 1];
+    if (!valid) return;
+    if (i == 0 || h != hp) {
+        cellRange[h].x = i;
+        if (i > 0) cellRange[hp].y = i;
+    }
+    if (i == n - 1) cellRange[h].y = i + 1;
+    const uint32_t src = index[i];
+    s.pos[i] = o.pos[src];
+    s.vel[i] = o.vel[src];
+    s.theta[i] = o.theta[src];
+    s.omega[i] = o.omega[src];
+    sS.radius[i] = oS.radius[src];
+    sS.mass[i] = oS.mass[src];
+    const uint32_t id = oS.id[src];
+    sS.id[i] = id;
+    sLoc[id] = i;
+    if (TYPED) sS.type[i] = oS.type[src];
+}
+
+__global__ void unpack_cells_kernel(const uint2* __restrict__ range, uint32_t numCells,
+                                    uint32_t* __restrict__ cellStart,
+                                    uint32_t* __restrict__ cellEnd) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= numCells) return;
+    const uint2 v = range[c];
+    if (cellStart) cellStart[c] = v.x;
+    if (cellEnd) cellEnd[c] = v.y;
 }
 
 // One row of the reference's followed-particle output per id
@@ -359,22 +452,24 @@ cudaError_t launch_integrate(const KParams& P, float2* pos, float2* vel, const f
     return cudaGetLastError();
 }
 
-cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t* cellStart,
-                        const uint32_t* cellEnd, DynSet out, uint32_t* nextHash, float* pressure,
+cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t* sortedKey,
+                        const uint2* cellRange, DynSet out, uint32_t* nextHash, float* pressure,
                         float2* acc, float* alpha, uint32_t* errFlag, uint32_t n,
                         cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     const bool typed = inS.type != nullptr && P.nmat > 1;
     const bool attract = has_attraction(P);
     const unsigned b = blocks_for(n, kCollideThreads);
-#define DEM_STEP(T, A, C)                                                                   \
-    step_kernel<T, A, C><<<b, kCollideThreads, 0, st>>>(P, in, inS, cellStart, cellEnd, out,  \
-                                                        nextHash, pressure, acc, alpha,       \
-                                                        errFlag, n)
+    uint32_t log2gx = 0;
+    while ((1u << log2gx) < P.gx) ++log2gx;
     // culling also needs cells wider than any contact distance, so that a
     // wrapped neighbour column/row is never within reach
     const bool cull = isfinite(P.rmax) && P.gx >= 3 && P.gy >= 3 &&
                       P.cellW > 2.002f * P.rmax && P.cellH > 2.002f * P.rmax;
+#define DEM_STEP(T, A, C)                                                                 \
+    step_kernel<T, A, C><<<b, kCollideThreads, 0, st>>>(P, in, inS, sortedKey, cellRange, out, \
+                                                        nextHash, pressure, acc, alpha,     \
+                                                        errFlag, n, log2gx)
     if (typed) {
         if (attract) DEM_STEP(true, true, false);
         else if (cull) DEM_STEP(true, false, true);
@@ -385,6 +480,30 @@ cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t
         else DEM_STEP(false, false, false);
     }
 #undef DEM_STEP
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reorder_packed(uint2* cellRange, DynSet sorted, StatSet sortedS,
+                                  uint32_t* sortedLoc, const uint32_t* hash, const uint32_t* index,
+                                  DynSet old, StatSet oldS, uint32_t n, uint32_t numCells,
+                                  cudaStream_t st, int* launches) {
+    cudaError_t e = cudaMemsetAsync(cellRange, 0xff, sizeof(uint2) * (size_t)numCells, st);
+    if (e != cudaSuccess || n == 0) return e;
+    if (sortedS.type && oldS.type)
+        reorder_packed_kernel<true><<<blocks_for(n, kThreads), kThreads, 0, st>>>(
+            cellRange, sorted, sortedS, sortedLoc, hash, index, old, oldS, n);
+    else
+        reorder_packed_kernel<false><<<blocks_for(n, kThreads), kThreads, 0, st>>>(
+            cellRange, sorted, sortedS, sortedLoc, hash, index, old, oldS, n);
+    if (launches) ++*launches;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack_cells(const uint2* cellRange, uint32_t numCells, uint32_t* cellStart,
+                                uint32_t* cellEnd, cudaStream_t st) {
+    if (numCells == 0) return cudaSuccess;
+    unpack_cells_kernel<<<blocks_for(numCells, kThreads), kThreads, 0, st>>>(cellRange, numCells,
+                                                                             cellStart, cellEnd);
     return cudaGetLastError();
 }
 

@@ -54,12 +54,23 @@ cudaError_t launch_integrate(const KParams& P, float2* pos, float2* vel, const f
                              const float* radius, const float* mass, float* pressure, uint32_t n,
                              cudaStream_t st);
 
-// Fused collide + integrate + next-step hash: reads the sorted set `in`,
-// writes the integrated state to `out` (same order) and the cell key of each
-// new position to `nextHash`.  acc/alpha/pressure may be null.
-cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t* cellStart,
-                        const uint32_t* cellEnd, DynSet out, uint32_t* nextHash, float* pressure,
+// Fused collide + integrate + next-step hash: reads the sorted set `in`
+// (with its sort keys and interleaved cell ranges), writes the integrated
+// state to `out` (same order) and the cell key of each new position to
+// `nextHash`.  acc/alpha/pressure may be null.
+cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t* sortedKey,
+                        const uint2* cellRange, DynSet out, uint32_t* nextHash, float* pressure,
                         float2* acc, float* alpha, uint32_t* errFlag, uint32_t n,
                         cudaStream_t st);
+
+// Reorder with interleaved (start, end) cell ranges; resets the ranges first.
+cudaError_t launch_reorder_packed(uint2* cellRange, DynSet sorted, StatSet sortedS,
+                                  uint32_t* sortedLoc, const uint32_t* hash, const uint32_t* index,
+                                  DynSet old, StatSet oldS, uint32_t n, uint32_t numCells,
+                                  cudaStream_t st, int* launches);
+
+// Splits interleaved ranges into the reference's cellStart/cellEnd arrays.
+cudaError_t launch_unpack_cells(const uint2* cellRange, uint32_t numCells, uint32_t* cellStart,
+                                uint32_t* cellEnd, cudaStream_t st);
 
 }  // namespace dem

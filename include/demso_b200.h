@@ -176,8 +176,9 @@ int dem_get_state(DemContext* ctx, float* pos, float* vel, float* theta, float* 
 /* Advances `nsteps` full steps (hash, sort, reorder, collide, integrate). */
 int dem_step(DemContext* ctx, uint32_t nsteps, void* stream);
 
-/* Cell arrays of the last step's reorder (device pointers owned by ctx). */
-int dem_get_cells(DemContext* ctx, const uint32_t** cellStart, const uint32_t** cellEnd);
+/* Cell ranges of the last step's reorder, written to caller device buffers
+ * of numCells words each in the reference's layout (either may be NULL). */
+int dem_get_cells(DemContext* ctx, uint32_t* cellStart, uint32_t* cellEnd, void* stream);
 
 /* Reads the device error flag (synchronises `stream`): DEM_OK or DEM_ERR_OOB. */
 int dem_check(DemContext* ctx, void* stream);
