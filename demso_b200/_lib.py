@@ -50,6 +50,7 @@ SIGNATURES = [
     ("dem_calc_hash", C.c_int, [_SYS, _P, _P, _P, _U, _P]),
     ("dem_sort_scratch_bytes", C.c_size_t, [_U, _U]),
     ("dem_sort_particles", C.c_int, [_P, _P, _U, _U, _P, C.c_size_t, _P]),
+    ("dem_sort_particles_static", C.c_int, [_P, _P, _U, _U, _P]),
     ("dem_reorder_data_and_find_cell_start", C.c_int,
      [_SYS, _P, _P] + [_P] * 9 + [_P, _P] + [_P] * 8 + [_U, _U, _P]),
     ("dem_collide", C.c_int, [_SYS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _U, _U, _P, _P]),

@@ -107,6 +107,9 @@ bool misaligned(const T* p, size_t a) { return ((uintptr_t)p % a) != 0; }
 
 }  // namespace
 
+// Error recording for entry points defined in other translation units.
+int dem_record_error(int code, const char* msg) { return fail(code, "%s", msg); }
+
 // ---------------------------------------------------------------------------
 // library
 // ---------------------------------------------------------------------------

@@ -109,6 +109,21 @@ int dem_sort_particles(uint32_t* gridParticleHash, uint32_t* gridParticleIndex,
                        uint32_t numParticles, uint32_t keyBits, void* scratch,
                        size_t scratchBytes, void* stream);
 
+/* No counterpart in the reference: dem_sort_particles for callers that
+ * cannot allocate device memory -- code running while its stream is being
+ * captured into a CUDA graph, loops that must not stall on the device-wide
+ * synchronisation an allocation can cause, and host programs whose memory
+ * manager owns all device memory.  Same stable in-place sort and result as
+ * dem_sort_particles, but the scratch is a fixed array inside the library
+ * (about 2.6 MB, held on every GPU that loads the library until exit), so at
+ * most 262,144 pairs per call; larger calls fail with DEM_ERR_CAPACITY.
+ * Allocates nothing.  The first call on a device looks up that array's
+ * device address; make that first call before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU race and must be ordered on
+ * one stream or synchronised. */
+int dem_sort_particles_static(uint32_t* gridParticleHash, uint32_t* gridParticleIndex,
+                              uint32_t numParticles, uint32_t keyBits, void* stream);
+
 /* Replaces reorderDataAndFindCellStart (functions.cu:347-393 ->
  * reorderDataAndFindCellStartD, particles_kernel.cuh:156-233): marks every
  * cell empty, records [cellStart, cellEnd) of each occupied cell, gathers the
