@@ -297,19 +297,18 @@ def main():
     value = n * world * args.steps / (elapsed * 1e-3)
 
     stage_ms = [ms[i] / max(1, nprof.value) for i in range(3)]
-    stage_names = ["sort", "reorder", "collide_integrate"]
-    dom = int(np.argmax(stage_ms))
+    stage_names = ["sort_reorder", "reorder_separate", "collide_integrate"]
+    dom = 2 if stage_ms[2] >= stage_ms[0] else 0
     hbm, kind = peaks()
     cells = sc.sys.num_cells
     if dom == 2:
         bytes_launch = STEP_KERNEL_BYTES_PER_PARTICLE * n + STEP_KERNEL_BYTES_PER_CELL * cells
         kname = "step_kernel (collide + integrate + next hash)"
-    elif dom == 1:
-        bytes_launch = 84 * n + 12 * cells
-        kname = "reorder_kernel (+ cell reset)"
     else:
-        bytes_launch = 36 * n
-        kname = "radix sort (2 passes)"
+        # counted as the reorder alone (gather 36 B, write 36 B, key+index 8 B,
+        # loc 4 B per particle, 12 B per cell); the sort work is not counted
+        bytes_launch = 84 * n + 12 * cells
+        kname = "sort phase (incremental sort + state reorder)"
     achieved = bytes_launch / (stage_ms[dom] * 1e-3) / 1e9
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.txt")
@@ -375,7 +374,8 @@ def main():
                              "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                              "peak_kind": kind, "traffic": traffic,
                              "bytes_per_launch": bytes_launch},
-                "stage_ms_per_step": dict(zip(stage_names, stage_ms)),
+                "stage_ms_per_step": {"sort_reorder": stage_ms[0],
+                                      "collide_integrate": stage_ms[2]},
                 "whole_step": {"model_bytes_per_step": whole_bytes,
                                "achieved_gbs": whole_bytes / (step_ms * 1e-3) / 1e9,
                                "frac": whole_bytes / (step_ms * 1e-3) / 1e9 / hbm},

@@ -9,6 +9,7 @@
 #include <string>
 
 #include "dem_common.cuh"
+#include "dem_incsort.cuh"
 #include "dem_kernels.cuh"
 #include "dem_sort.cuh"
 
@@ -260,33 +261,38 @@ struct DemContext {
     bool typed = false;
     // dynamic fields: dyn[0] holds the integrated state, dyn[1] the sorted copy
     DynSet dyn[2];
-    // static fields ping-pong between the two sets on every reorder
+    // static fields ping-pong between the two sets on every sort
     StatSet stat[2];
     int cur = 0;               // static set holding the current state
     uint32_t* loc = nullptr;   // indexed by id
     uint32_t* keys = nullptr;  // cell of each particle of the current state
-    uint32_t* perm = nullptr;  // sort values (source index of each sorted slot)
-    uint2* cellRange = nullptr;  // interleaved (cellStart, cellEnd) per cell
+    uint32_t* perm = nullptr;  // radix sort values (full path)
+    uint32_t* skey[2] = {};    // sorted keys of the order made when stat[p] was filled
+    uint2* cells[2] = {};      // interleaved (cellStart, cellEnd) of that order
     float* pressure = nullptr;
     float2* acc = nullptr;
     float* alpha = nullptr;
     uint32_t* errFlag = nullptr;
     void* sortScratch = nullptr;
     OnesweepScratch ss;
-    bool keysValid = false;
+    void* incScratch = nullptr;
+    IncSort inc;
+    bool keysValid = false;  // keys[] holds the cell of every particle of the current state
+    bool haveOrder = false;  // the last step recorded its movers: incremental sort possible
     float rmax = INFINITY;   // largest radius of the current state (culling bound)
-    cudaStream_t capStream = nullptr;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaStream_t capStream = nullptr, bodyStream = nullptr;
+    // Each step is two graph launches: the sort phase sortGraph[kind][parity]
+    // (kind 0 = full radix sort, 1 = incremental sort with the full sort as a
+    // device-chosen fallback), then the step kernel stepGraph[parity].
+    cudaGraphExec_t sortGraph[2][2] = {};
+    cudaGraphExec_t stepGraph[2] = {};
     int launchesPerStep = 0;
     void* block = nullptr;  // one allocation for every per-particle/per-cell array
     // followed-particle staging (device), see dem_get_followed
     float* followRows = nullptr;
-    // stage profiling: graphs with event-record nodes at the stage boundaries
+    // stage profiling: events recorded on the caller's stream around the two
+    // launches of each step (3 per step)
     bool profiling = false;
-    cudaEvent_t marker[DEM_NUM_STAGES + 1] = {};
-    cudaGraphExec_t pgraph[2] = {nullptr, nullptr};
-    cudaGraph_t pgraphSrc[2] = {nullptr, nullptr};  // kept: its nodes address the exec's nodes
-    cudaGraphNode_t pnode[2][DEM_NUM_STAGES + 1] = {};
     cudaEvent_t* evPool = nullptr;
     uint32_t evCap = 0, evUsed = 0, stepsProfiled = 0;
 };
@@ -294,62 +300,124 @@ struct DemContext {
 namespace {
 
 void drop_graphs(DemContext* c) {
-    for (auto& g : c->graph)
-        if (g) {
-            cudaGraphExecDestroy(g);
-            g = nullptr;
+    for (int k = 0; k < 2; ++k)
+        for (int p = 0; p < 2; ++p) {
+            if (c->sortGraph[k][p]) cudaGraphExecDestroy(c->sortGraph[k][p]);
+            c->sortGraph[k][p] = nullptr;
         }
-    for (auto& g : c->pgraph)
-        if (g) {
-            cudaGraphExecDestroy(g);
-            g = nullptr;
-        }
-    for (auto& g : c->pgraphSrc)
-        if (g) {
-            cudaGraphDestroy(g);
-            g = nullptr;
-        }
+    for (int p = 0; p < 2; ++p) {
+        if (c->stepGraph[p]) cudaGraphExecDestroy(c->stepGraph[p]);
+        c->stepGraph[p] = nullptr;
+    }
 }
 
-// One step from (dyn[0], stat[cur]) into (dyn[0], stat[cur^1]).  With
-// `markers`, an event is recorded before the sort, between the stages and
-// after the last kernel (captured as event-record nodes).
-cudaError_t enqueue_step(DemContext* c, cudaStream_t st, int* launches,
-                         const cudaEvent_t* markers) {
-    const int a = c->cur, b = c->cur ^ 1;
-    cudaError_t e;
-    if (markers && (e = cudaEventRecordWithFlags(markers[0], st, cudaEventRecordExternal)) != cudaSuccess)
-        return e;
-    uint32_t *ko, *vo;
-    e = onesweep_sort_pairs(c->keys, c->perm, c->n, c->keyBits, true, c->ss, c->errFlag, st, &ko,
-                            &vo, launches);
+MoverSinkArgs sink_of(DemContext* c) {
+    MoverSinkArgs m;
+    m.leavers = c->inc.leavers;
+    m.arrCnt = c->inc.arrCnt;
+    m.arrLo = c->inc.arrLo;
+    m.movers = c->inc.movers;
+    m.ctrl = c->inc.ctrl;
+    m.moverCap = c->inc.moverCap;
+    return m;
+}
+
+// Full sort of the current state (parity a) into the other static set.
+cudaError_t enqueue_full_sort(DemContext* c, int a, cudaStream_t st, int* launches) {
+    const int b = a ^ 1;
+    return enqueue_full(c->inc, c->n, c->keyBits, c->keys, c->perm, c->ss, c->errFlag, c->skey[b],
+                        c->cells[b], c->dyn[0], c->stat[a], c->dyn[1], c->stat[b], c->loc, st,
+                        launches);
+}
+
+cudaError_t enqueue_inc_sort(DemContext* c, int a, cudaStream_t st, int* launches) {
+    const int b = a ^ 1;
+    return enqueue_incremental(c->inc, c->n, c->keys, c->skey[a], c->cells[a], c->skey[b],
+                               c->cells[b], c->dyn[0], c->stat[a], c->dyn[1], c->stat[b], c->loc,
+                               st, launches);
+}
+
+// Adds an IF node on `h` at the current capture point of `st` and captures
+// `body` into it on c->bodyStream.
+template <typename Body>
+cudaError_t add_if(DemContext* c, cudaStream_t st, cudaGraphConditionalHandle h, Body body) {
+    cudaStreamCaptureStatus status;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(st, &status, nullptr, &g, &deps, &nd);
     if (e != cudaSuccess) return e;
-    if (markers && (e = cudaEventRecordWithFlags(markers[1], st, cudaEventRecordExternal)) != cudaSuccess)
-        return e;
-    e = launch_reorder_packed(c->cellRange, c->dyn[1], c->stat[b], c->loc, ko, vo, c->dyn[0],
-                              c->stat[a], c->n, c->numCells, st, launches);
+    cudaGraphNodeParams prm = {};
+    prm.type = cudaGraphNodeTypeConditional;
+    prm.conditional.handle = h;
+    prm.conditional.type = cudaGraphCondTypeIf;
+    prm.conditional.size = 1;
+    cudaGraphNode_t node;
+    e = cudaGraphAddNode(&node, g, deps, nd, &prm);
     if (e != cudaSuccess) return e;
-    if (markers && (e = cudaEventRecordWithFlags(markers[2], st, cudaEventRecordExternal)) != cudaSuccess)
-        return e;
-    e = launch_step(c->P, c->dyn[1], c->stat[b], ko, c->cellRange, c->dyn[0], c->keys,
-                    (c->flags & DEM_CTX_PRESSURE) ? c->pressure : nullptr,
-                    (c->flags & DEM_CTX_ACCEL) ? c->acc : nullptr,
-                    (c->flags & DEM_CTX_ACCEL) ? c->alpha : nullptr, c->errFlag, c->n, st);
+    e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
+    if (e != cudaSuccess) return e;
+    cudaGraph_t bodyGraph = prm.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(c->bodyStream, bodyGraph, nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    cudaError_t eb = body(c->bodyStream);
+    e = cudaStreamEndCapture(c->bodyStream, &bodyGraph);
+    return eb != cudaSuccess ? eb : e;
+}
+
+// Sort phase of one step: the state (dyn[0], stat[cur]) is sorted into
+// (dyn[1], stat[cur^1]) with its cell ranges.  kind 0: full radix sort;
+// kind 1: incremental sort, or the full sort when the last step's movers did
+// not fit (chosen on the device by conditional nodes).
+cudaError_t enqueue_sort_phase(DemContext* c, int kind, cudaStream_t st, int* launches) {
+    const int a = c->cur;
+    if (kind == 0) return enqueue_full_sort(c, a, st, launches);
+    cudaStreamCaptureStatus status;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamGetCaptureInfo(st, &status, nullptr, &g, nullptr, nullptr);
+    if (e != cudaSuccess) return e;
+    if (status != cudaStreamCaptureStatusActive) return cudaErrorStreamCaptureUnsupported;
+    cudaGraphConditionalHandle hFast, hFull;
+    e = cudaGraphConditionalHandleCreate(&hFast, g, 0, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hFull, g, 0, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) e = enqueue_choose_path(c->inc, hFast, hFull, st);
     if (launches) ++*launches;
-    if (e != cudaSuccess) return e;
-    if (markers && (e = cudaEventRecordWithFlags(markers[3], st, cudaEventRecordExternal)) != cudaSuccess)
-        return e;
-    return cudaSuccess;
+    int fastLaunches = 0, fullLaunches = 0;
+    if (e == cudaSuccess)
+        e = add_if(c, st, hFast, [&](cudaStream_t bs) {
+            return enqueue_inc_sort(c, a, bs, &fastLaunches);
+        });
+    if (e == cudaSuccess)
+        e = add_if(c, st, hFull, [&](cudaStream_t bs) {
+            return enqueue_full_sort(c, a, bs, &fullLaunches);
+        });
+    if (launches) *launches += fastLaunches;  // the usual path
+    return e;
 }
 
-int build_graph(DemContext* c, int parity, bool profiled) {
+// Collide + integrate + next hash over the sorted set made by the sort phase.
+cudaError_t enqueue_step_kernel(DemContext* c, cudaStream_t st, int* launches) {
+    const int b = c->cur ^ 1;
+    cudaError_t e = launch_step(c->P, c->dyn[1], c->stat[b], c->skey[b], c->cells[b], c->dyn[0],
+                                c->keys, (c->flags & DEM_CTX_PRESSURE) ? c->pressure : nullptr,
+                                (c->flags & DEM_CTX_ACCEL) ? c->acc : nullptr,
+                                (c->flags & DEM_CTX_ACCEL) ? c->alpha : nullptr, c->errFlag, c->n,
+                                sink_of(c), st);
+    if (launches) ++*launches;
+    return e;
+}
+
+// what: 0/1 = sort phase of that kind, 2 = step kernel.
+int build_graph(DemContext* c, int what, int parity) {
     cudaGraph_t g = nullptr;
     const int saved = c->cur;
     c->cur = parity;
     DEM_TRY_CUDA(cudaStreamBeginCapture(c->capStream, cudaStreamCaptureModeThreadLocal),
                  "begin capture");
     int launches = 0;
-    cudaError_t e = enqueue_step(c, c->capStream, &launches, profiled ? c->marker : nullptr);
+    cudaError_t e = what < 2 ? enqueue_sort_phase(c, what, c->capStream, &launches)
+                             : enqueue_step_kernel(c, c->capStream, &launches);
     cudaError_t e2 = cudaStreamEndCapture(c->capStream, &g);
     c->cur = saved;
     if (e != cudaSuccess) {
@@ -357,55 +425,20 @@ int build_graph(DemContext* c, int parity, bool profiled) {
         return cuda_fail(e, "step capture");
     }
     if (e2 != cudaSuccess) return cuda_fail(e2, "end capture");
-    if (profiled) {
-        // find the event-record nodes by the marker they record
-        size_t nn = 0;
-        cudaGraphGetNodes(g, nullptr, &nn);
-        cudaGraphNode_t* nodes = new cudaGraphNode_t[nn ? nn : 1];
-        cudaGraphGetNodes(g, nodes, &nn);
-        for (size_t i = 0; i < nn; ++i) {
-            cudaGraphNodeType t;
-            cudaGraphNodeGetType(nodes[i], &t);
-            if (t != cudaGraphNodeTypeEventRecord) continue;
-            cudaEvent_t ev;
-            cudaGraphEventRecordNodeGetEvent(nodes[i], &ev);
-            for (int k = 0; k <= DEM_NUM_STAGES; ++k)
-                if (ev == c->marker[k]) c->pnode[parity][k] = nodes[i];
-        }
-        delete[] nodes;
-    }
-    cudaGraphExec_t* slot = profiled ? &c->pgraph[parity] : &c->graph[parity];
+    cudaGraphExec_t* slot = what < 2 ? &c->sortGraph[what][parity] : &c->stepGraph[parity];
     e = cudaGraphInstantiate(slot, g, 0);
-    if (profiled && e == cudaSuccess)
-        c->pgraphSrc[parity] = g;  // node handles stay valid while the graph lives
-    else
-        cudaGraphDestroy(g);
+    cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(e, "graph instantiate");
-    c->launchesPerStep = launches;
+    if (what == 1) c->launchesPerStep = launches + 1;  // + the step kernel
     return DEM_OK;
 }
 
 void drop_profile(DemContext* c) {
-    for (auto& g : c->pgraph)
-        if (g) {
-            cudaGraphExecDestroy(g);
-            g = nullptr;
-        }
-    for (auto& g : c->pgraphSrc)
-        if (g) {
-            cudaGraphDestroy(g);
-            g = nullptr;
-        }
     if (c->evPool) {
         for (uint32_t i = 0; i < c->evCap; ++i) cudaEventDestroy(c->evPool[i]);
         delete[] c->evPool;
         c->evPool = nullptr;
     }
-    for (auto& m : c->marker)
-        if (m) {
-            cudaEventDestroy(m);
-            m = nullptr;
-        }
     c->evCap = c->evUsed = 0;
     c->profiling = false;
 }
@@ -421,6 +454,7 @@ extern "C" int dem_create(const DemSystem* sys, uint32_t capacity, uint32_t flag
     int rc = validate(sys);
     if (rc) return rc;
     if (capacity == 0) return fail(DEM_ERR_INVALID_ARG, "capacity must be > 0");
+    if (capacity >= (1u << 30)) return fail(DEM_ERR_INVALID_ARG, "capacity must be < 2^30");
     DemContext* c = new (std::nothrow) DemContext();
     if (!c) return fail(DEM_ERR_NO_MEMORY, "host allocation failed");
     c->sys = *sys;
@@ -432,25 +466,26 @@ extern "C" int dem_create(const DemSystem* sys, uint32_t capacity, uint32_t flag
     c->P = make_kparams(sys, 0);
     cudaGetDevice(&c->device);
 
-    const size_t N = capacity, f4 = al256(4 * N), f8 = al256(8 * N), cells = al256(4 * (size_t)c->numCells);
+    const size_t N = capacity, f4 = al256(4 * N), f8 = al256(8 * N),
+                 cells8 = al256(8 * (size_t)c->numCells);
     size_t total = 0;
-    total += 2 * (2 * f8 + 2 * f4);             // dyn sets
-    total += 2 * (3 * f4 + (c->typed ? f4 : 0)); // static sets
-    total += 3 * f4;                            // loc, keys, perm
-    total += 2 * cells;                         // interleaved cell ranges
-    total += f4 + f8 + f4;                      // pressure, acc, alpha
-    total += 256;                               // error flag
+    total += 2 * (2 * f8 + 2 * f4);              // dyn sets
+    total += 2 * (3 * f4 + (c->typed ? f4 : 0));  // static sets
+    total += 3 * f4 + 2 * f4;                    // loc, keys, perm, sorted keys x2
+    total += 2 * cells8;                         // cell ranges x2
+    total += f4 + f8 + f4;                       // pressure, acc, alpha
+    total += 256;                                // error flag
     const size_t sortBytes = onesweep_scratch_bytes(capacity, c->keyBits);
+    const size_t incBytes = incsort_bytes(capacity, c->numCells, nullptr);
     cudaError_t e = cudaMalloc(&c->block, total);
+    if (e == cudaSuccess) e = cudaMalloc(&c->sortScratch, sortBytes);
+    if (e == cudaSuccess) e = cudaMalloc(&c->incScratch, incBytes);
     if (e != cudaSuccess) {
-        delete c;
-        return cuda_fail(e, "cudaMalloc state");
-    }
-    e = cudaMalloc(&c->sortScratch, sortBytes);
-    if (e != cudaSuccess) {
+        cudaFree(c->incScratch);
+        cudaFree(c->sortScratch);
         cudaFree(c->block);
         delete c;
-        return cuda_fail(e, "cudaMalloc sort scratch");
+        return cuda_fail(e, "cudaMalloc context");
     }
     char* p = static_cast<char*>(c->block);
     auto take = [&p](size_t b) { char* q = p; p += b; return q; };
@@ -467,16 +502,25 @@ extern "C" int dem_create(const DemSystem* sys, uint32_t capacity, uint32_t flag
     c->loc = reinterpret_cast<uint32_t*>(take(f4));
     c->keys = reinterpret_cast<uint32_t*>(take(f4));
     c->perm = reinterpret_cast<uint32_t*>(take(f4));
-    c->cellRange = reinterpret_cast<uint2*>(take(2 * cells));
+    for (int s = 0; s < 2; ++s) {
+        c->skey[s] = reinterpret_cast<uint32_t*>(take(f4));
+        c->cells[s] = reinterpret_cast<uint2*>(take(cells8));
+    }
     c->pressure = reinterpret_cast<float*>(take(f4));
     c->acc = reinterpret_cast<float2*>(take(f8));
     c->alpha = reinterpret_cast<float*>(take(f4));
     c->errFlag = reinterpret_cast<uint32_t*>(take(256));
     c->ss = carve_onesweep_scratch(c->sortScratch, capacity, c->keyBits);
+    c->inc = carve_incsort(c->incScratch, capacity, c->numCells);
     e = cudaMemset(c->block, 0, total);
-    if (e == cudaSuccess) e = cudaMemset(c->cellRange, 0xff, 8 * (size_t)c->numCells);
+    if (e == cudaSuccess) e = cudaMemset(c->incScratch, 0, incBytes);
+    for (int s = 0; s < 2 && e == cudaSuccess; ++s)
+        e = cudaMemset(c->cells[s], 0xff, 8 * (size_t)c->numCells);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->capStream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->bodyStream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
+        if (c->capStream) cudaStreamDestroy(c->capStream);
+        cudaFree(c->incScratch);
         cudaFree(c->sortScratch);
         cudaFree(c->block);
         delete c;
@@ -491,7 +535,9 @@ extern "C" int dem_destroy(DemContext* c) {
     drop_graphs(c);
     drop_profile(c);
     if (c->capStream) cudaStreamDestroy(c->capStream);
+    if (c->bodyStream) cudaStreamDestroy(c->bodyStream);
     cudaFree(c->followRows);
+    cudaFree(c->incScratch);
     cudaFree(c->sortScratch);
     cudaFree(c->block);
     delete c;
@@ -510,8 +556,9 @@ extern "C" int dem_set_system(DemContext* c, const DemSystem* sys) {
     c->P = make_kparams(sys, c->n);
     c->P.rmax = c->rmax;
     drop_graphs(c);
-    // keys depend on the box size; recompute before the next step
+    // keys depend on the box size; recompute them and sort from scratch
     c->keysValid = false;
+    c->haveOrder = false;
     return DEM_OK;
 }
 
@@ -551,6 +598,7 @@ extern "C" int dem_set_state(DemContext* c, uint32_t n, const float* pos, const 
     c->P.rmax = c->rmax;
     drop_graphs(c);
     c->keysValid = false;
+    c->haveOrder = false;
     return DEM_OK;
 }
 
@@ -586,31 +634,35 @@ extern "C" int dem_step(DemContext* c, uint32_t nsteps, void* stream) {
     if (!c->keysValid) {
         DEM_TRY_CUDA(launch_calc_hash(c->P, c->dyn[0].pos, c->keys, nullptr, c->n, st), "hash");
         c->keysValid = true;
+        c->haveOrder = false;
     }
     for (int p = 0; p < 2; ++p) {
-        if (!c->graph[p]) {
-            int rc = build_graph(c, p, false);
-            if (rc) return rc;
-        }
-        if (c->profiling && !c->pgraph[p]) {
-            int rc = build_graph(c, p, true);
+        for (int k = 0; k < 2; ++k)
+            if (!c->sortGraph[k][p]) {
+                int rc = build_graph(c, k, p);
+                if (rc) return rc;
+            }
+        if (!c->stepGraph[p]) {
+            int rc = build_graph(c, 2, p);
             if (rc) return rc;
         }
     }
     for (uint32_t s = 0; s < nsteps; ++s) {
         const int p = c->cur;
-        if (c->profiling && c->evUsed + DEM_NUM_STAGES + 1 <= c->evCap) {
-            for (int k = 0; k <= DEM_NUM_STAGES; ++k)
-                DEM_TRY_CUDA(cudaGraphExecEventRecordNodeSetEvent(c->pgraph[p], c->pnode[p][k],
-                                                                  c->evPool[c->evUsed + k]),
-                             "set profile event");
-            c->evUsed += DEM_NUM_STAGES + 1;
+        const int kind = c->haveOrder ? 1 : 0;
+        const bool prof = c->profiling && c->evUsed + 3 <= c->evCap;
+        cudaEvent_t* ev = prof ? c->evPool + c->evUsed : nullptr;
+        if (prof) DEM_TRY_CUDA(cudaEventRecord(ev[0], st), "profile event");
+        DEM_TRY_CUDA(cudaGraphLaunch(c->sortGraph[kind][p], st), "graph launch");
+        if (prof) DEM_TRY_CUDA(cudaEventRecord(ev[1], st), "profile event");
+        DEM_TRY_CUDA(cudaGraphLaunch(c->stepGraph[p], st), "graph launch");
+        if (prof) {
+            DEM_TRY_CUDA(cudaEventRecord(ev[2], st), "profile event");
+            c->evUsed += 3;
             ++c->stepsProfiled;
-            DEM_TRY_CUDA(cudaGraphLaunch(c->pgraph[p], st), "graph launch");
-        } else {
-            DEM_TRY_CUDA(cudaGraphLaunch(c->graph[p], st), "graph launch");
         }
         c->cur ^= 1;
+        c->haveOrder = true;
     }
     return DEM_OK;
 }
@@ -618,7 +670,7 @@ extern "C" int dem_step(DemContext* c, uint32_t nsteps, void* stream) {
 extern "C" int dem_get_cells(DemContext* c, uint32_t* cellStart, uint32_t* cellEnd,
                              void* stream) {
     if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
-    DEM_TRY_CUDA(launch_unpack_cells(c->cellRange, c->numCells, cellStart, cellEnd,
+    DEM_TRY_CUDA(launch_unpack_cells(c->cells[c->cur], c->numCells, cellStart, cellEnd,
                                      (cudaStream_t)stream),
                  "unpack cells");
     return DEM_OK;
@@ -638,8 +690,8 @@ extern "C" int dem_check(DemContext* c, void* stream) {
 
 extern "C" int dem_kernels_per_step(DemContext* c) {
     if (!c) return -1;
-    if (!c->graph[0] && c->n > 0) {
-        if (build_graph(c, 0, false) != DEM_OK) return -1;
+    if (!c->sortGraph[1][0] && c->n > 0) {
+        if (build_graph(c, 1, 0) != DEM_OK) return -1;
     }
     return c->launchesPerStep;
 }
@@ -679,7 +731,7 @@ extern "C" int dem_profile_begin(DemContext* c, uint32_t maxSteps) {
     if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
     if (maxSteps == 0) return fail(DEM_ERR_INVALID_ARG, "maxSteps must be > 0");
     drop_profile(c);
-    const uint32_t cap = maxSteps * (DEM_NUM_STAGES + 1);
+    const uint32_t cap = maxSteps * 3;
     c->evPool = new (std::nothrow) cudaEvent_t[cap];
     if (!c->evPool) return fail(DEM_ERR_NO_MEMORY, "host allocation failed");
     for (uint32_t i = 0; i < cap; ++i) {
@@ -691,7 +743,6 @@ extern "C" int dem_profile_begin(DemContext* c, uint32_t maxSteps) {
         }
     }
     c->evCap = cap;
-    for (auto& m : c->marker) DEM_TRY_CUDA(cudaEventCreate(&m), "cudaEventCreate");
     c->evUsed = 0;
     c->stepsProfiled = 0;
     c->profiling = true;
@@ -704,12 +755,12 @@ extern "C" int dem_profile_end(DemContext* c, float* ms, uint32_t* steps) {
     float acc[DEM_NUM_STAGES] = {0.0f, 0.0f, 0.0f};
     if (c->evUsed) DEM_TRY_CUDA(cudaEventSynchronize(c->evPool[c->evUsed - 1]), "event sync");
     for (uint32_t s = 0; s < c->stepsProfiled; ++s) {
-        cudaEvent_t* e = c->evPool + s * (DEM_NUM_STAGES + 1);
-        for (int k = 0; k < DEM_NUM_STAGES; ++k) {
-            float t = 0.0f;
-            DEM_TRY_CUDA(cudaEventElapsedTime(&t, e[k], e[k + 1]), "event elapsed");
-            acc[k] += t;
-        }
+        cudaEvent_t* e = c->evPool + 3 * s;
+        float t0 = 0.0f, t1 = 0.0f;
+        DEM_TRY_CUDA(cudaEventElapsedTime(&t0, e[0], e[1]), "event elapsed");
+        DEM_TRY_CUDA(cudaEventElapsedTime(&t1, e[1], e[2]), "event elapsed");
+        acc[0] += t0;
+        acc[2] += t1;
     }
     if (ms)
         for (int k = 0; k < DEM_NUM_STAGES; ++k) ms[k] = acc[k];

@@ -17,6 +17,9 @@
 namespace dem {
 
 constexpr uint32_t kEmptyCell = 0xffffffffu;
+// Largest arrival group / leaving cell the incremental sort scans per particle;
+// anything larger sends the next step to the full radix sort.
+constexpr uint32_t kMaxGroup = 64;
 constexpr int kMaxMat = DEM_MAX_MATERIALS;
 
 // Launch-time parameters, passed by value (lives in the kernel-parameter

@@ -1,0 +1,349 @@
+// Incremental stable sort of the context step (see dem_incsort.cuh).
+#include "dem_incsort.cuh"
+
+#include <algorithm>
+
+namespace dem {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kCellItems = 16;
+constexpr uint32_t kCellChunk = kThreads * kCellItems;  // cells per scan block
+constexpr int kTopThreads = 1024;
+constexpr int kTopItems = 8;
+
+inline unsigned blocks_for(size_t n, int t) { return (unsigned)((n + (size_t)t - 1) / (size_t)t); }
+inline size_t al256(size_t b) { return (b + 255u) & ~(size_t)255u; }
+
+__global__ void fill_u32_kernel(uint32_t* __restrict__ p, uint32_t value, size_t count) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+         i += (size_t)gridDim.x * blockDim.x)
+        p[i] = value;
+}
+
+cudaError_t fill_u32(uint32_t* p, uint32_t value, size_t count, cudaStream_t st, int* launches) {
+    if (count == 0) return cudaSuccess;
+    const unsigned b = std::min<unsigned>(blocks_for(count, kThreads), 148u * 8u);
+    fill_u32_kernel<<<b, kThreads, 0, st>>>(p, value, count);
+    if (launches) ++*launches;
+    return cudaGetLastError();
+}
+
+// Inclusive warp scan of 64-bit values.
+__device__ __forceinline__ unsigned long long warp_incl_scan(unsigned long long x) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    return x;
+}
+
+template <int THREADS>
+__device__ __forceinline__ unsigned long long block_excl_scan64(unsigned long long v,
+                                                                unsigned long long* warpTot,
+                                                                unsigned long long& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned long long x = warp_incl_scan(v);
+    if (lane == 31) warpTot[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        unsigned long long t = lane < THREADS / 32 ? warpTot[lane] : 0ull;
+        t = warp_incl_scan(t);
+        if (lane < THREADS / 32) warpTot[lane] = t;
+    }
+    __syncthreads();
+    total = warpTot[THREADS / 32 - 1];
+    return (warp > 0 ? warpTot[warp - 1] : 0ull) + x - v;
+}
+
+// New particle count and arrival count of a cell, packed (count | arrivals << 32).
+__device__ __forceinline__ unsigned long long cell_counts(const uint2* __restrict__ prevCells,
+                                                          const uint32_t* __restrict__ leavers,
+                                                          const uint32_t* __restrict__ arrCnt,
+                                                          uint32_t c) {
+    const uint2 pr = prevCells[c];
+    const uint32_t occ = pr.x < pr.y ? pr.y - pr.x : 0u;
+    const uint32_t ac = arrCnt[c];
+    const uint32_t cnt = occ - leavers[c] + ac;
+    return (unsigned long long)cnt | ((unsigned long long)ac << 32);
+}
+
+__global__ void __launch_bounds__(kThreads)
+cells_reduce_kernel(const uint2* __restrict__ prevCells, const uint32_t* __restrict__ leavers,
+                    const uint32_t* __restrict__ arrCnt, uint32_t numCells,
+                    unsigned long long* __restrict__ partials) {
+    __shared__ unsigned long long warpTot[kThreads / 32];
+    const size_t base = (size_t)blockIdx.x * kCellChunk;
+    unsigned long long s = 0;
+#pragma unroll 4
+    for (int k = 0; k < kCellItems; ++k) {
+        const size_t c = base + (size_t)k * kThreads + threadIdx.x;
+        if (c < numCells) s += cell_counts(prevCells, leavers, arrCnt, (uint32_t)c);
+    }
+    unsigned long long total;
+    (void)block_excl_scan64<kThreads>(s, warpTot, total);
+    if (threadIdx.x == 0) partials[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kTopThreads)
+cells_top_kernel(unsigned long long* __restrict__ partials, uint32_t np) {
+    __shared__ unsigned long long warpTot[kTopThreads / 32];
+    unsigned long long v[kTopItems];
+    unsigned long long s = 0;
+    const uint32_t b = threadIdx.x * kTopItems;
+#pragma unroll
+    for (int k = 0; k < kTopItems; ++k) {
+        v[k] = (b + k < np) ? partials[b + k] : 0ull;
+        s += v[k];
+    }
+    unsigned long long total;
+    unsigned long long run = block_excl_scan64<kTopThreads>(s, warpTot, total);
+#pragma unroll
+    for (int k = 0; k < kTopItems; ++k) {
+        if (b + k < np) partials[b + k] = run;
+        run += v[k];
+    }
+}
+
+// New ranges, stayer bases and arrival bases of a tile of kCellChunk cells,
+// processed in kCellItems block-wide slabs so every access is coalesced; the
+// per-cell counters are cleared for the next step.
+__global__ void __launch_bounds__(kThreads)
+cells_apply_kernel(const uint2* __restrict__ prevCells, uint32_t* __restrict__ leavers,
+                   uint32_t* __restrict__ arrCnt, uint32_t* __restrict__ arrLo,
+                   uint32_t numCells, const unsigned long long* __restrict__ partials,
+                   uint2* __restrict__ newCells, uint32_t* __restrict__ stayBase,
+                   uint2* __restrict__ arrInfo) {
+    __shared__ unsigned long long warpTot[kThreads / 32];
+    const size_t base = (size_t)blockIdx.x * kCellChunk;
+    unsigned long long carry = partials[blockIdx.x];
+#pragma unroll 1
+    for (int k = 0; k < kCellItems; ++k) {
+        const size_t c = base + (size_t)k * kThreads + threadIdx.x;
+        const bool valid = c < numCells;
+        uint32_t occ = 0, lv = 0, ac = 0, lo = 0;
+        if (valid) {
+            const uint2 pr = prevCells[c];
+            occ = pr.x < pr.y ? pr.y - pr.x : 0u;
+            lv = leavers[c];
+            ac = arrCnt[c];
+            lo = arrLo[c];
+        }
+        const uint32_t cnt = occ - lv + ac;
+        const unsigned long long v = valid ? ((unsigned long long)cnt | ((unsigned long long)ac << 32))
+                                           : 0ull;
+        unsigned long long total;
+        const unsigned long long run = carry + block_excl_scan64<kThreads>(v, warpTot, total);
+        if (valid) {
+            const uint32_t start = (uint32_t)run, abase = (uint32_t)(run >> 32);
+            newCells[c] = cnt ? make_uint2(start, start + cnt) : make_uint2(kEmptyCell, kEmptyCell);
+            stayBase[c] = (start + lo) | (lv ? kHasLeavers : 0u);
+            if (ac) arrInfo[c] = make_uint2(abase, ac);
+            if (lv) leavers[c] = 0u;
+            if (ac) arrCnt[c] = 0u;
+            if (lo) arrLo[c] = 0u;
+        }
+        carry += total;
+        __syncthreads();  // warpTot is reused by the next slab
+    }
+}
+
+__global__ void arrivals_scatter_kernel(const uint4* __restrict__ movers,
+                                        const uint32_t* __restrict__ ctrl, uint32_t cap,
+                                        const uint2* __restrict__ arrInfo,
+                                        uint32_t* __restrict__ arrSlots) {
+    const uint32_t count = min(ctrl[kCtrlMovers], cap);
+    for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < count;
+         m += gridDim.x * blockDim.x) {
+        const uint4 r = movers[m];
+        arrSlots[arrInfo[r.y].x + r.w] = r.x;
+    }
+}
+
+__device__ __forceinline__ void move_particle(uint32_t src, uint32_t dst, DynSet from,
+                                              StatSet fromS, DynSet to, StatSet toS,
+                                              uint32_t* __restrict__ loc) {
+    to.pos[dst] = from.pos[src];
+    to.vel[dst] = from.vel[src];
+    to.theta[dst] = from.theta[src];
+    to.omega[dst] = from.omega[src];
+    toS.radius[dst] = fromS.radius[src];
+    toS.mass[dst] = fromS.mass[src];
+    const uint32_t id = fromS.id[src];
+    toS.id[dst] = id;
+    loc[id] = dst;
+    if (toS.type) toS.type[dst] = fromS.type[src];
+}
+
+// A mover goes after the arrivals of its new cell with smaller index, and
+// after the cell's stayers when it comes from a higher cell.
+__global__ void place_movers_kernel(const uint4* __restrict__ movers,
+                                    const uint32_t* __restrict__ ctrl, uint32_t cap,
+                                    const uint2* __restrict__ arrInfo,
+                                    const uint32_t* __restrict__ arrSlots,
+                                    const uint2* __restrict__ newCells,
+                                    uint32_t* __restrict__ newSortedKey, DynSet from,
+                                    StatSet fromS, DynSet to, StatSet toS,
+                                    uint32_t* __restrict__ loc) {
+    const uint32_t count = min(ctrl[kCtrlMovers], cap);
+    for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < count;
+         m += gridDim.x * blockDim.x) {
+        const uint4 r = movers[m];
+        const uint2 info = arrInfo[r.y];
+        const uint32_t g = min(info.y, kMaxGroup);
+        uint32_t rank = 0;
+        for (uint32_t k = 0; k < g; ++k) rank += arrSlots[info.x + k] < r.x ? 1u : 0u;
+        const uint2 cr = newCells[r.y];
+        const uint32_t stay = (cr.y - cr.x) - info.y;
+        const uint32_t dst = cr.x + rank + (r.z > r.y ? stay : 0u);
+        newSortedKey[dst] = r.y;
+        move_particle(r.x, dst, from, fromS, to, toS, loc);
+    }
+}
+
+// A stayer keeps its rank among the stayers of its cell.
+__global__ void __launch_bounds__(kThreads)
+place_stayers_kernel(uint32_t n, const uint32_t* __restrict__ keys,
+                     const uint32_t* __restrict__ prevSortedKey,
+                     const uint2* __restrict__ prevCells, const uint32_t* __restrict__ stayBase,
+                     uint32_t* __restrict__ newSortedKey, DynSet from, StatSet fromS, DynSet to,
+                     StatSet toS, uint32_t* __restrict__ loc, uint32_t* __restrict__ ctrl) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) ctrl[kCtrlMovers] = 0u;  // movers were consumed by the previous kernels
+    if (i >= n) return;
+    const uint32_t o = prevSortedKey[i];
+    if (keys[i] != o) return;
+    const uint32_t os = prevCells[o].x;
+    const uint32_t sb = stayBase[o];
+    uint32_t rank = i - os;
+    if (sb & kHasLeavers) {
+        const uint32_t stop = min(i, os + kMaxGroup);
+        for (uint32_t j = os; j < stop; ++j) rank -= (keys[j] != prevSortedKey[j]) ? 1u : 0u;
+    }
+    const uint32_t dst = (sb & ~kHasLeavers) + rank;
+    newSortedKey[dst] = o;
+    move_particle(i, dst, from, fromS, to, toS, loc);
+}
+
+// Full path, after the radix sort: cell ranges from the sorted keys, the
+// gather by the sorted indices, and the sorted keys kept for the next step.
+__global__ void __launch_bounds__(kThreads)
+full_reorder_kernel(uint32_t n, const uint32_t* __restrict__ hash,
+                    const uint32_t* __restrict__ index, uint2* __restrict__ cells,
+                    uint32_t* __restrict__ newSortedKey, DynSet from, StatSet fromS, DynSet to,
+                    StatSet toS, uint32_t* __restrict__ loc) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < n;
+    const uint32_t h = valid ? hash[i] : 0u;
+    uint32_t hp = __shfl_up_sync(0xffffffffu, h, 1);
+    if ((threadIdx.x & 31) == 0 && valid && i > 0) hp = hash[i - 1];
+    if (!valid) return;
+    if (i == 0 || h != hp) {
+        cells[h].x = i;
+        if (i > 0) cells[hp].y = i;
+    }
+    if (i == n - 1) cells[h].y = i + 1;
+    newSortedKey[i] = h;
+    move_particle(index[i], i, from, fromS, to, toS, loc);
+}
+
+__global__ void choose_path_kernel(const uint32_t* __restrict__ ctrl,
+                                   cudaGraphConditionalHandle fast,
+                                   cudaGraphConditionalHandle full) {
+    const bool needFull = ctrl[kCtrlNeedFull] != 0u;
+    cudaGraphSetConditional(fast, needFull ? 0u : 1u);
+    cudaGraphSetConditional(full, needFull ? 1u : 0u);
+}
+
+}  // namespace
+
+size_t incsort_bytes(uint32_t n, uint32_t numCells, uint32_t* moverCapOut) {
+    const uint32_t cap = std::max<uint32_t>(4096u, n / 8u);
+    if (moverCapOut) *moverCapOut = cap;
+    const size_t cells = al256(4ull * numCells);
+    const size_t np = (numCells + kCellChunk - 1) / kCellChunk;
+    return 4 * cells + al256(8ull * numCells) + al256(16ull * cap) + al256(4ull * cap) +
+           al256(8ull * std::max<size_t>(np, 1)) + 256;
+}
+
+IncSort carve_incsort(void* base, uint32_t n, uint32_t numCells) {
+    IncSort s;
+    s.numCells = numCells;
+    incsort_bytes(n, numCells, &s.moverCap);
+    const size_t cells = al256(4ull * numCells);
+    const size_t np = (numCells + kCellChunk - 1) / kCellChunk;
+    char* p = static_cast<char*>(base);
+    s.leavers = reinterpret_cast<uint32_t*>(p); p += cells;
+    s.arrCnt = reinterpret_cast<uint32_t*>(p); p += cells;
+    s.arrLo = reinterpret_cast<uint32_t*>(p); p += cells;
+    s.stayBase = reinterpret_cast<uint32_t*>(p); p += cells;
+    s.arrInfo = reinterpret_cast<uint2*>(p); p += al256(8ull * numCells);
+    s.movers = reinterpret_cast<uint4*>(p); p += al256(16ull * s.moverCap);
+    s.arrSlots = reinterpret_cast<uint32_t*>(p); p += al256(4ull * s.moverCap);
+    s.partials = reinterpret_cast<unsigned long long*>(p); p += al256(8ull * std::max<size_t>(np, 1));
+    s.ctrl = reinterpret_cast<uint32_t*>(p);
+    return s;
+}
+
+cudaError_t enqueue_incremental(const IncSort& s, uint32_t n, const uint32_t* keys,
+                                const uint32_t* prevSortedKey, const uint2* prevCells,
+                                uint32_t* newSortedKey, uint2* newCells, DynSet from,
+                                StatSet fromS, DynSet to, StatSet toS, uint32_t* loc,
+                                cudaStream_t st, int* launches) {
+    const uint32_t C = s.numCells;
+    const unsigned nb = blocks_for(C, kCellChunk);
+    if (nb > (unsigned)(kTopThreads * kTopItems)) return cudaErrorInvalidValue;
+    cells_reduce_kernel<<<nb, kThreads, 0, st>>>(prevCells, s.leavers, s.arrCnt, C, s.partials);
+    cells_top_kernel<<<1, kTopThreads, 0, st>>>(s.partials, nb);
+    cells_apply_kernel<<<nb, kThreads, 0, st>>>(prevCells, s.leavers, s.arrCnt, s.arrLo, C,
+                                                s.partials, newCells, s.stayBase, s.arrInfo);
+    const unsigned mb = std::min<unsigned>(blocks_for(s.moverCap, kThreads), 296u);
+    arrivals_scatter_kernel<<<mb, kThreads, 0, st>>>(s.movers, s.ctrl, s.moverCap, s.arrInfo,
+                                                     s.arrSlots);
+    place_movers_kernel<<<mb, kThreads, 0, st>>>(s.movers, s.ctrl, s.moverCap, s.arrInfo,
+                                                 s.arrSlots, newCells, newSortedKey, from, fromS,
+                                                 to, toS, loc);
+    if (n) {
+        place_stayers_kernel<<<blocks_for(n, kThreads), kThreads, 0, st>>>(
+            n, keys, prevSortedKey, prevCells, s.stayBase, newSortedKey, from, fromS, to, toS,
+            loc, s.ctrl);
+    }
+    if (launches) *launches += 6;
+    return cudaGetLastError();
+}
+
+cudaError_t enqueue_full(const IncSort& s, uint32_t n, uint32_t keyBits, uint32_t* keys,
+                         uint32_t* perm, const OnesweepScratch& os, uint32_t* errFlag,
+                         uint32_t* newSortedKey, uint2* newCells, DynSet from, StatSet fromS,
+                         DynSet to, StatSet toS, uint32_t* loc, cudaStream_t st, int* launches) {
+    uint32_t *ko, *vo;
+    cudaError_t e = onesweep_sort_pairs(keys, perm, n, keyBits, true, os, errFlag, st, &ko, &vo,
+                                        launches);
+    if (e != cudaSuccess) return e;
+    e = fill_u32(reinterpret_cast<uint32_t*>(newCells), kEmptyCell, 2ull * s.numCells, st,
+                 launches);
+    if (e != cudaSuccess) return e;
+    if (n) {
+        full_reorder_kernel<<<blocks_for(n, kThreads), kThreads, 0, st>>>(
+            n, ko, vo, newCells, newSortedKey, from, fromS, to, toS, loc);
+        if (launches) ++*launches;
+    }
+    // the incremental counters restart from zero: the step kernel of this
+    // step records the movers of the next one
+    e = fill_u32(s.leavers, 0u, s.numCells, st, launches);
+    if (e == cudaSuccess) e = fill_u32(s.arrCnt, 0u, s.numCells, st, launches);
+    if (e == cudaSuccess) e = fill_u32(s.arrLo, 0u, s.numCells, st, launches);
+    if (e == cudaSuccess) e = fill_u32(s.ctrl, 0u, 2, st, launches);
+    if (e != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
+cudaError_t enqueue_choose_path(const IncSort& s, cudaGraphConditionalHandle fast,
+                                cudaGraphConditionalHandle full, cudaStream_t st) {
+    choose_path_kernel<<<1, 1, 0, st>>>(s.ctrl, fast, full);
+    return cudaGetLastError();
+}
+
+}  // namespace dem

@@ -1,0 +1,76 @@
+// Incremental stable sort of the context step.
+//
+// Between two steps a particle changes cell only when it crosses a cell
+// border, which in a granular packing is rare.  The state is kept sorted by
+// cell, and the stable sort of the new keys is rebuilt from the old order:
+// for each cell c the stable order is
+//     [arrivals from cells < c, by index] [stayers of c, in old order]
+//     [arrivals from cells > c, by index]
+// because the old order is sorted by old cell.  The step kernel records every
+// particle whose cell changes ("mover") with its old and new cell and a slot
+// in the new cell's arrival group, and counts leavers/arrivals per cell.
+// Then:
+//   cells pass  : new count per cell = old count - leavers + arrivals, and
+//                 an exclusive scan of (count, arrivals) gives each cell's
+//                 start and its arrivals' base;
+//   movers      : each mover's rank among its cell's arrivals by index;
+//   placement   : every particle computes its sorted position and moves its
+//                 own state there (scatter, nearly coalesced), writing
+//                 loc[id] and its sorted key.
+// The result is identical to the stable radix sort + reorder of the
+// reference.  When the mover list overflows, an arrival group or a leaving
+// cell is larger than kMaxGroup, or there is no previous order (first
+// step), the full path runs instead: the onesweep radix sort, cell ranges
+// from the sorted keys, and the gather.  Graph conditional nodes choose the
+// path on the device.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "dem_kernels.cuh"
+#include "dem_sort.cuh"
+
+namespace dem {
+
+constexpr uint32_t kCtrlNeedFull = 0;        // ctrl[0]: non-zero -> full path next step
+constexpr uint32_t kCtrlMovers = 1;          // ctrl[1]: movers recorded by the step kernel
+constexpr uint32_t kHasLeavers = 0x80000000u;  // flag bit in stayBase
+
+// Buffers of the incremental path (all device memory, owned by the context).
+struct IncSort {
+    uint32_t numCells = 0, moverCap = 0;
+    uint32_t* leavers = nullptr;   // per cell, zero between steps
+    uint32_t* arrCnt = nullptr;    // per cell, zero between steps
+    uint32_t* arrLo = nullptr;     // per cell, zero between steps
+    uint32_t* stayBase = nullptr;  // per cell
+    uint2* arrInfo = nullptr;      // per cell (written for cells with arrivals)
+    uint4* movers = nullptr;       // moverCap records (index, new cell, old cell, arrival slot)
+    uint32_t* arrSlots = nullptr;  // moverCap
+    unsigned long long* partials = nullptr;  // scan partials
+    uint32_t* ctrl = nullptr;      // kCtrlNeedFull, kCtrlMovers
+};
+
+size_t incsort_bytes(uint32_t n, uint32_t numCells, uint32_t* moverCapOut);
+IncSort carve_incsort(void* base, uint32_t n, uint32_t numCells);
+
+// Fast path: new cell ranges, sorted keys, moved state.  prev* describe the
+// order the step kernel just stepped; `keys` are the new keys.
+cudaError_t enqueue_incremental(const IncSort& s, uint32_t n, const uint32_t* keys,
+                                const uint32_t* prevSortedKey, const uint2* prevCells,
+                                uint32_t* newSortedKey, uint2* newCells, DynSet from,
+                                StatSet fromS, DynSet to, StatSet toS, uint32_t* loc,
+                                cudaStream_t st, int* launches);
+
+// Full path: onesweep sort of `keys`, cell ranges, gather, reset of the
+// incremental counters.  `perm` and `keys` are overwritten.
+cudaError_t enqueue_full(const IncSort& s, uint32_t n, uint32_t keyBits, uint32_t* keys,
+                         uint32_t* perm, const OnesweepScratch& os, uint32_t* errFlag,
+                         uint32_t* newSortedKey, uint2* newCells, DynSet from, StatSet fromS,
+                         DynSet to, StatSet toS, uint32_t* loc, cudaStream_t st, int* launches);
+
+// Sets the two conditional handles from ctrl[kCtrlNeedFull].
+cudaError_t enqueue_choose_path(const IncSort& s, cudaGraphConditionalHandle fast,
+                                cudaGraphConditionalHandle full, cudaStream_t st);
+
+}  // namespace dem

@@ -195,6 +195,93 @@ __device__ __forceinline__ void collide_one(const KParams& P, uint32_t i, int2 g
     }
 }
 
+// Row-interval form of collide_one for the context step (no attraction, no
+// x-wrap among the visited columns).  The cells (cx-1, cx, cx+1) of one row
+// are consecutive cells, so their particles form one contiguous index
+// interval in sorted order.  A lane walks its (culled) row intervals as one
+// flat loop, so the lanes of a warp run about as many iterations as their
+// own candidates instead of the per-cell maximum over the warp.  The
+// summation order is the reference's: contacts are met in (row, index)
+// order, the cell a contact belongs to is found from the cell boundaries,
+// each row keeps one subtotal per cell and adds them to the force in cell
+// order at the end of the row (an empty or culled cell adds +0, which
+// changes nothing).  Returns false, without touching the outputs, when the
+// visited columns wrap; the caller then uses collide_one.
+template <bool TYPED>
+__device__ __forceinline__ bool collide_rows(const KParams& P, uint32_t i, int2 g, float2 p,
+                                             float2 v, float w, float r, uint32_t mat,
+                                             const float2* __restrict__ pos,
+                                             const float2* __restrict__ vel,
+                                             const float* __restrict__ omega,
+                                             const float* __restrict__ radius,
+                                             const uint32_t* __restrict__ type,
+                                             const uint2* __restrict__ cells, float2& force,
+                                             float& moment, float& pr) {
+    int y0 = -1, y1 = 1, x0 = -1, x1 = 1;
+    float reach2 = INFINITY;
+    if (p.x > P.cullMargin && p.x < P.Lx - P.cullMargin && p.y > P.cullMargin &&
+        p.y < P.Ly - P.cullMargin) {
+        const float reach = (r + P.rmax) * 1.0001f + P.cullMargin;
+        const float X0 = (float)g.x * P.cellW, Y0 = (float)g.y * P.cellH;
+        if (p.x - X0 > reach) x0 = 0;
+        if (X0 + P.cellW - p.x > reach) x1 = 0;
+        if (p.y - Y0 > reach) y0 = 0;
+        if (Y0 + P.cellH - p.y > reach) y1 = 0;
+        const float rr = (r + P.rmax) * 1.0001f;
+        reach2 = rr * rr;
+    }
+    if (g.x + x0 < 0 || g.x + x1 >= (int)P.gx) return false;
+    force = make_float2(0.0f, 0.0f);
+    moment = 0.0f;
+    pr = 0.0f;
+    const float4 pc0 = P.pair[0];
+#pragma unroll 1
+    for (int dy = y0; dy <= y1; ++dy) {
+        const uint32_t row = (uint32_t)((g.y + dy) & (int)(P.gy - 1u)) * P.gx;
+        // the visited cells of this row: [first, last] of x0..x1; boundaries
+        // b1/b2 = first index of the 2nd/3rd visited cell (a contact at index
+        // j belongs to visited cell (j >= b1) + (j >= b2))
+        const uint2 c0 = __ldg(cells + row + (uint32_t)(g.x + x0));
+        const uint2 c1 = x1 - x0 >= 1 ? __ldg(cells + row + (uint32_t)(g.x + x0 + 1)) : c0;
+        const uint2 c2 = x1 - x0 >= 2 ? __ldg(cells + row + (uint32_t)(g.x + x1)) : c1;
+        const uint32_t e0 = c0.x < c0.y ? c0.y : 0u;
+        const uint32_t s1 = c1.x < c1.y ? c1.x : 0xffffffffu;
+        const uint32_t e1 = c1.x < c1.y ? c1.y : 0u;
+        const uint32_t s2 = c2.x < c2.y ? c2.x : 0xffffffffu;
+        uint32_t a = c0.x < c0.y ? c0.x : (s1 != 0xffffffffu ? s1 : s2);
+        uint32_t b = x1 - x0 >= 2 ? (c2.x < c2.y ? c2.y : (x1 - x0 >= 1 ? max(e1, e0) : e0))
+                                  : (x1 - x0 >= 1 ? max(e1, e0) : e0);
+        if (a == 0xffffffffu) a = b = 0u;  // every visited cell is empty
+        const uint32_t b1 = x1 - x0 >= 1 ? (s1 != 0xffffffffu ? s1 : (e0 ? e0 : a)) : 0xffffffffu;
+        const uint32_t b2 = x1 - x0 >= 2 ? (s2 != 0xffffffffu ? s2 : max(max(e1, e0), a))
+                                         : 0xffffffffu;
+        float2 f0 = make_float2(0.0f, 0.0f), f1 = f0, f2 = f0;
+#pragma unroll 1
+        for (uint32_t j = a; j < b; ++j) {
+            if (j == i) continue;
+            const float2 pj = __ldg(pos + j);
+            const float relx = pj.x - p.x, rely = pj.y - p.y;
+            const float d2 = relx * relx + rely * rely;
+            if (d2 > reach2) continue;
+            const float rj = __ldg(radius + j);
+            float4 pc = pc0;
+            if (TYPED) pc = P.pair[mat * P.nmat + __ldg(type + j)];
+            const float cd = r + rj;
+            if (d2 <= cd * cd * 1.000002f && sqrtf(d2) < cd) {
+                const float2 f = pair_force(p, pj, v, __ldg(vel + j), w, __ldg(omega + j), r, rj,
+                                            pc, P.dt, moment, pr);
+                if (j >= b2) { f2.x += f.x; f2.y += f.y; }
+                else if (j >= b1) { f1.x += f.x; f1.y += f.y; }
+                else { f0.x += f.x; f0.y += f.y; }
+            }
+        }
+        force.x += f0.x; force.y += f0.y;
+        force.x += f1.x; force.y += f1.y;
+        force.x += f2.x; force.y += f2.y;
+    }
+    return true;
+}
+
 template <bool TYPED, bool ATTRACT>
 __global__ void __launch_bounds__(kCollideThreads)
 collide_kernel(KParams P, const float2* __restrict__ pos, const float2* __restrict__ vel,
@@ -253,7 +340,7 @@ __global__ void __launch_bounds__(kCollideThreads)
 step_kernel(KParams P, DynSet in, StatSet inS, const uint32_t* __restrict__ sortedKey,
             const uint2* __restrict__ cellRange, DynSet out, uint32_t* __restrict__ nextHash,
             float* __restrict__ pressure, float2* __restrict__ acc, float* __restrict__ alpha,
-            uint32_t* __restrict__ errFlag, uint32_t n, uint32_t log2gx) {
+            uint32_t* __restrict__ errFlag, uint32_t n, uint32_t log2gx, MoverSinkArgs sink) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     Dyn s;
@@ -267,9 +354,12 @@ step_kernel(KParams P, DynSet in, StatSet inS, const uint32_t* __restrict__ sort
     const int2 g = make_int2((int)(key & (P.gx - 1u)), (int)(key >> log2gx));
     float2 f;
     float moment, pr;
-    collide_one<TYPED, ATTRACT, CULL>(P, i, g, s.p, s.v, s.w, r, mat, in.pos, in.vel, in.omega,
-                                      inS.radius, inS.type, PackedCells{cellRange}, f, moment,
-                                      pr);
+    if (ATTRACT || !CULL ||
+        !collide_rows<TYPED>(P, i, g, s.p, s.v, s.w, r, mat, in.pos, in.vel, in.omega,
+                             inS.radius, inS.type, cellRange, f, moment, pr))
+        collide_one<TYPED, ATTRACT, CULL>(P, i, g, s.p, s.v, s.w, r, mat, in.pos, in.vel,
+                                          in.omega, inS.radius, inS.type, PackedCells{cellRange},
+                                          f, moment, pr);
     const float m = inS.mass[i];
     const float2 a = make_float2(f.x / m, f.y / m);
     const float al = moment / inertia_of(m, r);
@@ -283,8 +373,21 @@ step_kernel(KParams P, DynSet in, StatSet inS, const uint32_t* __restrict__ sort
     out.omega[i] = s.w;
     if (pressure) pressure[i] = pr;
     const int2 gn = grid_pos(P, s.p);
-    nextHash[i] = grid_hash(P, gn.x, gn.y);
+    const uint32_t nk = grid_hash(P, gn.x, gn.y);
+    nextHash[i] = nk;
     if (!(isfinite(s.p.x) && isfinite(s.p.y))) atomicOr(errFlag, 1u);
+    if (sink.ctrl && nk != key) {
+        // a mover: count it as a leaver of its cell and an arrival of the new
+        // one, and record it for the next step's incremental sort
+        const uint32_t slot = atomicAdd(sink.arrCnt + nk, 1u);
+        atomicAdd(sink.leavers + key, 1u);
+        if (nk > key) atomicAdd(sink.arrLo + nk, 1u);
+        const uint32_t m = atomicAdd(sink.ctrl + 1, 1u);
+        const uint2 own = cellRange[key];
+        if (m < sink.moverCap) sink.movers[m] = make_uint4(i, nk, key, slot);
+        if (m >= sink.moverCap || slot >= kMaxGroup || own.y - own.x > kMaxGroup)
+            atomicOr(sink.ctrl, 1u);
+    }
 }
 
 // Reorder for the context step: as reorder_kernel, but the cell ranges are
@@ -455,7 +558,7 @@ cudaError_t launch_integrate(const KParams& P, float2* pos, float2* vel, const f
 cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t* sortedKey,
                         const uint2* cellRange, DynSet out, uint32_t* nextHash, float* pressure,
                         float2* acc, float* alpha, uint32_t* errFlag, uint32_t n,
-                        cudaStream_t st) {
+                        MoverSinkArgs sink, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     const bool typed = inS.type != nullptr && P.nmat > 1;
     const bool attract = has_attraction(P);
@@ -469,7 +572,7 @@ cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t
 #define DEM_STEP(T, A, C)                                                                 \
     step_kernel<T, A, C><<<b, kCollideThreads, 0, st>>>(P, in, inS, sortedKey, cellRange, out, \
                                                         nextHash, pressure, acc, alpha,     \
-                                                        errFlag, n, log2gx)
+                                                        errFlag, n, log2gx, sink)
     if (typed) {
         if (attract) DEM_STEP(true, true, false);
         else if (cull) DEM_STEP(true, false, true);

@@ -58,10 +58,20 @@ cudaError_t launch_integrate(const KParams& P, float2* pos, float2* vel, const f
 // (with its sort keys and interleaved cell ranges), writes the integrated
 // state to `out` (same order) and the cell key of each new position to
 // `nextHash`.  acc/alpha/pressure may be null.
+// Movers (particles whose cell changes) are reported to `sink` for the
+// incremental sort; a null sink.ctrl disables the recording.
+struct MoverSinkArgs {
+    uint32_t* leavers;
+    uint32_t* arrCnt;
+    uint32_t* arrLo;
+    uint4* movers;
+    uint32_t* ctrl;
+    uint32_t moverCap;
+};
 cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t* sortedKey,
                         const uint2* cellRange, DynSet out, uint32_t* nextHash, float* pressure,
                         float2* acc, float* alpha, uint32_t* errFlag, uint32_t n,
-                        cudaStream_t st);
+                        MoverSinkArgs sink, cudaStream_t st);
 
 // Reorder with interleaved (start, end) cell ranges; resets the ranges first.
 cudaError_t launch_reorder_packed(uint2* cellRange, DynSet sorted, StatSet sortedS,

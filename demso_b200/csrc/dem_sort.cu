@@ -364,6 +364,12 @@ onesweep_kernel(const uint32_t* __restrict__ keysIn, const uint32_t* __restrict_
     }
 }
 
+__global__ void fill_words_kernel(uint32_t* __restrict__ p, uint32_t value, size_t count) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+         i += (size_t)gridDim.x * blockDim.x)
+        p[i] = value;
+}
+
 __global__ void iota_kernel(uint32_t* __restrict__ v, uint32_t n) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) v[i] = i;
@@ -475,7 +481,10 @@ cudaError_t onesweep_impl(uint32_t* keys, uint32_t* vals, uint32_t n, const Sort
                           int* launches) {
     constexpr int R = 1 << BITS;
     const uint32_t numTiles = (n + kSortTile - 1) / kSortTile;
-    cudaError_t e = cudaMemsetAsync(s.globalHist, 0, sizeof(uint32_t) * 4 * R, st);
+    // clearing by kernel (not memset nodes) keeps this path valid inside a
+    // conditional graph body
+    fill_words_kernel<<<4, 256, 0, st>>>(s.globalHist, 0u, 4 * (size_t)R);
+    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -489,11 +498,15 @@ cudaError_t onesweep_impl(uint32_t* keys, uint32_t* vals, uint32_t n, const Sort
     global_hist_kernel<BITS><<<hb, kSortThreads, 0, st>>>(keys, n, plan.passes, shifts, rowsv,
                                                           s.globalHist);
     global_hist_scan_kernel<BITS><<<plan.passes, 1024, 0, st>>>(s.globalHist);
-    if (launches) *launches += 2;
+    if (launches) *launches += 3;
     uint32_t *ki = keys, *vi = vals, *ko = s.altKeys, *vo = s.altVals;
     for (int p = 0; p < plan.passes; ++p) {
         const uint32_t rows = 1u << plan.bits[p];
-        e = cudaMemsetAsync(s.lookback, 0, sizeof(uint32_t) * (64 + (size_t)numTiles * rows), st);
+        const size_t lbWords = 64 + (size_t)numTiles * rows;
+        fill_words_kernel<<<(unsigned)std::min<size_t>((lbWords + 255) / 256, 1184), 256, 0, st>>>(
+            s.lookback, 0u, lbWords);
+        if (launches) ++*launches;
+        e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         const uint32_t* go = s.globalHist + (size_t)p * R;
         if (identityVals && p == 0)

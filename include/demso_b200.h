@@ -211,11 +211,14 @@ int dem_kernels_per_step(DemContext* ctx);
 int dem_get_followed(DemContext* ctx, const uint32_t* ids, uint32_t count, float* rows,
                      void* stream);
 
-/* Stage timing inside dem_step (CUDA events recorded by the step's graph):
- * after dem_profile_begin(ctx, maxSteps) the next dem_step calls (up to
- * maxSteps steps in total) bracket each stage with events; dem_profile_end
- * synchronises and returns the summed milliseconds per stage
- *   ms[0] = sort (all passes), ms[1] = reorder (cell reset + gather),
+/* Stage timing inside dem_step.  Each step is two graph launches on the
+ * caller's stream: the sort phase (incremental sort, or the full radix sort
+ * with cell ranges and gather) and the step kernel.  After
+ * dem_profile_begin(ctx, maxSteps) the next dem_step calls (up to maxSteps
+ * steps in total) record CUDA events around the two launches;
+ * dem_profile_end synchronises and returns the summed milliseconds
+ *   ms[0] = sort phase (sort + reorder of the state into sorted order),
+ *   ms[1] = 0 (the reorder is part of the sort phase),
  *   ms[2] = collide + integrate + next hash
  * and the number of steps profiled. */
 #define DEM_NUM_STAGES 3
