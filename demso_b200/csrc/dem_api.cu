@@ -84,6 +84,8 @@ KParams make_kparams(const DemSystem* s, uint32_t n) {
     P.cellW = P.Lx / P.gxf;
     P.cellH = P.Ly / P.gyf;
     P.cullMargin = 4e-6f * (P.Lx > P.Ly ? P.Lx : P.Ly);
+    P.invLx = 1.0f / P.Lx;
+    P.invLy = 1.0f / P.Ly;
     for (uint32_t a = 0; a < P.nmat; ++a) {
         const DemMaterial& A = s->materials[a];
         P.cn[a] = A.normalDamping;

@@ -47,6 +47,7 @@ struct KParams {
     float rmax;
     float cellW, cellH;
     float cullMargin;
+    float invLx, invLy;  // rn(1/Lx), rn(1/Ly) for grid_pos_fast
 };
 
 // particles_kernel.cuh:36-41, evaluated on the host when KParams is built.
@@ -67,6 +68,25 @@ __device__ __forceinline__ int2 grid_pos(const KParams& P, float2 p) {
     g.x = (int)floorf(p.x * P.gxf / P.Lx);
     g.y = (int)floorf(p.y * P.gyf / P.Ly);
     return g;
+}
+
+// grid_pos without the two divisions in the common case.  The reference's
+// quotient q = rn(rn(p * g) / L) and t * rn(1/L) (t = rn(p * g)) differ by at
+// most 3 ulp of q (two roundings of the product, one of the reciprocal, one
+// of the quotient: 4 * 2^-24 relative), so floor() of both agrees unless
+// t * rn(1/L) lies within 2^-20 * |q| of an integer; then, and for
+// non-finite or huge values, the IEEE division decides.
+__device__ __forceinline__ int grid_axis_fast(float p, float gf, float L, float invL) {
+    const float t = p * gf;
+    const float qa = t * invL;
+    const float fl = floorf(qa);
+    const float tol = fabsf(qa) * 9.5367431640625e-07f;  // 2^-20
+    if (fabsf(qa) < 8388608.0f && qa - fl > tol && (fl + 1.0f) - qa > tol) return (int)fl;
+    return (int)floorf(t / L);
+}
+__device__ __forceinline__ int2 grid_pos_fast(const KParams& P, float2 p) {
+    return make_int2(grid_axis_fast(p.x, P.gxf, P.Lx, P.invLx),
+                     grid_axis_fast(p.y, P.gyf, P.Ly, P.invLy));
 }
 
 // particles_kernel.cuh:124-130: power-of-two wrap, row-major cell index.
@@ -219,7 +239,10 @@ __device__ __forceinline__ void integrate_one(const KParams& P, Dyn& s, float2 a
     s.w += al * P.dt;
     s.th += s.w * P.dt;
     const double twopi = 2.0 * 3.14159265358979323846;
-    if ((double)s.th > twopi) s.th = (float)((double)s.th - twopi * floor((double)s.th / twopi));
+    // (double)th > 2*pi exactly when th > 6.2831850f, the largest float below
+    // 2*pi (the next float up, 6.28318548f, is above it)
+    if (s.th > 6.28318500518798828125f)
+        s.th = (float)((double)s.th - twopi * floor((double)s.th / twopi));
     if (s.th < 0.0f) s.th = (float)((double)s.th - twopi * floor((double)s.th / twopi));
     const float eb = P.eb[mat];
     if (s.p.x > P.Lx - r) { s.p.x = P.Lx - r; s.v.x *= -eb; }

@@ -256,23 +256,34 @@ __device__ __forceinline__ bool collide_rows(const KParams& P, uint32_t i, int2 
         const uint32_t b2 = x1 - x0 >= 2 ? (s2 != 0xffffffffu ? s2 : max(max(e1, e0), a))
                                          : 0xffffffffu;
         float2 f0 = make_float2(0.0f, 0.0f), f1 = f0, f2 = f0;
+        // four candidates per iteration, their loads issued together; indices
+        // past the interval load its last element and are masked off
 #pragma unroll 1
-        for (uint32_t j = a; j < b; ++j) {
-            if (j == i) continue;
-            const float2 pj = __ldg(pos + j);
-            const float relx = pj.x - p.x, rely = pj.y - p.y;
-            const float d2 = relx * relx + rely * rely;
-            if (d2 > reach2) continue;
-            const float rj = __ldg(radius + j);
-            float4 pc = pc0;
-            if (TYPED) pc = P.pair[mat * P.nmat + __ldg(type + j)];
-            const float cd = r + rj;
-            if (d2 <= cd * cd * 1.000002f && sqrtf(d2) < cd) {
-                const float2 f = pair_force(p, pj, v, __ldg(vel + j), w, __ldg(omega + j), r, rj,
-                                            pc, P.dt, moment, pr);
-                if (j >= b2) { f2.x += f.x; f2.y += f.y; }
-                else if (j >= b1) { f1.x += f.x; f1.y += f.y; }
-                else { f0.x += f.x; f0.y += f.y; }
+        for (uint32_t j0 = a; j0 < b; j0 += 4) {
+            float2 q[4];
+            float d2[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) q[k] = __ldg(pos + min(j0 + k, b - 1));
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const float relx = q[k].x - p.x, rely = q[k].y - p.y;
+                d2[k] = relx * relx + rely * rely;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const uint32_t j = j0 + k;
+                if (j >= b || j == i || d2[k] > reach2) continue;
+                const float rj = __ldg(radius + j);
+                float4 pc = pc0;
+                if (TYPED) pc = P.pair[mat * P.nmat + __ldg(type + j)];
+                const float cd = r + rj;
+                if (d2[k] <= cd * cd * 1.000002f && sqrtf(d2[k]) < cd) {
+                    const float2 f = pair_force(p, q[k], v, __ldg(vel + j), w, __ldg(omega + j),
+                                                r, rj, pc, P.dt, moment, pr);
+                    if (j >= b2) { f2.x += f.x; f2.y += f.y; }
+                    else if (j >= b1) { f1.x += f.x; f1.y += f.y; }
+                    else { f0.x += f.x; f0.y += f.y; }
+                }
             }
         }
         force.x += f0.x; force.y += f0.y;
@@ -332,11 +343,63 @@ integrate_kernel(KParams P, float2* __restrict__ pos, float2* __restrict__ vel,
     if (pressure) pressure[i] = pr;
 }
 
+// collide_one/rows/staged done: acceleration, integration, next hash, mover
+// record (shared tail of step_kernel).
+template <bool TYPED>
+__device__ __forceinline__ void finish_particle(
+    const KParams& P, uint32_t i, Dyn& s, float2 f, float moment, float pr, float r, uint32_t mat,
+    uint32_t key, DynSet in, StatSet inS, const uint2* __restrict__ cellRange, DynSet out,
+    uint32_t* __restrict__ nextHash, float* __restrict__ pressure, float2* __restrict__ acc,
+    float* __restrict__ alpha, uint32_t* __restrict__ errFlag, MoverSinkArgs sink) {
+    const float m = inS.mass[i];
+    // F/m and M/I as the reference divides them.  Without contacts F and M
+    // are +0 (sums that start at +0 never become -0), and +0 divided by a
+    // positive finite mass or inertia is exactly +0, so the divisions are
+    // skipped then; 2 m r^2 in [1e-30, 1e30] keeps the inertia positive and
+    // finite.
+    const bool quiet = f.x == 0.0f && f.y == 0.0f && moment == 0.0f && m > 0.0f && m < INFINITY;
+    const float two_mrr = 2.0f * m * r * r;
+    float2 a;
+    float al;
+    if (quiet && two_mrr >= 1e-30f && two_mrr <= 1e30f) {
+        a = make_float2(0.0f, 0.0f);
+        al = 0.0f;
+    } else {
+        a = make_float2(f.x / m, f.y / m);
+        al = moment / inertia_of(m, r);
+    }
+    if (acc) acc[i] = a;
+    if (alpha) alpha[i] = al;
+    s.th = in.theta[i];
+    integrate_one(P, s, a, al, r, m, mat, pr);
+    out.pos[i] = s.p;
+    out.vel[i] = s.v;
+    out.theta[i] = s.th;
+    out.omega[i] = s.w;
+    if (pressure) pressure[i] = pr;
+    const int2 gn = grid_pos_fast(P, s.p);
+    const uint32_t nk = grid_hash(P, gn.x, gn.y);
+    nextHash[i] = nk;
+    if (!(isfinite(s.p.x) && isfinite(s.p.y))) atomicOr(errFlag, 1u);
+    if (sink.ctrl && nk != key) {
+        // a mover: count it as a leaver of its cell and an arrival of the new
+        // one, and record it for the next step's incremental sort
+        const uint32_t slot = atomicAdd(sink.arrCnt + nk, 1u);
+        atomicAdd(sink.leavers + key, 1u);
+        if (nk > key) atomicAdd(sink.arrLo + nk, 1u);
+        const uint32_t m = atomicAdd(sink.ctrl + 1, 1u);
+        const uint2 own = cellRange[key];
+        if (m < sink.moverCap) sink.movers[m] = make_uint4(i, nk, key, slot);
+        if (m >= sink.moverCap || slot >= kMaxGroup || own.y - own.x > kMaxGroup)
+            atomicOr(sink.ctrl, 1u);
+    }
+}
+
 // collideD + integrateSystemD + calcHashD of the next step for one particle.
 // The acceleration stays in registers instead of a round trip through HBM;
 // the arithmetic is the same expressions in the same order.
 template <bool TYPED, bool ATTRACT, bool CULL>
-__global__ void __launch_bounds__(kCollideThreads)
+__global__ void __launch_bounds__(kCollideThreads, 8)
 step_kernel(KParams P, DynSet in, StatSet inS, const uint32_t* __restrict__ sortedKey,
             const uint2* __restrict__ cellRange, DynSet out, uint32_t* __restrict__ nextHash,
             float* __restrict__ pressure, float2* __restrict__ acc, float* __restrict__ alpha,
@@ -360,34 +423,8 @@ step_kernel(KParams P, DynSet in, StatSet inS, const uint32_t* __restrict__ sort
         collide_one<TYPED, ATTRACT, CULL>(P, i, g, s.p, s.v, s.w, r, mat, in.pos, in.vel,
                                           in.omega, inS.radius, inS.type, PackedCells{cellRange},
                                           f, moment, pr);
-    const float m = inS.mass[i];
-    const float2 a = make_float2(f.x / m, f.y / m);
-    const float al = moment / inertia_of(m, r);
-    if (acc) acc[i] = a;
-    if (alpha) alpha[i] = al;
-    s.th = in.theta[i];
-    integrate_one(P, s, a, al, r, m, mat, pr);
-    out.pos[i] = s.p;
-    out.vel[i] = s.v;
-    out.theta[i] = s.th;
-    out.omega[i] = s.w;
-    if (pressure) pressure[i] = pr;
-    const int2 gn = grid_pos(P, s.p);
-    const uint32_t nk = grid_hash(P, gn.x, gn.y);
-    nextHash[i] = nk;
-    if (!(isfinite(s.p.x) && isfinite(s.p.y))) atomicOr(errFlag, 1u);
-    if (sink.ctrl && nk != key) {
-        // a mover: count it as a leaver of its cell and an arrival of the new
-        // one, and record it for the next step's incremental sort
-        const uint32_t slot = atomicAdd(sink.arrCnt + nk, 1u);
-        atomicAdd(sink.leavers + key, 1u);
-        if (nk > key) atomicAdd(sink.arrLo + nk, 1u);
-        const uint32_t m = atomicAdd(sink.ctrl + 1, 1u);
-        const uint2 own = cellRange[key];
-        if (m < sink.moverCap) sink.movers[m] = make_uint4(i, nk, key, slot);
-        if (m >= sink.moverCap || slot >= kMaxGroup || own.y - own.x > kMaxGroup)
-            atomicOr(sink.ctrl, 1u);
-    }
+    finish_particle<TYPED>(P, i, s, f, moment, pr, r, mat, key, in, inS, cellRange, out, nextHash,
+                           pressure, acc, alpha, errFlag, sink);
 }
 
 // Reorder for the context step: as reorder_kernel, but the cell ranges are
