@@ -222,6 +222,64 @@ def config_dict(n, sc):
     return d
 
 
+# ------------------------------------------------------------------ batched form
+def measure_batched(steps: int, warmup: int, num: int = 4096, loop_sample: int = 256):
+    """Batched form on the batched workload (4,096 specimens of 256..8,192
+    disks, own boxes/parameters) against looping the plain single-scene step
+    over an evenly spaced sample of the same specimens."""
+    import torch
+    import demso_b200 as D
+    from demso_b200 import scenes
+    specimens = scenes.specimen_batch(num=num, seed=0)
+    total = sum(sc.n for sc in specimens)
+    b = D.Batch([(sc.sys, sc.n) for sc in specimens], flags=D.CTX_PRESSURE)
+    st = scenes.concat_specimens(specimens)
+    t = lambda a: torch.from_numpy(a.view(np.int32) if a.dtype == np.uint32 else a)
+    b.set_state(t(st["pos"]), t(st["vel"]), t(st["theta"]), t(st["omega"]), t(st["radius"]),
+                t(st["mass"]), t(st["id"]))
+    b.step(max(3, warmup))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    b.step(steps)
+    e1.record()
+    torch.cuda.synchronize()
+    b.check()
+    batched = total * steps / (e0.elapsed_time(e1) * 1e-3)
+    kernels = b.kernels_per_step()
+    b.close()
+    # looped plain step: one single-scene context per specimen, stepped in turn
+    sample = specimens[::max(1, num // loop_sample)]
+    sims = []
+    for sc in sample:
+        sim = D.Simulation(sc.sys, capacity=sc.n, flags=D.CTX_PRESSURE)
+        sim.set_state(t(sc.pos), t(sc.vel), t(sc.theta), t(sc.omega), t(sc.radius), t(sc.mass),
+                      t(sc.id))
+        sim.step(3)
+        sims.append(sim)
+    torch.cuda.synchronize()
+    lsteps = max(3, min(steps, 20))
+    e0.record()
+    for _ in range(lsteps):
+        for sim in sims:
+            sim.step(1)
+    e1.record()
+    torch.cuda.synchronize()
+    looped = sum(sc.n for sc in sample) * lsteps / (e0.elapsed_time(e1) * 1e-3)
+    for sim in sims:
+        sim.close()
+    return {"metric": "aggregate particle-steps/s, batched vs looped plain",
+            "value": batched, "looped_plain": looped, "ratio": batched / looped,
+            "unit": UNIT, "specimens": num, "particles": total, "steps": steps,
+            "kernels_per_step": kernels,
+            "looped_sample": "%d of the %d specimens (every %d-th), %d steps each"
+                             % (len(sample), num, max(1, num // loop_sample), lsteps),
+            "workload": "batched: specimens with counts log-uniform in [256, 8192], square "
+                        "walled boxes at area fraction 0.5, radii U[0.9, 1.1] mm, kn "
+                        "log-uniform [5e4, 5e5] N/m, friction U[0.2, 0.8], damping ratio "
+                        "U[0.1, 0.5], dt 2e-6 s"}
+
+
 # ------------------------------------------------------------------ our arm
 def main():
     ap = argparse.ArgumentParser()
@@ -232,6 +290,7 @@ def main():
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -365,6 +424,13 @@ def main():
                "d2h_bytes_per_step": state_bytes / args.steps + rows.nbytes}
         sim2.close()
 
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        try:
+            batched = measure_batched(min(args.steps, 200), args.warmup)
+        except Exception as e:  # reported beside the headline, never instead of it
+            batched = {"error": str(e)}
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
@@ -379,7 +445,7 @@ def main():
                 "whole_step": {"model_bytes_per_step": whole_bytes,
                                "achieved_gbs": whole_bytes / (step_ms * 1e-3) / 1e9,
                                "frac": whole_bytes / (step_ms * 1e-3) / 1e9 / hbm},
-                "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+                "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "batched": batched,
                 "gpu_launches": kernels_per_step * args.steps,
                 "kernels_per_step": kernels_per_step}
         print(json.dumps(line), flush=True)

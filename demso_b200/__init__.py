@@ -22,7 +22,7 @@ from . import _lib
 from ._lib import CTX_ACCEL, CTX_PRESSURE, DEM_MAX_MATERIALS, DemError, check, load
 
 __all__ = ["Material", "System", "DemError", "calcHash", "sortParticles",
-           "reorderDataAndFindCellStart", "collide", "integrateSystem", "Simulation",
+           "reorderDataAndFindCellStart", "collide", "integrateSystem", "Simulation", "Batch",
            "sort_scratch_bytes", "load", "CTX_PRESSURE", "CTX_ACCEL"]
 
 
@@ -169,13 +169,16 @@ def integrateSystem(sys: System, pos, vel, acc, theta, omega, alpha, type_, radi
 class Simulation:
     """Library-owned state and the fused, graph-captured step (dem_step)."""
 
-    def __init__(self, sys: System, capacity: int, flags: int = CTX_PRESSURE):
+    def __init__(self, sys: System, capacity: int, flags: int = CTX_PRESSURE, _handle=None):
         import ctypes as C
         self.sys = sys
         self.capacity = int(capacity)
         self.flags = flags
-        self._h = C.c_void_p()
-        check(load().dem_create(sys.to_c(0), self.capacity, flags, C.byref(self._h)))
+        if _handle is None:
+            self._h = C.c_void_p()
+            check(load().dem_create(sys.to_c(0), self.capacity, flags, C.byref(self._h)))
+        else:
+            self._h = _handle
         self.n = 0
 
     def close(self) -> None:
@@ -264,3 +267,41 @@ class Simulation:
         ce = torch.empty(nc, dtype=torch.int32, device="cuda")
         check(load().dem_get_cells(self._h, cs.data_ptr(), ce.data_ptr(), _stream(stream)))
         return cs, ce
+
+
+class Batch(Simulation):
+    """Many independent scenes stepped together (dem_batch_create).
+
+    ``specs`` is a list of (System, particle count).  State arrays are the
+    concatenation of the specimens in order; ``slots(s)`` gives the slot range
+    of specimen s, which never changes."""
+
+    def __init__(self, specs, flags: int = CTX_PRESSURE):
+        import ctypes as C
+        arr = (_lib.DemSystem * len(specs))()
+        total = 0
+        for k, (sys, n) in enumerate(specs):
+            arr[k] = sys.to_c(int(n))
+            total += int(n)
+        h = C.c_void_p()
+        check(load().dem_batch_create(arr, len(specs), flags, C.byref(h)))
+        super().__init__(specs[0][0], total, flags, _handle=h)
+        self.specs = specs
+        self.materials_max = max(len(sys.materials) for sys, _ in specs)
+
+    def slots(self, s: int):
+        import ctypes as C
+        a, b = C.c_uint32(), C.c_uint32()
+        check(load().dem_batch_specimen(self._h, s, C.byref(a), C.byref(b)))
+        return a.value, a.value + b.value
+
+    def get_state(self, device="cuda", stream=None) -> dict:
+        # the typed layout follows the largest material count in the batch
+        saved = self.sys
+        if self.materials_max > 1 and len(self.sys.materials) == 1:
+            self.sys = self.specs[[len(sp.materials) for sp, _ in self.specs].index(
+                self.materials_max)][0]
+        try:
+            return super().get_state(device, stream)
+        finally:
+            self.sys = saved

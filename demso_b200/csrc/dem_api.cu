@@ -7,6 +7,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "dem_common.cuh"
 #include "dem_incsort.cuh"
@@ -86,6 +87,10 @@ KParams make_kparams(const DemSystem* s, uint32_t n) {
     P.cullMargin = 4e-6f * (P.Lx > P.Ly ? P.Lx : P.Ly);
     P.invLx = 1.0f / P.Lx;
     P.invLy = 1.0f / P.Ly;
+    P.cellOff = 0;
+    P.log2gx = 0;
+    while ((1u << P.log2gx) < P.gx) ++P.log2gx;
+    P.cull = 0;
     for (uint32_t a = 0; a < P.nmat; ++a) {
         const DemMaterial& A = s->materials[a];
         P.cn[a] = A.normalDamping;
@@ -103,6 +108,16 @@ KParams make_kparams(const DemSystem* s, uint32_t n) {
         }
     }
     return P;
+}
+
+// Culling bound: the largest radius, and whether culling is valid for this
+// grid (at least 3 cells per axis, cells wider than any contact distance).
+void set_rmax(KParams& P, float rmax) {
+    P.rmax = rmax;
+    P.cull = (std::isfinite(rmax) && P.gx >= 3 && P.gy >= 3 && P.cellW > 2.002f * rmax &&
+              P.cellH > 2.002f * rmax)
+                 ? 1u
+                 : 0u;
 }
 
 template <typename T>
@@ -279,6 +294,13 @@ struct DemContext {
     OnesweepScratch ss;
     void* incScratch = nullptr;
     IncSort inc;
+    // batched form: specimen table (device + host copy), slot -> specimen,
+    // first slot of every specimen (nspec + 1 entries)
+    uint32_t nspec = 0;
+    KParams* dTable = nullptr;
+    std::vector<KParams> hTable;
+    uint32_t* spec = nullptr;
+    std::vector<uint32_t> partOff;
     bool keysValid = false;  // keys[] holds the cell of every particle of the current state
     bool haveOrder = false;  // the last step recorded its movers: incremental sort possible
     float rmax = INFINITY;   // largest radius of the current state (culling bound)
@@ -405,7 +427,7 @@ cudaError_t enqueue_step_kernel(DemContext* c, cudaStream_t st, int* launches) {
                                 c->keys, (c->flags & DEM_CTX_PRESSURE) ? c->pressure : nullptr,
                                 (c->flags & DEM_CTX_ACCEL) ? c->acc : nullptr,
                                 (c->flags & DEM_CTX_ACCEL) ? c->alpha : nullptr, c->errFlag, c->n,
-                                sink_of(c), st);
+                                sink_of(c), st, c->nspec ? c->dTable : nullptr, c->spec);
     if (launches) ++*launches;
     return e;
 }
@@ -449,6 +471,10 @@ size_t al256(size_t b) { return (b + 255u) & ~(size_t)255u; }
 
 }  // namespace
 
+// Allocates the buffers of a context of `capacity` particles over `numCells`
+// cells (c->sys, c->P, c->typed and c->flags already set).
+int init_context(DemContext* c, uint32_t capacity, uint32_t numCells, DemContext** out);
+
 extern "C" int dem_create(const DemSystem* sys, uint32_t capacity, uint32_t flags,
                           DemContext** out) {
     if (!out) return fail(DEM_ERR_INVALID_ARG, "out is NULL");
@@ -460,12 +486,87 @@ extern "C" int dem_create(const DemSystem* sys, uint32_t capacity, uint32_t flag
     DemContext* c = new (std::nothrow) DemContext();
     if (!c) return fail(DEM_ERR_NO_MEMORY, "host allocation failed");
     c->sys = *sys;
-    c->capacity = capacity;
     c->flags = flags;
-    c->numCells = sys->gridSize[0] * sys->gridSize[1];
-    c->keyBits = log2_u32(c->numCells);
     c->typed = sys->numMaterials > 1;
     c->P = make_kparams(sys, 0);
+    return init_context(c, capacity, sys->gridSize[0] * sys->gridSize[1], out);
+}
+
+extern "C" int dem_batch_create(const DemSystem* specs, uint32_t numSpecimens, uint32_t flags,
+                                DemContext** out) {
+    if (!out) return fail(DEM_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    if (!specs || numSpecimens == 0) return fail(DEM_ERR_INVALID_ARG, "no specimens");
+    uint64_t total = 0, cells = 0;
+    uint32_t nmat = 1;
+    bool attract = false;
+    for (uint32_t s = 0; s < numSpecimens; ++s) {
+        int rc = validate(&specs[s]);
+        if (rc) return rc;
+        total += specs[s].numParticles;
+        cells += (uint64_t)specs[s].gridSize[0] * specs[s].gridSize[1];
+        nmat = std::max(nmat, specs[s].numMaterials);
+        for (uint32_t m = 0; m < specs[s].numMaterials; ++m)
+            attract = attract || specs[s].materials[m].attractCoefficient != 0.0f;
+    }
+    if (total == 0 || total >= (1u << 30)) return fail(DEM_ERR_INVALID_ARG, "batch size %llu", (unsigned long long)total);
+    if (cells > (1ull << 31)) return fail(DEM_ERR_INVALID_ARG, "too many cells in the batch");
+    DemContext* c = new (std::nothrow) DemContext();
+    if (!c) return fail(DEM_ERR_NO_MEMORY, "host allocation failed");
+    c->sys = specs[0];
+    c->flags = flags;
+    c->typed = nmat > 1;
+    c->nspec = numSpecimens;
+    c->hTable.resize(numSpecimens);
+    c->partOff.assign(numSpecimens + 1, 0u);
+    uint32_t cellOff = 0;
+    for (uint32_t s = 0; s < numSpecimens; ++s) {
+        c->hTable[s] = make_kparams(&specs[s], specs[s].numParticles);
+        c->hTable[s].cellOff = cellOff;
+        cellOff += specs[s].gridSize[0] * specs[s].gridSize[1];
+        c->partOff[s + 1] = c->partOff[s] + specs[s].numParticles;
+    }
+    // the context-wide parameters only steer template choices: a material
+    // count and an attraction flag that cover every specimen
+    c->P = make_kparams(&specs[0], (uint32_t)total);
+    c->P.nmat = nmat;
+    c->P.at[0] = attract ? 1.0f : 0.0f;
+    for (uint32_t m = 1; m < kMaxMat; ++m) c->P.at[m] = 0.0f;
+    int rc = init_context(c, (uint32_t)total, (uint32_t)cells, out);
+    if (rc) return rc;
+    c = *out;
+    std::vector<uint32_t> slotSpec(total);
+    for (uint32_t s = 0; s < numSpecimens; ++s)
+        for (uint32_t k = c->partOff[s]; k < c->partOff[s + 1]; ++k) slotSpec[k] = s;
+    cudaError_t e = cudaMalloc(&c->dTable, sizeof(KParams) * numSpecimens);
+    if (e == cudaSuccess) e = cudaMalloc(&c->spec, sizeof(uint32_t) * total);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(c->dTable, c->hTable.data(), sizeof(KParams) * numSpecimens,
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(c->spec, slotSpec.data(), sizeof(uint32_t) * total, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        dem_destroy(c);
+        *out = nullptr;
+        return cuda_fail(e, "batch tables");
+    }
+    return DEM_OK;
+}
+
+extern "C" int dem_batch_specimen(DemContext* c, uint32_t specimen, uint32_t* firstSlot,
+                                  uint32_t* count) {
+    if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    if (!c->nspec) return fail(DEM_ERR_INVALID_ARG, "not a batch");
+    if (specimen >= c->nspec) return fail(DEM_ERR_INVALID_ARG, "specimen %u >= %u", specimen, c->nspec);
+    if (firstSlot) *firstSlot = c->partOff[specimen];
+    if (count) *count = c->partOff[specimen + 1] - c->partOff[specimen];
+    return DEM_OK;
+}
+
+int init_context(DemContext* c, uint32_t capacity, uint32_t numCells, DemContext** out) {
+    c->capacity = capacity;
+    c->numCells = numCells;
+    c->keyBits = log2_u32(c->numCells);
     cudaGetDevice(&c->device);
 
     const size_t N = capacity, f4 = al256(4 * N), f8 = al256(8 * N),
@@ -539,6 +640,8 @@ extern "C" int dem_destroy(DemContext* c) {
     if (c->capStream) cudaStreamDestroy(c->capStream);
     if (c->bodyStream) cudaStreamDestroy(c->bodyStream);
     cudaFree(c->followRows);
+    cudaFree(c->dTable);
+    cudaFree(c->spec);
     cudaFree(c->incScratch);
     cudaFree(c->sortScratch);
     cudaFree(c->block);
@@ -548,6 +651,7 @@ extern "C" int dem_destroy(DemContext* c) {
 
 extern "C" int dem_set_system(DemContext* c, const DemSystem* sys) {
     if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    if (c->nspec) return fail(DEM_ERR_INVALID_ARG, "dem_set_system: use dem_batch_create for batches");
     int rc = validate(sys);
     if (rc) return rc;
     if (sys->gridSize[0] != c->sys.gridSize[0] || sys->gridSize[1] != c->sys.gridSize[1])
@@ -556,7 +660,7 @@ extern "C" int dem_set_system(DemContext* c, const DemSystem* sys) {
         return fail(DEM_ERR_INVALID_ARG, "single/multi-material layout is fixed at dem_create");
     c->sys = *sys;
     c->P = make_kparams(sys, c->n);
-    c->P.rmax = c->rmax;
+    set_rmax(c->P, c->rmax);
     drop_graphs(c);
     // keys depend on the box size; recompute them and sort from scratch
     c->keysValid = false;
@@ -570,6 +674,9 @@ extern "C" int dem_set_state(DemContext* c, uint32_t n, const float* pos, const 
                              void* stream) {
     if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
     if (n > c->capacity) return fail(DEM_ERR_CAPACITY, "n %u > capacity %u", n, c->capacity);
+    if (c->nspec && n != c->capacity)
+        return fail(DEM_ERR_INVALID_ARG, "a batch takes all %u particles, specimen by specimen",
+                    c->capacity);
     if (n && (!pos || !vel || !theta || !omega || !radius || !mass || !id))
         return fail(DEM_ERR_INVALID_ARG, "dem_set_state: NULL buffer");
     if (c->typed && n && !type)
@@ -596,8 +703,16 @@ extern "C" int dem_set_state(DemContext* c, uint32_t n, const float* pos, const 
     memcpy(&rmax, &rbits, 4);
     c->n = n;
     c->rmax = (n > 0 && std::isfinite(rmax)) ? rmax : INFINITY;
-    c->P = make_kparams(&c->sys, n);
-    c->P.rmax = c->rmax;
+    if (c->nspec) {
+        for (uint32_t sp = 0; sp < c->nspec; ++sp) set_rmax(c->hTable[sp], c->rmax);
+        set_rmax(c->P, c->rmax);
+        DEM_TRY_CUDA(cudaMemcpy(c->dTable, c->hTable.data(), sizeof(KParams) * c->nspec,
+                                cudaMemcpyHostToDevice),
+                     "specimen table");
+    } else {
+        c->P = make_kparams(&c->sys, n);
+        set_rmax(c->P, c->rmax);
+    }
     drop_graphs(c);
     c->keysValid = false;
     c->haveOrder = false;
@@ -634,7 +749,13 @@ extern "C" int dem_step(DemContext* c, uint32_t nsteps, void* stream) {
     if (nsteps == 0 || c->n == 0) return DEM_OK;
     cudaStream_t st = (cudaStream_t)stream;
     if (!c->keysValid) {
-        DEM_TRY_CUDA(launch_calc_hash(c->P, c->dyn[0].pos, c->keys, nullptr, c->n, st), "hash");
+        if (c->nspec)
+            DEM_TRY_CUDA(launch_calc_hash_batched(c->dTable, c->spec, c->dyn[0].pos, c->keys, c->n,
+                                                  st),
+                         "hash");
+        else
+            DEM_TRY_CUDA(launch_calc_hash(c->P, c->dyn[0].pos, c->keys, nullptr, c->n, st),
+                         "hash");
         c->keysValid = true;
         c->haveOrder = false;
     }

@@ -48,6 +48,11 @@ struct KParams {
     float cellW, cellH;
     float cullMargin;
     float invLx, invLy;  // rn(1/Lx), rn(1/Ly) for grid_pos_fast
+    // Batched form: the specimen's first cell in the global cell numbering (0
+    // for a single scene), log2(gx), and whether culling is valid here.
+    uint32_t cellOff;
+    uint32_t log2gx;
+    uint32_t cull;
 };
 
 // particles_kernel.cuh:36-41, evaluated on the host when KParams is built.
@@ -93,7 +98,7 @@ __device__ __forceinline__ int2 grid_pos_fast(const KParams& P, float2 p) {
 __device__ __forceinline__ uint32_t grid_hash(const KParams& P, int x, int y) {
     x &= (int)(P.gx - 1u);
     y &= (int)(P.gy - 1u);
-    return (uint32_t)y * P.gx + (uint32_t)x;
+    return P.cellOff + (uint32_t)y * P.gx + (uint32_t)x;
 }
 
 // `pressure += length(force) / (4*M_PI*r*r)` -- the reference does this sum in

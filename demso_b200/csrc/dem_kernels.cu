@@ -21,6 +21,17 @@ calc_hash_kernel(KParams P, const float2* __restrict__ pos, uint32_t* __restrict
     if (index) index[i] = i;
 }
 
+// calcHashD for the batched form: each slot hashes with its specimen's grid.
+__global__ void __launch_bounds__(kThreads)
+calc_hash_batched_kernel(const KParams* __restrict__ table, const uint32_t* __restrict__ spec,
+                         const float2* __restrict__ pos, uint32_t* __restrict__ hash, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const KParams& P = table[spec[i]];
+    const int2 g = grid_pos(P, pos[i]);
+    hash[i] = grid_hash(P, g.x, g.y);
+}
+
 // particles_kernel.cuh:156-233.  A cell starts where the sorted hash differs
 // from its predecessor; the predecessor's cell ends there.  The reference
 // stages hashes in shared memory; here the neighbour comes from the next lane
@@ -237,7 +248,7 @@ __device__ __forceinline__ bool collide_rows(const KParams& P, uint32_t i, int2 
     const float4 pc0 = P.pair[0];
 #pragma unroll 1
     for (int dy = y0; dy <= y1; ++dy) {
-        const uint32_t row = (uint32_t)((g.y + dy) & (int)(P.gy - 1u)) * P.gx;
+        const uint32_t row = P.cellOff + (uint32_t)((g.y + dy) & (int)(P.gy - 1u)) * P.gx;
         // the visited cells of this row: [first, last] of x0..x1; boundaries
         // b1/b2 = first index of the 2nd/3rd visited cell (a contact at index
         // j belongs to visited cell (j >= b1) + (j >= b2))
@@ -399,13 +410,15 @@ __device__ __forceinline__ void finish_particle(
 // The acceleration stays in registers instead of a round trip through HBM;
 // the arithmetic is the same expressions in the same order.
 template <bool TYPED, bool ATTRACT, bool CULL>
-__global__ void __launch_bounds__(kCollideThreads, 8)
-step_kernel(KParams P, DynSet in, StatSet inS, const uint32_t* __restrict__ sortedKey,
-            const uint2* __restrict__ cellRange, DynSet out, uint32_t* __restrict__ nextHash,
-            float* __restrict__ pressure, float2* __restrict__ acc, float* __restrict__ alpha,
-            uint32_t* __restrict__ errFlag, uint32_t n, uint32_t log2gx, MoverSinkArgs sink) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__device__ __forceinline__ void step_particle(const KParams& P, uint32_t i, DynSet in,
+                                              StatSet inS,
+                                              const uint32_t* __restrict__ sortedKey,
+                                              const uint2* __restrict__ cellRange, DynSet out,
+                                              uint32_t* __restrict__ nextHash,
+                                              float* __restrict__ pressure,
+                                              float2* __restrict__ acc,
+                                              float* __restrict__ alpha,
+                                              uint32_t* __restrict__ errFlag, MoverSinkArgs sink) {
     Dyn s;
     s.p = in.pos[i];
     s.v = in.vel[i];
@@ -414,17 +427,53 @@ step_kernel(KParams P, DynSet in, StatSet inS, const uint32_t* __restrict__ sort
     const uint32_t mat = TYPED ? inS.type[i] : 0u;
     // the sort key of particle i is calcGridPos of this very position, wrapped
     const uint32_t key = sortedKey[i];
-    const int2 g = make_int2((int)(key & (P.gx - 1u)), (int)(key >> log2gx));
+    const uint32_t local = key - P.cellOff;
+    const int2 g = make_int2((int)(local & (P.gx - 1u)), (int)(local >> P.log2gx));
     float2 f;
     float moment, pr;
-    if (ATTRACT || !CULL ||
+    if (ATTRACT || !CULL || !P.cull ||
         !collide_rows<TYPED>(P, i, g, s.p, s.v, s.w, r, mat, in.pos, in.vel, in.omega,
-                             inS.radius, inS.type, cellRange, f, moment, pr))
-        collide_one<TYPED, ATTRACT, CULL>(P, i, g, s.p, s.v, s.w, r, mat, in.pos, in.vel,
-                                          in.omega, inS.radius, inS.type, PackedCells{cellRange},
-                                          f, moment, pr);
+                             inS.radius, inS.type, cellRange, f, moment, pr)) {
+        if (CULL && P.cull)
+            collide_one<TYPED, ATTRACT, true>(P, i, g, s.p, s.v, s.w, r, mat, in.pos, in.vel,
+                                              in.omega, inS.radius, inS.type,
+                                              PackedCells{cellRange}, f, moment, pr);
+        else
+            collide_one<TYPED, ATTRACT, false>(P, i, g, s.p, s.v, s.w, r, mat, in.pos, in.vel,
+                                               in.omega, inS.radius, inS.type,
+                                               PackedCells{cellRange}, f, moment, pr);
+    }
     finish_particle<TYPED>(P, i, s, f, moment, pr, r, mat, key, in, inS, cellRange, out, nextHash,
                            pressure, acc, alpha, errFlag, sink);
+}
+
+template <bool TYPED, bool ATTRACT, bool CULL>
+__global__ void __launch_bounds__(kCollideThreads, 8)
+step_kernel(KParams P, DynSet in, StatSet inS, const uint32_t* __restrict__ sortedKey,
+            const uint2* __restrict__ cellRange, DynSet out, uint32_t* __restrict__ nextHash,
+            float* __restrict__ pressure, float2* __restrict__ acc, float* __restrict__ alpha,
+            uint32_t* __restrict__ errFlag, uint32_t n, MoverSinkArgs sink) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    step_particle<TYPED, ATTRACT, CULL>(P, i, in, inS, sortedKey, cellRange, out, nextHash,
+                                        pressure, acc, alpha, errFlag, sink);
+}
+
+// Batched form: particle slot i belongs to specimen spec[i] (slots of a
+// specimen are contiguous and never change specimen), whose parameters --
+// box, grid, cell offset, contact coefficients -- come from a device table.
+template <bool TYPED, bool ATTRACT, bool CULL>
+__global__ void __launch_bounds__(kCollideThreads, 8)
+step_kernel_batched(const KParams* __restrict__ table, const uint32_t* __restrict__ spec,
+                    DynSet in, StatSet inS, const uint32_t* __restrict__ sortedKey,
+                    const uint2* __restrict__ cellRange, DynSet out,
+                    uint32_t* __restrict__ nextHash, float* __restrict__ pressure,
+                    float2* __restrict__ acc, float* __restrict__ alpha,
+                    uint32_t* __restrict__ errFlag, uint32_t n, MoverSinkArgs sink) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    step_particle<TYPED, ATTRACT, CULL>(table[spec[i]], i, in, inS, sortedKey, cellRange, out,
+                                        nextHash, pressure, acc, alpha, errFlag, sink);
 }
 
 // Reorder for the context step: as reorder_kernel, but the cell ranges are
@@ -527,6 +576,14 @@ cudaError_t launch_max_radius(const float* radius, uint32_t n, uint32_t* out, cu
     return cudaGetLastError();
 }
 
+cudaError_t launch_calc_hash_batched(const KParams* table, const uint32_t* spec, const float2* pos,
+                                     uint32_t* hash, uint32_t n, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    calc_hash_batched_kernel<<<blocks_for(n, kThreads), kThreads, 0, st>>>(table, spec, pos, hash,
+                                                                           n);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_calc_hash(const KParams& P, const float2* pos, uint32_t* hash, uint32_t* index,
                              uint32_t n, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
@@ -595,21 +652,25 @@ cudaError_t launch_integrate(const KParams& P, float2* pos, float2* vel, const f
 cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t* sortedKey,
                         const uint2* cellRange, DynSet out, uint32_t* nextHash, float* pressure,
                         float2* acc, float* alpha, uint32_t* errFlag, uint32_t n,
-                        MoverSinkArgs sink, cudaStream_t st) {
+                        MoverSinkArgs sink, cudaStream_t st, const KParams* table,
+                        const uint32_t* spec) {
     if (n == 0) return cudaSuccess;
     const bool typed = inS.type != nullptr && P.nmat > 1;
     const bool attract = has_attraction(P);
     const unsigned b = blocks_for(n, kCollideThreads);
-    uint32_t log2gx = 0;
-    while ((1u << log2gx) < P.gx) ++log2gx;
-    // culling also needs cells wider than any contact distance, so that a
-    // wrapped neighbour column/row is never within reach
-    const bool cull = isfinite(P.rmax) && P.gx >= 3 && P.gy >= 3 &&
-                      P.cellW > 2.002f * P.rmax && P.cellH > 2.002f * P.rmax;
-#define DEM_STEP(T, A, C)                                                                 \
-    step_kernel<T, A, C><<<b, kCollideThreads, 0, st>>>(P, in, inS, sortedKey, cellRange, out, \
-                                                        nextHash, pressure, acc, alpha,     \
-                                                        errFlag, n, log2gx, sink)
+    const bool cull = table ? true : P.cull != 0u;
+#define DEM_STEP(T, A, C)                                                                      \
+    do {                                                                                       \
+        if (table)                                                                             \
+            step_kernel_batched<T, A, C><<<b, kCollideThreads, 0, st>>>(                       \
+                table, spec, in, inS, sortedKey, cellRange, out, nextHash, pressure, acc, alpha, \
+                errFlag, n, sink);                                                             \
+        else                                                                                   \
+            step_kernel<T, A, C><<<b, kCollideThreads, 0, st>>>(P, in, inS, sortedKey,         \
+                                                                cellRange, out, nextHash,      \
+                                                                pressure, acc, alpha, errFlag, \
+                                                                n, sink);                      \
+    } while (0)
     if (typed) {
         if (attract) DEM_STEP(true, true, false);
         else if (cull) DEM_STEP(true, false, true);

@@ -36,6 +36,8 @@ cudaError_t launch_max_radius(const float* radius, uint32_t n, uint32_t* out, cu
 
 cudaError_t launch_calc_hash(const KParams& P, const float2* pos, uint32_t* hash, uint32_t* index,
                              uint32_t n, cudaStream_t st);
+cudaError_t launch_calc_hash_batched(const KParams* table, const uint32_t* spec, const float2* pos,
+                                     uint32_t* hash, uint32_t n, cudaStream_t st);
 
 cudaError_t launch_reorder(const KParams& P, uint32_t* cellStart, uint32_t* cellEnd,
                            DynSet sorted, StatSet sortedS, uint32_t* sortedLoc,
@@ -71,7 +73,8 @@ struct MoverSinkArgs {
 cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t* sortedKey,
                         const uint2* cellRange, DynSet out, uint32_t* nextHash, float* pressure,
                         float2* acc, float* alpha, uint32_t* errFlag, uint32_t n,
-                        MoverSinkArgs sink, cudaStream_t st);
+                        MoverSinkArgs sink, cudaStream_t st, const KParams* table = nullptr,
+                        const uint32_t* spec = nullptr);
 
 // Reorder with interleaved (start, end) cell ranges; resets the ranges first.
 cudaError_t launch_reorder_packed(uint2* cellRange, DynSet sorted, StatSet sortedS,

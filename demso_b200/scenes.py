@@ -223,3 +223,53 @@ def cell_hash(pos, sys: System) -> np.ndarray:
     cx &= sys.gx - 1
     cy &= sys.gy - 1
     return (cy * sys.gx + cx).astype(np.uint32)
+
+
+def specimen_batch(num=4096, seed=0, nmin=256, nmax=8192, phi=0.5, dt=2e-6):
+    """Batched workload: `num` independent specimens with particle counts
+    log-uniform in [nmin, nmax]; each has its own square walled box at area
+    fraction `phi`, radii uniform in [0.9, 1.1] mm, kn log-uniform in
+    [5e4, 5e5] N/m, friction uniform in [0.2, 0.8] and damping ratio uniform
+    in [0.1, 0.5]; seeded random sequential placement, zero velocity.
+    Returns a list of Scenes (one per specimen)."""
+    rng = np.random.default_rng(seed)
+    counts = np.exp(rng.uniform(np.log(nmin), np.log(nmax), size=num)).astype(np.int64)
+    kns = np.exp(rng.uniform(np.log(5e4), np.log(5e5), size=num))
+    mus = rng.uniform(0.2, 0.8, size=num)
+    zetas = rng.uniform(0.1, 0.5, size=num)
+    out = []
+    rmax = 1.1e-3
+    radii = [rng.uniform(0.9e-3, 1.1e-3, size=int(counts[k])).astype(np.float32)
+             for k in range(num)]
+    boxes = [math.sqrt(r.size * math.pi * float(np.mean(r.astype(np.float64) ** 2)) / phi)
+             for r in radii]
+    # the native placement releases the GIL: place the specimens in parallel
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=16) as ex:
+        placed = list(ex.map(lambda k: rsa_positions(radii[k], boxes[k], boxes[k],
+                                                     seed=seed * 100003 + k, strips=1),
+                             range(num)))
+    for k in range(num):
+        n = int(counts[k])
+        r, L, pos = radii[k], boxes[k], placed[k]
+        g = grid_2r(L, rmax)
+        mat = pair_material(kn=float(kns[k]), zeta=float(zetas[k]), mu=float(mus[k]))
+        sys = System(Lx=L, Ly=L, gx=g, gy=g, dt=dt, gravity=(0.0, -9.81),
+                     knWall=mat.normalStiffness, ktWall=mat.shearStiffness, materials=[mat])
+        order = np.argsort(cell_hash(pos, sys), kind="stable")
+        out.append(_finish(sys, pos[order], np.zeros((n, 2)), r[order],
+                           name="specimen_%d" % k))
+    return out
+
+
+def concat_specimens(specimens):
+    """Concatenated state arrays of a batch (ids renumbered 0..N-1)."""
+    n = sum(sc.n for sc in specimens)
+    cat = lambda k: np.concatenate([getattr(sc, k) for sc in specimens])
+    st = dict(pos=cat("pos"), vel=cat("vel"), theta=cat("theta"), omega=cat("omega"),
+              radius=cat("radius"), mass=cat("mass"), id=np.arange(n, dtype=np.uint32))
+    types = [sc.type for sc in specimens]
+    st["type"] = (None if all(t is None for t in types) else
+                  np.concatenate([t if t is not None else np.zeros(sc.n, np.uint32)
+                                  for t, sc in zip(types, specimens)]))
+    return st

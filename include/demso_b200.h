@@ -181,6 +181,23 @@ int dem_set_state(DemContext* ctx, uint32_t n, const float* pos, const float* ve
                   const float* theta, const float* omega, const float* radius,
                   const float* mass, const uint32_t* id, const uint32_t* type, int host,
                   void* stream);
+/* Batched form: `numSpecimens` independent scenes stepped together, each with
+ * its own particle count (specs[s].numParticles), box, grid, gravity, time
+ * step and materials.  The state is the concatenation of the specimens
+ * (specimen 0 first); ids are one permutation of 0..N-1 over the whole
+ * batch and loc is indexed by them.  Every other context call
+ * (dem_set_state with all N particles, dem_step, dem_get_state, dem_check,
+ * dem_get_followed, profiling) works on a batch; dem_set_system does not.
+ * Cell keys carry a per-specimen offset, so the one stable sort of the batch
+ * is each specimen's own stable sort and every specimen evolves bit for bit
+ * as it would alone.  No counterpart in the reference (one scene per
+ * process). */
+int dem_batch_create(const DemSystem* specs, uint32_t numSpecimens, uint32_t flags,
+                     DemContext** out);
+/* Slots [*firstSlot, *firstSlot + *count) of the state hold specimen s (fixed
+ * for the life of the batch). */
+int dem_batch_specimen(DemContext* ctx, uint32_t specimen, uint32_t* firstSlot, uint32_t* count);
+
 /* Copies out the current state in its current (cell-sorted) order, plus loc
  * (indexed by id) and, when requested at create time, pressure/acc/alpha of
  * the last step.  NULL outputs are skipped. */

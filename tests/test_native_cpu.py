@@ -103,3 +103,15 @@ def test_bad_arguments_are_status_codes_not_crashes():
 def test_python_errors_raise():
     with pytest.raises(D.DemError):
         _lib.check(1)
+
+
+def test_batch_create_rejects_bad_specimens():
+    import ctypes as C
+    lib = _lib.load()
+    arr = (_lib.DemSystem * 2)()
+    arr[0] = _sys().to_c(10)
+    arr[1] = _sys(gx=12).to_c(10)
+    h = C.c_void_p()
+    assert lib.dem_batch_create(arr, 2, 0, C.byref(h)) == 1
+    assert lib.dem_batch_create(None, 0, 0, C.byref(h)) == 1
+    assert lib.dem_batch_specimen(None, 0, None, None) == 1
