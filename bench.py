@@ -280,6 +280,77 @@ def measure_batched(steps: int, warmup: int, num: int = 4096, loop_sample: int =
                         "U[0.1, 0.5], dt 2e-6 s"}
 
 
+# ------------------------------------------------------------------ adjoint
+def measure_adjoint(n: int = 16384, steps: int = 2000, every: int = 100):
+    """Cost of the adjoint on the differentiable workload (n disks released
+    from a seeded heap onto a 20-degree incline, `steps` steps, a checkpoint
+    every `every` steps): the plain forward, the checkpointing forward and the
+    backward (recompute of each window plus the reverse steps), per step."""
+    import ctypes as C
+    import torch
+    import demso_b200 as D
+    from demso_b200 import scenes
+    sc = scenes.incline_heap(n=n, seed=0)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int32) if a.dtype == np.uint32
+                                   else np.ascontiguousarray(a))
+    L = D.load()
+    sim = D.Simulation(sc.sys, capacity=n, flags=D.CTX_PRESSURE | D.CTX_ACCEL)
+    stream = torch.cuda.current_stream().cuda_stream
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+
+    def reset():
+        sim.set_state(t(sc.pos), t(sc.vel), t(sc.theta), t(sc.omega), t(sc.radius), t(sc.mass),
+                      t(sc.id))
+
+    reset()
+    sim.step(50)
+    reset()
+    torch.cuda.synchronize()
+    e0, e1, e2, e3 = ev(), ev(), ev(), ev()
+    e0.record()
+    sim.step(steps)
+    e1.record()
+    torch.cuda.synchronize()
+    plain = e0.elapsed_time(e1) / steps
+    reset()
+    torch.cuda.synchronize()
+    e0.record()
+    D.check(L.dem_adj_forward(sim.handle, steps, every, stream))
+    e1.record()
+    torch.cuda.synchronize()
+    fwd = e0.elapsed_time(e1) / steps
+    # cotangents of loss = mean x-displacement + kinetic energy, by id
+    st = {k: v.numpy() for k, v in sim.get_state("cpu").items() if v is not None}
+    order = np.argsort(st["id"].view(np.uint32))
+    m = st["mass"][order]
+    r = st["radius"][order]
+    inertia = (np.float32(2.0) * m * r * r) / np.float32(5.0)
+    lam_pos = np.zeros((n, 2), np.float32)
+    lam_pos[:, 0] = np.float32(1.0 / n)
+    lam_vel = (m[:, None] * st["vel"][order]).astype(np.float32)
+    lam_om = (inertia * st["omega"][order]).astype(np.float32)
+    dp, dv, dw = (torch.from_numpy(a).cuda() for a in (lam_pos, lam_vel, lam_om))
+    grad = (C.c_double * 7)()
+    torch.cuda.synchronize()
+    e2.record()
+    D.check(L.dem_adj_backward(sim.handle, dp.data_ptr(), dv.data_ptr(), dw.data_ptr(), grad,
+                               stream))
+    e3.record()
+    torch.cuda.synchronize()
+    bwd = e2.elapsed_time(e3) / steps
+    sim.check()
+    sim.close()
+    return {"workload": "differentiable: %d disks (radii U[0.9, 1.1] mm) released from a seeded "
+                        "heap onto a 20-degree incline, %d steps, checkpoint every %d steps"
+                        % (n, steps, every),
+            "plain_forward_ms_per_step": plain, "checkpointing_forward_ms_per_step": fwd,
+            "backward_ms_per_step": bwd, "backward_over_forward": bwd / plain,
+            "forward_plus_backward_over_forward": (fwd + bwd) / plain,
+            "coefficient_gradients": list(grad),
+            "finite": bool(np.all(np.isfinite(list(grad))) and
+                           torch.isfinite(dv).all().item())}
+
+
 # ------------------------------------------------------------------ our arm
 def main():
     ap = argparse.ArgumentParser()
@@ -291,6 +362,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -431,6 +503,13 @@ def main():
         except Exception as e:  # reported beside the headline, never instead of it
             batched = {"error": str(e)}
 
+    adjoint = None
+    if rank == 0 and world == 1 and not args.no_adjoint:
+        try:
+            adjoint = measure_adjoint()
+        except Exception as e:  # reported beside the headline, never instead of it
+            adjoint = {"error": str(e)}
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
@@ -446,6 +525,7 @@ def main():
                                "achieved_gbs": whole_bytes / (step_ms * 1e-3) / 1e9,
                                "frac": whole_bytes / (step_ms * 1e-3) / 1e9 / hbm},
                 "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "batched": batched,
+                "adjoint": adjoint,
                 "gpu_launches": kernels_per_step * args.steps,
                 "kernels_per_step": kernels_per_step}
         print(json.dumps(line), flush=True)

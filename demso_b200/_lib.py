@@ -17,6 +17,7 @@ STATUS = {0: "DEM_OK", 1: "DEM_ERR_INVALID_ARG", 2: "DEM_ERR_CUDA", 3: "DEM_ERR_
 CTX_PRESSURE = 1
 CTX_ACCEL = 2
 NUM_STAGES = 3  # DEM_NUM_STAGES: sort, reorder, collide + integrate
+ADJ_NUM_COEF = 7  # DEM_ADJ_NUM_COEF
 
 
 class DemError(RuntimeError):
@@ -69,6 +70,8 @@ SIGNATURES = [
     ("dem_get_followed", C.c_int, [_P, _P, _U, _P, _P]),
     ("dem_profile_begin", C.c_int, [_P, _U]),
     ("dem_profile_end", C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(_U)]),
+    ("dem_adj_forward", C.c_int, [_P, _U, _U, _P]),
+    ("dem_adj_backward", C.c_int, [_P, _P, _P, _P, C.POINTER(C.c_double), _P]),
     ("dem_scene_rsa", C.c_int, [_U, _P, C.c_float, C.c_float, C.c_uint64, _U, _U, _P,
                                 C.POINTER(_U)]),
 ]

@@ -319,6 +319,11 @@ struct DemContext {
     bool profiling = false;
     cudaEvent_t* evPool = nullptr;
     uint32_t evCap = 0, evUsed = 0, stepsProfiled = 0;
+    // adjoint: checkpoints of the state every adjEvery steps of the last
+    // dem_adj_forward (pos, vel, theta, omega, radius, mass, id per slot)
+    void* adjCheck = nullptr;
+    size_t adjCheckBytes = 0;
+    uint32_t adjSteps = 0, adjEvery = 0, adjWindows = 0;
 };
 
 namespace {
@@ -640,6 +645,7 @@ extern "C" int dem_destroy(DemContext* c) {
     if (c->capStream) cudaStreamDestroy(c->capStream);
     if (c->bodyStream) cudaStreamDestroy(c->bodyStream);
     cudaFree(c->followRows);
+    cudaFree(c->adjCheck);
     cudaFree(c->dTable);
     cudaFree(c->spec);
     cudaFree(c->incScratch);
@@ -889,5 +895,184 @@ extern "C" int dem_profile_end(DemContext* c, float* ms, uint32_t* steps) {
         for (int k = 0; k < DEM_NUM_STAGES; ++k) ms[k] = acc[k];
     if (steps) *steps = c->stepsProfiled;
     drop_profile(c);
+    return DEM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// adjoint
+// ---------------------------------------------------------------------------
+namespace {
+
+size_t snapshot_bytes(uint32_t n) { return al256(8ull * n) * 2 + al256(4ull * n) * 5; }
+
+struct Snapshot {
+    float *pos, *vel, *theta, *omega, *radius, *mass;
+    uint32_t* id;
+};
+
+Snapshot carve_snapshot(void* base, uint32_t n) {
+    char* p = static_cast<char*>(base);
+    Snapshot s;
+    s.pos = reinterpret_cast<float*>(p); p += al256(8ull * n);
+    s.vel = reinterpret_cast<float*>(p); p += al256(8ull * n);
+    s.theta = reinterpret_cast<float*>(p); p += al256(4ull * n);
+    s.omega = reinterpret_cast<float*>(p); p += al256(4ull * n);
+    s.radius = reinterpret_cast<float*>(p); p += al256(4ull * n);
+    s.mass = reinterpret_cast<float*>(p); p += al256(4ull * n);
+    s.id = reinterpret_cast<uint32_t*>(p);
+    return s;
+}
+
+// One step as dem_step takes it; with `rec`, the sorted state, cell ranges
+// and accelerations of the step are copied there.
+int step_recorded(DemContext* c, cudaStream_t st, char* rec) {
+    const int p = c->cur, b = c->cur ^ 1;
+    const int kind = c->haveOrder ? 1 : 0;
+    DEM_TRY_CUDA(cudaGraphLaunch(c->sortGraph[kind][p], st), "graph launch");
+    const uint32_t n = c->n;
+    if (rec) {
+        char* q = rec;
+        auto cp = [&](const void* src, size_t bytes, size_t slot) -> cudaError_t {
+            cudaError_t e = cudaMemcpyAsync(q, src, bytes, cudaMemcpyDeviceToDevice, st);
+            q += slot;
+            return e;
+        };
+        const size_t s8 = al256(8ull * n), s4 = al256(4ull * n);
+        // layout of carve_step: pos, vel, acc, spare, omega, radius, mass, alpha, id, cells
+        DEM_TRY_CUDA(cp(c->dyn[1].pos, 8ull * n, s8), "record");
+        DEM_TRY_CUDA(cp(c->dyn[1].vel, 8ull * n, s8), "record");
+        q += s8 + s8;  // acc (after the step), spare
+        DEM_TRY_CUDA(cp(c->dyn[1].omega, 4ull * n, s4), "record");
+        DEM_TRY_CUDA(cp(c->stat[b].radius, 4ull * n, s4), "record");
+        DEM_TRY_CUDA(cp(c->stat[b].mass, 4ull * n, s4), "record");
+        q += s4;  // alpha (after the step)
+        DEM_TRY_CUDA(cp(c->stat[b].id, 4ull * n, s4), "record");
+        DEM_TRY_CUDA(cp(c->cells[b], 8ull * c->numCells, al256(8ull * c->numCells)), "record");
+    }
+    DEM_TRY_CUDA(cudaGraphLaunch(c->stepGraph[p], st), "graph launch");
+    if (rec) {
+        const size_t s8 = al256(8ull * n), s4 = al256(4ull * n);
+        DEM_TRY_CUDA(cudaMemcpyAsync(rec + 2 * s8, c->acc, 8ull * n, cudaMemcpyDeviceToDevice, st),
+                     "record");
+        DEM_TRY_CUDA(cudaMemcpyAsync(rec + 4 * s8 + 3 * s4, c->alpha, 4ull * n,
+                                     cudaMemcpyDeviceToDevice, st),
+                     "record");
+    }
+    c->cur ^= 1;
+    c->haveOrder = true;
+    return DEM_OK;
+}
+
+bool has_attraction_host(const KParams& P) {
+    for (uint32_t m = 0; m < P.nmat; ++m)
+        if (P.at[m] != 0.0f) return true;
+    return false;
+}
+
+int adj_check_context(DemContext* c) {
+    if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    if (c->nspec) return fail(DEM_ERR_INVALID_ARG, "the adjoint takes a single scene, not a batch");
+    if (c->typed) return fail(DEM_ERR_INVALID_ARG, "the adjoint takes a single material");
+    if (!(c->flags & DEM_CTX_ACCEL)) return fail(DEM_ERR_INVALID_ARG, "create the context with DEM_CTX_ACCEL");
+    if (c->sys.gridSize[0] < 3 || c->sys.gridSize[1] < 3)
+        return fail(DEM_ERR_INVALID_ARG, "the adjoint needs at least 3 cells per axis");
+    if (has_attraction_host(c->P)) return fail(DEM_ERR_INVALID_ARG, "the adjoint has no attraction law");
+    return DEM_OK;
+}
+
+}  // namespace
+
+extern "C" int dem_adj_forward(DemContext* c, uint32_t nsteps, uint32_t every, void* stream) {
+    int rc = adj_check_context(c);
+    if (rc) return rc;
+    if (nsteps == 0 || every == 0) return fail(DEM_ERR_INVALID_ARG, "nsteps and every must be > 0");
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint32_t windows = (nsteps + every - 1) / every;
+    const size_t snap = snapshot_bytes(c->n);
+    if (c->adjCheckBytes < snap * windows) {
+        cudaFree(c->adjCheck);
+        c->adjCheck = nullptr;
+        c->adjCheckBytes = 0;
+        DEM_TRY_CUDA(cudaMalloc(&c->adjCheck, snap * windows), "cudaMalloc checkpoints");
+        c->adjCheckBytes = snap * windows;
+    }
+    for (uint32_t w = 0; w < windows; ++w) {
+        Snapshot s = carve_snapshot(static_cast<char*>(c->adjCheck) + snap * w, c->n);
+        rc = dem_get_state(c, s.pos, s.vel, s.theta, s.omega, s.radius, s.mass, s.id, nullptr,
+                           nullptr, nullptr, nullptr, nullptr, 0, stream);
+        if (rc) return rc;
+        const uint32_t k = std::min(every, nsteps - w * every);
+        rc = dem_step(c, k, stream);
+        if (rc) return rc;
+    }
+    DEM_TRY_CUDA(cudaStreamSynchronize(st), "adjoint forward");
+    c->adjSteps = nsteps;
+    c->adjEvery = every;
+    c->adjWindows = windows;
+    return DEM_OK;
+}
+
+extern "C" int dem_adj_backward(DemContext* c, float* lamPos, float* lamVel, float* lamOmega,
+                                double* grad, void* stream) {
+    int rc = adj_check_context(c);
+    if (rc) return rc;
+    if (!c->adjWindows) return fail(DEM_ERR_INVALID_ARG, "run dem_adj_forward first");
+    if (!lamPos || !lamVel || !lamOmega || !grad) return fail(DEM_ERR_INVALID_ARG, "NULL buffer");
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint32_t n = c->n;
+    const size_t stepBytes = adj_step_bytes(n, c->numCells);
+    const uint32_t pblocks = adj_partial_blocks(n);
+    const size_t tmpBytes = 2 * al256(8ull * n) + 2 * al256(4ull * n) + al256(8ull * n) +
+                            al256(8ull * DEM_ADJ_NUM_COEF * pblocks) + 256;
+    char* rec = nullptr;
+    char* tmp = nullptr;
+    DEM_TRY_CUDA(cudaMalloc(&rec, stepBytes * c->adjEvery), "cudaMalloc adjoint record");
+    cudaError_t e = cudaMalloc(&tmp, tmpBytes);
+    if (e != cudaSuccess) {
+        cudaFree(rec);
+        return cuda_fail(e, "cudaMalloc adjoint scratch");
+    }
+    char* q = tmp;
+    float2* tlx = reinterpret_cast<float2*>(q); q += al256(8ull * n);
+    float2* tlv = reinterpret_cast<float2*>(q); q += al256(8ull * n);
+    float* tlw = reinterpret_cast<float*>(q); q += al256(4ull * n);
+    float* lamM = reinterpret_cast<float*>(q); q += al256(4ull * n);
+    float2* lamF = reinterpret_cast<float2*>(q); q += al256(8ull * n);
+    double* partial = reinterpret_cast<double*>(q); q += al256(8ull * DEM_ADJ_NUM_COEF * pblocks);
+    double* sum = reinterpret_cast<double*>(q);
+    rc = DEM_OK;
+    e = cudaMemsetAsync(partial, 0, 8ull * DEM_ADJ_NUM_COEF * pblocks, st);
+    const size_t snap = snapshot_bytes(n);
+    for (int w = (int)c->adjWindows - 1; w >= 0 && rc == DEM_OK && e == cudaSuccess; --w) {
+        Snapshot s = carve_snapshot(static_cast<char*>(c->adjCheck) + snap * w, n);
+        rc = dem_set_state(c, n, s.pos, s.vel, s.theta, s.omega, s.radius, s.mass, s.id, nullptr,
+                           0, stream);
+        if (rc) break;
+        const uint32_t k = std::min(c->adjEvery, c->adjSteps - (uint32_t)w * c->adjEvery);
+        if (!c->keysValid) {
+            e = launch_calc_hash(c->P, c->dyn[0].pos, c->keys, nullptr, n, st);
+            c->keysValid = true;
+            c->haveOrder = false;
+        }
+        for (int pp = 0; pp < 2 && rc == DEM_OK; ++pp) {
+            for (int kk = 0; kk < 2 && rc == DEM_OK; ++kk)
+                if (!c->sortGraph[kk][pp]) rc = build_graph(c, kk, pp);
+            if (rc == DEM_OK && !c->stepGraph[pp]) rc = build_graph(c, 2, pp);
+        }
+        for (uint32_t t = 0; t < k && rc == DEM_OK; ++t) rc = step_recorded(c, st, rec + stepBytes * t);
+        for (int t = (int)k - 1; t >= 0 && rc == DEM_OK && e == cudaSuccess; --t)
+            e = adj_backward_step(c->P, rec + stepBytes * t, n, c->numCells,
+                                  reinterpret_cast<float2*>(lamPos),
+                                  reinterpret_cast<float2*>(lamVel), lamOmega, tlx, tlv, tlw, lamF,
+                                  lamM, partial, st);
+    }
+    if (rc == DEM_OK && e == cudaSuccess) e = adj_sum_coef(partial, n, sum, st);
+    if (rc == DEM_OK && e == cudaSuccess)
+        e = cudaMemcpyAsync(grad, sum, 8ull * DEM_ADJ_NUM_COEF, cudaMemcpyDeviceToHost, st);
+    if (rc == DEM_OK && e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(rec);
+    cudaFree(tmp);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint backward");
     return DEM_OK;
 }

@@ -86,4 +86,13 @@ cudaError_t launch_reorder_packed(uint2* cellRange, DynSet sorted, StatSet sorte
 cudaError_t launch_unpack_cells(const uint2* cellRange, uint32_t numCells, uint32_t* cellStart,
                                 uint32_t* cellEnd, cudaStream_t st);
 
+// Adjoint (dem_adjoint.cu).
+size_t adj_step_bytes(uint32_t n, uint32_t numCells);
+cudaError_t adj_backward_step(const KParams& P, void* recBase, uint32_t n, uint32_t numCells,
+                              float2* lamX, float2* lamV, float* lamW, float2* tlx, float2* tlv,
+                              float* tlw, float2* lamF, float* lamM, double* coefPartial,
+                              cudaStream_t st);
+cudaError_t adj_sum_coef(const double* partial, uint32_t n, double* out, cudaStream_t st);
+uint32_t adj_partial_blocks(uint32_t n);
+
 }  // namespace dem

@@ -273,3 +273,29 @@ def concat_specimens(specimens):
                   np.concatenate([t if t is not None else np.zeros(sc.n, np.uint32)
                                   for t, sc in zip(types, specimens)]))
     return st
+
+
+def incline_heap(n=16384, seed=0, slope_deg=20.0, vel_std=0.05, phi=0.5, dt=2e-6,
+                 kn=1e5, zeta=0.3, mu=0.5):
+    """Differentiable workload: n disks (radii U[0.9, 1.1] mm) in a seeded
+    heap -- random sequential placement at area fraction `phi` in a
+    rectangle twice as wide as high at the bottom-left of a walled box three
+    times as wide and twice as high -- with initial velocities N(0, vel_std^2)
+    and gravity rotated by `slope_deg`, so that the floor is a wall inclined
+    at that angle in the frame of gravity."""
+    rng = np.random.default_rng(seed)
+    r = rng.uniform(0.9e-3, 1.1e-3, size=n).astype(np.float32)
+    area = n * math.pi * float(np.mean(r.astype(np.float64) ** 2)) / phi
+    h = math.sqrt(area / 2.0)
+    w = 2.0 * h
+    pos = rsa_positions(r, w, h, seed=seed + 7, strips=max(1, int(h / 0.02)))
+    Lx, Ly = 3.0 * w, 2.0 * h
+    vel = rng.normal(0.0, vel_std, size=(n, 2))
+    a = math.radians(slope_deg)
+    rmax = 1.1e-3
+    mat = pair_material(kn=kn, zeta=zeta, mu=mu)
+    sys = System(Lx=Lx, Ly=Ly, gx=grid_2r(Lx, rmax), gy=grid_2r(Ly, rmax), dt=dt,
+                 gravity=(9.81 * math.sin(a), -9.81 * math.cos(a)),
+                 knWall=mat.normalStiffness, ktWall=mat.shearStiffness, materials=[mat])
+    order = np.argsort(cell_hash(pos, sys), kind="stable")
+    return _finish(sys, pos[order], vel[order], r[order], name="incline_heap_%d" % n)

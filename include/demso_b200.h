@@ -243,6 +243,34 @@ int dem_profile_begin(DemContext* ctx, uint32_t maxSteps);
 int dem_profile_end(DemContext* ctx, float* ms, uint32_t* steps);
 
 /* ---------------------------------------------------------------------------
+ * Adjoint (no counterpart in the reference): reverse-mode gradients of a
+ * scalar loss of the final state with respect to the initial state and the
+ * contact coefficients, for a single-material scene (not a batch) created
+ * with DEM_CTX_ACCEL and at least 3 cells per axis.
+ *
+ * dem_adj_forward runs nsteps steps exactly as dem_step and keeps the state
+ * every `every` steps (device memory held by the context).  The caller then
+ * reads the final state, forms the loss cotangents and calls
+ * dem_adj_backward, which re-runs each window from its checkpoint while
+ * recording it and reverses its steps.  The branch taken by every contact,
+ * wall and floor contact in the forward is kept in the reverse ("frozen"
+ * contact set).  lamPos/lamVel/lamOmega are device arrays in particle-id
+ * order: on entry the cotangents of the final pos (2n), vel (2n) and omega
+ * (n), on return those of the initial state.  grad (host, DEM_ADJ_NUM_COEF
+ * doubles) receives dL/d of: pair normal stiffness, pair shear stiffness,
+ * pair dashpot, pair friction (the series/mean values of
+ * particles_kernel.cuh:269-275), then the floor's dashpot (the material's
+ * normalDamping), friction and series shear stiffness
+ * (particles_kernel.cuh:419-421).  Coefficient sums are in double.  After
+ * dem_adj_backward the context holds the state at the end of the first
+ * window; set the state again before stepping on.
+ * ------------------------------------------------------------------------- */
+#define DEM_ADJ_NUM_COEF 7
+int dem_adj_forward(DemContext* ctx, uint32_t nsteps, uint32_t every, void* stream);
+int dem_adj_backward(DemContext* ctx, float* lamPos, float* lamVel, float* lamOmega,
+                     double* grad, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Scene generation (host only, no GPU needed)
  * ------------------------------------------------------------------------- */
 

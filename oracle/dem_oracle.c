@@ -20,6 +20,14 @@
 
 typedef struct { REAL x, y; } R2;
 
+/* Branch signature: a running hash of every branch the contact law and the
+ * integrator take (contact, dashpot, slip, walls, floor), so that a finite
+ * difference whose +h and -h runs took different branches can be detected. */
+static uint64_t g_sig = 1469598103934665603ull;
+static inline void sig_mix(uint64_t v) { g_sig = (g_sig ^ v) * 1099511628211ull; }
+void orc_signature_reset(void) { g_sig = 1469598103934665603ull; }
+uint64_t orc_signature(void) { return g_sig; }
+
 static inline R2 r2(REAL x, REAL y) { R2 v; v.x = x; v.y = y; return v; }
 static inline R2 ld2(const REAL* a, uint32_t i) { return r2(a[2 * i], a[2 * i + 1]); }
 static inline void st2(REAL* a, uint32_t i, R2 v) { a[2 * i] = v.x; a[2 * i + 1] = v.y; }
@@ -171,6 +179,7 @@ static R2 collide_spheres(const Sys* s, R2 pA, R2 pB, R2 vA, R2 vB, REAL wA, REA
             force.y += c * nrm.y;
         }
         *pressure = (float)((double)*pressure + (double)len2(force) / (4 * M_PI * rA * rA));
+        uint64_t br = 1u | (vn < 0 ? 2u : 0u);
         if (mu != 0.0) {
             REAL sw = rA * wA + rB * wB;
             R2 vc = r2(vt.x - sw * tng.x, vt.y - sw * tng.y);
@@ -182,11 +191,13 @@ static R2 collide_spheres(const Sys* s, R2 pA, R2 pB, R2 vA, R2 vB, REAL wA, REA
             } else {
                 REAL l = len2(vc);
                 ft = r2(ftmax * vc.x / l, ftmax * vc.y / l);
+                br |= 4u;
             }
             force.x += ft.x;
             force.y += ft.y;
             *moment += rA * dot2(ft, tng);
         }
+        sig_mix(br);
     }
     return force;
 }
@@ -320,10 +331,13 @@ void orc_integrate(const OrcSystem* os, uint32_t n, REAL* pos, REAL* vel, const 
         REAL r = radius[i];
         uint32_t mi = mat_of(type, i);
         REAL eb = s.eb[mi];
-        if (p.x > s.Lx - r) { p.x = s.Lx - r; v.x *= -eb; }
-        if (p.x < r) { p.x = r; v.x *= -eb; }
-        if (p.y > s.Ly - r) { p.y = s.Ly - r; v.y *= -eb; }
+        uint64_t wb = 0;
+        if (p.x > s.Lx - r) { p.x = s.Lx - r; v.x *= -eb; wb |= 1u; }
+        if (p.x < r) { p.x = r; v.x *= -eb; wb |= 2u; }
+        if (p.y > s.Ly - r) { p.y = s.Ly - r; v.y *= -eb; wb |= 4u; }
+        if (wb) sig_mix(0x100u | wb);
         if (p.y < r) {
+            sig_mix(0x200u | ((uint64_t)i << 12));
             REAL wa = 0;
             R2 aw = collide_floor(&s, p, v, w, r, mass[i], mi, &wa, &pressure[i]);
             v.x += aw.x * s.dt;

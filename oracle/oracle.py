@@ -5,11 +5,13 @@ reference arms import this module, and only as the checker or the timed CPU
 baseline.  The product path (the ``demso_b200`` package and its CUDA
 library) never imports or calls anything here.
 
-Two oracles are wrapped:
+Three oracles are wrapped:
 
 * ``PortOracle`` -- ``dem_oracle.c``, our CPU restatement of the reference's
   step (particles_kernel.cuh / functions.cu / main.cu), in float
   (``libdem_oracle_f32.so``) or double (``libdem_oracle_f64.so``).
+* ``TangentOracle`` -- ``dem_tangent.cpp``, the forward-mode derivative of
+  the same step (the FP64 oracle of the adjoint).
 * ``RefHarness`` -- ``_ref/libdemso_ref.so``, the reference's own
   ``src/particles_kernel.cuh`` compiled for the host by oracle/Makefile (only
   when the reference tree was present at build time).
@@ -129,6 +131,7 @@ class PortOracle:
         L.orc_collide.argtypes = [sp, u32, rp, rp, rp, rp, rp, C.c_void_p, _u32p, _u32p,
                                   rp, rp, _f32p]
         L.orc_integrate.argtypes = [sp, u32, rp, rp, rp, rp, rp, rp, rp, rp, C.c_void_p, _f32p]
+        L.orc_signature.restype = C.c_uint64
         L.orc_step.argtypes = [sp, u32] + [rp] * 6 + [_u32p, C.c_void_p] + [rp] * 6 + \
             [_u32p, _u32p, C.c_void_p] + [rp, rp, _f32p, _u32p, _u32p, _u32p, _u32p]
 
@@ -215,7 +218,10 @@ class PortOracle:
 
     def run(self, sys: System, st: dict, nsteps: int):
         """`nsteps` full steps; returns the final sorted state dict plus
-        acc/alpha/pressure/cellStart/cellEnd/hash/index of the last step."""
+        acc/alpha/pressure/cellStart/cellEnd/hash/index of the last step, and
+        `signature`, a hash of every branch the contact law and the
+        integrator took."""
+        self.lib.orc_signature_reset()
         a = {k: self._r(st[k]).copy() for k in ("pos", "vel", "theta", "omega", "radius", "mass")}
         n = a["pos"].shape[0]
         a["id"] = np.ascontiguousarray(st["id"], dtype=np.uint32).copy()
@@ -244,7 +250,55 @@ class PortOracle:
                 acc.reshape(-1), alpha, pr, h, ix, cs, ce)
             a, b = b, a
         out = dict(a)
-        out.update(acc=acc, alpha=alpha, pressure=pr, cellStart=cs, cellEnd=ce, hash=h, index=ix)
+        out.update(acc=acc, alpha=alpha, pressure=pr, cellStart=cs, cellEnd=ce, hash=h, index=ix,
+                   signature=int(self.lib.orc_signature()))
+        return out
+
+
+class TangentOracle:
+    """Forward-mode tangent of the oracle step (dem_tangent.cpp) in float or
+    double: the oracle's trajectory, bit-identical to ``PortOracle`` at the
+    same precision, plus its exact derivatives along up to four seeded
+    directions (the derivative with every branch held as taken)."""
+
+    DIRECTIONS = 4
+
+    def __init__(self, precision: str = "f64"):
+        if precision not in ("f32", "f64"):
+            raise ValueError(precision)
+        path = os.path.join(OUT, "libdem_tangent_%s.so" % precision)
+        if not os.path.isfile(path):
+            build()
+        self.lib = C.CDLL(path)
+        u32 = C.c_uint32
+        self.lib.tan_run.argtypes = [C.POINTER(_OrcSystem), u32, u32] + [_f64p] * 6 + [_u32p] + \
+            [_f64p] * 5 + [C.POINTER(C.c_uint64)]
+        self.lib.tan_run.restype = C.c_int
+
+    def run(self, sys: System, st: dict, nsteps: int, dmat=None, dwall=None, dpos=None,
+            dvel=None, domega=None):
+        """`nsteps` steps from ``st`` with the given tangents (direction-major:
+        dmat (4, 6) over the material row of ``Material.row()``, dwall (4, 2)
+        over (knWall, ktWall), dpos/dvel (4, n, 2), domega (4, n)).  Returns
+        the final sorted state with ``dpos``/``dvel``/``domega`` (final
+        tangents, sorted order) and ``signature``."""
+        K = self.DIRECTIONS
+        f = lambda a: np.ascontiguousarray(a, dtype=np.float64).copy()
+        out = {k: f(st[k]) for k in ("pos", "vel", "theta", "omega", "radius", "mass")}
+        n = out["pos"].shape[0]
+        out["id"] = np.ascontiguousarray(st["id"], dtype=np.uint32).copy()
+        z = lambda shape, a: np.zeros(shape) if a is None else f(np.broadcast_to(a, shape))
+        dmat, dwall = z((K, 6), dmat), z((K, 2), dwall)
+        dpos, dvel, domega = z((K, n, 2), dpos), z((K, n, 2), dvel), z((K, n), domega)
+        sig = C.c_uint64(0)
+        rc = self.lib.tan_run(C.byref(_orc_system(sys)), n, nsteps, out["pos"].reshape(-1),
+                              out["vel"].reshape(-1), out["theta"], out["omega"], out["radius"],
+                              out["mass"], out["id"], dmat.reshape(-1), dwall.reshape(-1),
+                              dpos.reshape(-1), dvel.reshape(-1), domega.reshape(-1),
+                              C.byref(sig))
+        if rc != 0:
+            raise ValueError("the tangent oracle takes one material without attraction")
+        out.update(dpos=dpos, dvel=dvel, domega=domega, signature=int(sig.value))
         return out
 
 
