@@ -41,15 +41,18 @@ sys.path.insert(0, ROOT)
 METRIC = "particle-steps/s at 4M disks"
 UNIT = "particle-steps/s"
 N_DEFAULT = 4194304
-# Algorithmic bytes per particle of the fused collide+integrate+hash kernel:
-# read pos 8, vel 8, theta 4, omega 4, radius 4, mass 4; write pos 8, vel 8,
-# theta 4, omega 4, next hash 4, pressure 4 (neighbours are cache hits); plus
-# 8 bytes per cell (cellStart/cellEnd).
-STEP_KERNEL_BYTES_PER_PARTICLE = 68
+# Algorithmic bytes of the step kernel, which does the collide and integrate
+# stages of the reference step, counted per stage as the reference moves them:
+# collide reads own pos/vel/omega/radius/mass 28 and writes force 8 + torque 4
+# (neighbours are cache hits) = 40 per particle + 8 per cell (cell ranges);
+# integrate reads pos, vel, omega, theta, radius, mass, acc, alpha 44 and writes
+# pos, vel, omega, theta 24 = 68 per particle.  The fused kernel keeps force and
+# torque in registers, so its own minimum is 68 per particle (reported beside).
+STEP_KERNEL_BYTES_PER_PARTICLE = 108
 STEP_KERNEL_BYTES_PER_CELL = 8
-# Per-stage algorithmic bytes for the other stages: sort = 4 + 16 * passes
-# per particle (+ the per-tile histograms), reorder = key+index 8, gather 36,
-# write 36, loc 4 per particle + 12 per cell.
+FUSED_MIN_BYTES_PER_PARTICLE = 68
+# Whole step, per particle: hash 16 + sort 52 + reorder 84 + collide 40 +
+# integrate 68 = 260, plus 20 per cell (reorder 12, collide 8).
 WHOLE_STEP_BYTES = lambda n, c: 260.0 * n + 20.0 * c  # whole-step model, per step
 
 
@@ -363,6 +366,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--direct", action="store_true",
+                    help="launch each kernel directly instead of through CUDA graphs "
+                         "(for per-kernel profilers; one host read-back per step)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -389,7 +395,8 @@ def main():
 
     sc = scenes.plain_at_scale(args.n, seed=rank)
     n = sc.n
-    sim = D.Simulation(sc.sys, capacity=n, flags=D.CTX_PRESSURE)
+    sim = D.Simulation(sc.sys, capacity=n,
+                       flags=D.CTX_PRESSURE | (D.CTX_DIRECT if args.direct else 0))
     pin = lambda a: torch.from_numpy(a.view(np.int32) if a.dtype == np.uint32 else a).pin_memory()
     host = {k: pin(getattr(sc, k)) for k in ("pos", "vel", "theta", "omega", "radius", "mass",
                                               "id")}
@@ -514,11 +521,15 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f32", "data": "synthetic", "config": config_dict(n, sc),
+                "dtype": "f32", "data": "synthetic", "config": dict(config_dict(n, sc), launch="direct, no graphs" if args.direct
+                               else "two CUDA graphs per step"),
                 "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved,
                              "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                              "peak_kind": kind, "traffic": traffic,
-                             "bytes_per_launch": bytes_launch},
+                             "bytes_per_launch": bytes_launch,
+                             "fused_minimum_frac": (FUSED_MIN_BYTES_PER_PARTICLE * n
+                                                    / (stage_ms[dom] * 1e-3) / 1e9 / hbm
+                                                    if dom == 2 else None)},
                 "stage_ms_per_step": {"sort_reorder": stage_ms[0],
                                       "collide_integrate": stage_ms[2]},
                 "whole_step": {"model_bytes_per_step": whole_bytes,

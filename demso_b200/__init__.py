@@ -19,11 +19,11 @@ from dataclasses import dataclass, field
 from typing import Optional, Sequence
 
 from . import _lib
-from ._lib import CTX_ACCEL, CTX_PRESSURE, DEM_MAX_MATERIALS, DemError, check, load
+from ._lib import CTX_ACCEL, CTX_DIRECT, CTX_PRESSURE, DEM_MAX_MATERIALS, DemError, check, load
 
 __all__ = ["Material", "System", "DemError", "calcHash", "sortParticles",
            "reorderDataAndFindCellStart", "collide", "integrateSystem", "Simulation", "Batch",
-           "sort_scratch_bytes", "load", "CTX_PRESSURE", "CTX_ACCEL"]
+           "sort_scratch_bytes", "load", "CTX_PRESSURE", "CTX_ACCEL", "CTX_DIRECT"]
 
 
 @dataclass

@@ -16,6 +16,7 @@ STATUS = {0: "DEM_OK", 1: "DEM_ERR_INVALID_ARG", 2: "DEM_ERR_CUDA", 3: "DEM_ERR_
           4: "DEM_ERR_TIMEOUT", 5: "DEM_ERR_NO_MEMORY", 6: "DEM_ERR_CAPACITY"}
 CTX_PRESSURE = 1
 CTX_ACCEL = 2
+CTX_DIRECT = 4
 NUM_STAGES = 3  # DEM_NUM_STAGES: sort, reorder, collide + integrate
 ADJ_NUM_COEF = 7  # DEM_ADJ_NUM_COEF
 

@@ -750,6 +750,40 @@ extern "C" int dem_get_state(DemContext* c, float* pos, float* vel, float* theta
     return DEM_OK;
 }
 
+// DEM_CTX_DIRECT: the same kernels launched one by one, the sort path
+// (incremental, or full after a mover overflow) read back on the host each
+// step instead of chosen on the device by conditional graph nodes, so that
+// per-kernel profilers see every launch.
+int step_direct(DemContext* c, uint32_t nsteps, cudaStream_t st) {
+    for (uint32_t s = 0; s < nsteps; ++s) {
+        const int a = c->cur;
+        bool full = !c->haveOrder;
+        if (!full) {
+            uint32_t need = 0;
+            DEM_TRY_CUDA(cudaMemcpyAsync(&need, c->inc.ctrl + kCtrlNeedFull, 4,
+                                         cudaMemcpyDeviceToHost, st),
+                         "read sort path");
+            DEM_TRY_CUDA(cudaStreamSynchronize(st), "sync");
+            full = need != 0u;
+        }
+        const bool prof = c->profiling && c->evUsed + 3 <= c->evCap;
+        cudaEvent_t* ev = prof ? c->evPool + c->evUsed : nullptr;
+        if (prof) DEM_TRY_CUDA(cudaEventRecord(ev[0], st), "profile event");
+        DEM_TRY_CUDA(full ? enqueue_full_sort(c, a, st, nullptr) : enqueue_inc_sort(c, a, st, nullptr),
+                     "sort phase");
+        if (prof) DEM_TRY_CUDA(cudaEventRecord(ev[1], st), "profile event");
+        DEM_TRY_CUDA(enqueue_step_kernel(c, st, nullptr), "step kernel");
+        if (prof) {
+            DEM_TRY_CUDA(cudaEventRecord(ev[2], st), "profile event");
+            c->evUsed += 3;
+            ++c->stepsProfiled;
+        }
+        c->cur ^= 1;
+        c->haveOrder = true;
+    }
+    return DEM_OK;
+}
+
 extern "C" int dem_step(DemContext* c, uint32_t nsteps, void* stream) {
     if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
     if (nsteps == 0 || c->n == 0) return DEM_OK;
@@ -765,6 +799,7 @@ extern "C" int dem_step(DemContext* c, uint32_t nsteps, void* stream) {
         c->keysValid = true;
         c->haveOrder = false;
     }
+    if (c->flags & DEM_CTX_DIRECT) return step_direct(c, nsteps, st);
     for (int p = 0; p < 2; ++p) {
         for (int k = 0; k < 2; ++k)
             if (!c->sortGraph[k][p]) {

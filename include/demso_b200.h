@@ -166,6 +166,8 @@ typedef struct DemContext DemContext;
 /* Flags for dem_create. */
 #define DEM_CTX_PRESSURE 1u   /* maintain the pressure diagnostic (as the reference does) */
 #define DEM_CTX_ACCEL 2u      /* also store acc/alpha of the last step (output rows) */
+#define DEM_CTX_DIRECT 4u     /* launch each kernel directly instead of through CUDA graphs
+                                 (one host read-back per step; for per-kernel profiling) */
 
 int dem_create(const DemSystem* sys, uint32_t capacity, uint32_t flags, DemContext** out);
 int dem_destroy(DemContext* ctx);
