@@ -7,11 +7,23 @@ namespace dem {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kCellItems = 16;
-constexpr uint32_t kCellChunk = kThreads * kCellItems;  // cells per scan block
+constexpr uint32_t kMinCellItems = 2;
 constexpr int kTopThreads = 1024;
 constexpr int kTopItems = 8;
+constexpr uint32_t kMaxScanBlocks = kTopThreads * kTopItems;
 
+// Cells per thread of the cell scan: 2, or the smallest power of two that
+// keeps the number of scan blocks within what cells_top_kernel scans.
+inline uint32_t cell_items(uint32_t numCells) {
+    uint32_t items = kMinCellItems;
+    while ((size_t)numCells > (size_t)kMaxScanBlocks * kThreads * items && items < (1u << 20))
+        items <<= 1;
+    return items;
+}
+inline size_t cell_blocks(uint32_t numCells) {
+    const size_t chunk = (size_t)kThreads * cell_items(numCells);
+    return (numCells + chunk - 1) / chunk;
+}
 inline unsigned blocks_for(size_t n, int t) { return (unsigned)((n + (size_t)t - 1) / (size_t)t); }
 inline size_t al256(size_t b) { return (b + 255u) & ~(size_t)255u; }
 
@@ -72,13 +84,13 @@ __device__ __forceinline__ unsigned long long cell_counts(const uint2* __restric
 
 __global__ void __launch_bounds__(kThreads)
 cells_reduce_kernel(const uint2* __restrict__ prevCells, const uint32_t* __restrict__ leavers,
-                    const uint32_t* __restrict__ arrCnt, uint32_t numCells,
+                    const uint32_t* __restrict__ arrCnt, uint32_t numCells, uint32_t items,
                     unsigned long long* __restrict__ partials) {
     __shared__ unsigned long long warpTot[kThreads / 32];
-    const size_t base = (size_t)blockIdx.x * kCellChunk;
+    const size_t base = (size_t)blockIdx.x * kThreads * items;
     unsigned long long s = 0;
-#pragma unroll 4
-    for (int k = 0; k < kCellItems; ++k) {
+#pragma unroll 2
+    for (uint32_t k = 0; k < items; ++k) {
         const size_t c = base + (size_t)k * kThreads + threadIdx.x;
         if (c < numCells) s += cell_counts(prevCells, leavers, arrCnt, (uint32_t)c);
     }
@@ -107,20 +119,21 @@ cells_top_kernel(unsigned long long* __restrict__ partials, uint32_t np) {
     }
 }
 
-// New ranges, stayer bases and arrival bases of a tile of kCellChunk cells,
-// processed in kCellItems block-wide slabs so every access is coalesced; the
+// New ranges, stayer bases and arrival bases of a tile of kThreads * items
+// cells, processed in `items` block-wide slabs so every access is coalesced; the
 // per-cell counters are cleared for the next step.
 __global__ void __launch_bounds__(kThreads)
 cells_apply_kernel(const uint2* __restrict__ prevCells, uint32_t* __restrict__ leavers,
                    uint32_t* __restrict__ arrCnt, uint32_t* __restrict__ arrLo,
-                   uint32_t numCells, const unsigned long long* __restrict__ partials,
+                   uint32_t numCells, uint32_t items,
+                   const unsigned long long* __restrict__ partials,
                    uint2* __restrict__ newCells, uint32_t* __restrict__ stayBase,
                    uint2* __restrict__ arrInfo) {
     __shared__ unsigned long long warpTot[kThreads / 32];
-    const size_t base = (size_t)blockIdx.x * kCellChunk;
+    const size_t base = (size_t)blockIdx.x * kThreads * items;
     unsigned long long carry = partials[blockIdx.x];
 #pragma unroll 1
-    for (int k = 0; k < kCellItems; ++k) {
+    for (uint32_t k = 0; k < items; ++k) {
         const size_t c = base + (size_t)k * kThreads + threadIdx.x;
         const bool valid = c < numCells;
         uint32_t occ = 0, lv = 0, ac = 0, lo = 0;
@@ -263,7 +276,7 @@ size_t incsort_bytes(uint32_t n, uint32_t numCells, uint32_t* moverCapOut) {
     const uint32_t cap = std::max<uint32_t>(4096u, n / 8u);
     if (moverCapOut) *moverCapOut = cap;
     const size_t cells = al256(4ull * numCells);
-    const size_t np = (numCells + kCellChunk - 1) / kCellChunk;
+    const size_t np = cell_blocks(numCells);
     return 4 * cells + al256(8ull * numCells) + al256(16ull * cap) + al256(4ull * cap) +
            al256(8ull * std::max<size_t>(np, 1)) + 256;
 }
@@ -273,7 +286,7 @@ IncSort carve_incsort(void* base, uint32_t n, uint32_t numCells) {
     s.numCells = numCells;
     incsort_bytes(n, numCells, &s.moverCap);
     const size_t cells = al256(4ull * numCells);
-    const size_t np = (numCells + kCellChunk - 1) / kCellChunk;
+    const size_t np = cell_blocks(numCells);
     char* p = static_cast<char*>(base);
     s.leavers = reinterpret_cast<uint32_t*>(p); p += cells;
     s.arrCnt = reinterpret_cast<uint32_t*>(p); p += cells;
@@ -293,12 +306,15 @@ cudaError_t enqueue_incremental(const IncSort& s, uint32_t n, const uint32_t* ke
                                 StatSet fromS, DynSet to, StatSet toS, uint32_t* loc,
                                 cudaStream_t st, int* launches) {
     const uint32_t C = s.numCells;
-    const unsigned nb = blocks_for(C, kCellChunk);
-    if (nb > (unsigned)(kTopThreads * kTopItems)) return cudaErrorInvalidValue;
-    cells_reduce_kernel<<<nb, kThreads, 0, st>>>(prevCells, s.leavers, s.arrCnt, C, s.partials);
-    cells_top_kernel<<<1, kTopThreads, 0, st>>>(s.partials, nb);
-    cells_apply_kernel<<<nb, kThreads, 0, st>>>(prevCells, s.leavers, s.arrCnt, s.arrLo, C,
-                                                s.partials, newCells, s.stayBase, s.arrInfo);
+    const uint32_t items = cell_items(C);
+    const size_t nb = cell_blocks(C);
+    if (nb > kMaxScanBlocks) return cudaErrorInvalidValue;
+    cells_reduce_kernel<<<(unsigned)nb, kThreads, 0, st>>>(prevCells, s.leavers, s.arrCnt, C,
+                                                           items, s.partials);
+    cells_top_kernel<<<1, kTopThreads, 0, st>>>(s.partials, (uint32_t)nb);
+    cells_apply_kernel<<<(unsigned)nb, kThreads, 0, st>>>(prevCells, s.leavers, s.arrCnt, s.arrLo,
+                                                          C, items, s.partials, newCells,
+                                                          s.stayBase, s.arrInfo);
     const unsigned mb = std::min<unsigned>(blocks_for(s.moverCap, kThreads), 296u);
     arrivals_scatter_kernel<<<mb, kThreads, 0, st>>>(s.movers, s.ctrl, s.moverCap, s.arrInfo,
                                                      s.arrSlots);

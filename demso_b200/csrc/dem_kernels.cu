@@ -211,13 +211,24 @@ __device__ __forceinline__ void collide_one(const KParams& P, uint32_t i, int2 g
 // are consecutive cells, so their particles form one contiguous index
 // interval in sorted order.  A lane walks its (culled) row intervals as one
 // flat loop, so the lanes of a warp run about as many iterations as their
-// own candidates instead of the per-cell maximum over the warp.  The
-// summation order is the reference's: contacts are met in (row, index)
-// order, the cell a contact belongs to is found from the cell boundaries,
-// each row keeps one subtotal per cell and adds them to the force in cell
-// order at the end of the row (an empty or culled cell adds +0, which
-// changes nothing).  Returns false, without touching the outputs, when the
-// visited columns wrap; the caller then uses collide_one.
+// own candidates instead of the per-cell maximum over the warp.
+//
+// Each interval is walked twice, in chunks of 32 candidates: a lean filter
+// sets one bit per candidate whose squared distance is within
+// (rA + rB)^2 (1 + 2e-6) -- a superset of the contacts -- and the contact
+// law then runs on the set bits in increasing index.  The law's own
+// `dist < rA + rB` test rejects the few non-contacts among them with a +0
+// force, which changes no sum, so every contact is met in the same
+// (row, index) order as before.  Keeping the law out of the filter loop
+// means a warp runs it once per contact of its busiest lane rather than once
+// per candidate slot in which any lane has a contact.
+//
+// The summation order is the reference's: the cell a contact belongs to is
+// found from the cell boundaries, each row keeps one subtotal per cell and
+// adds them to the force in cell order at the end of the row (an empty or
+// culled cell adds +0, which changes nothing).  Returns false, without
+// touching the outputs, when the visited columns wrap; the caller then uses
+// collide_one.
 template <bool TYPED>
 __device__ __forceinline__ bool collide_rows(const KParams& P, uint32_t i, int2 g, float2 p,
                                              float2 v, float w, float r, uint32_t mat,
@@ -267,34 +278,43 @@ __device__ __forceinline__ bool collide_rows(const KParams& P, uint32_t i, int2 
         const uint32_t b2 = x1 - x0 >= 2 ? (s2 != 0xffffffffu ? s2 : max(max(e1, e0), a))
                                          : 0xffffffffu;
         float2 f0 = make_float2(0.0f, 0.0f), f1 = f0, f2 = f0;
-        // four candidates per iteration, their loads issued together; indices
-        // past the interval load its last element and are masked off
+        // filter: a bit per candidate that may touch (d2 within (r + rj)^2 (1 + 2e-6));
+        // then the contact law on the set bits in index order
 #pragma unroll 1
-        for (uint32_t j0 = a; j0 < b; j0 += 4) {
-            float2 q[4];
-            float d2[4];
+        for (uint32_t base = a; base < b; base += 32u) {
+            const uint32_t lim = min(b, base + 32u);
+            uint32_t mask = 0u;
+#pragma unroll 1
+            for (uint32_t j0 = base; j0 < lim; j0 += 4) {
+                float2 q[4];
+                float d2[4];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) q[k] = __ldg(pos + min(j0 + k, b - 1));
+                for (int k = 0; k < 4; ++k) q[k] = __ldg(pos + min(j0 + k, lim - 1));
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const float relx = q[k].x - p.x, rely = q[k].y - p.y;
-                d2[k] = relx * relx + rely * rely;
+                for (int k = 0; k < 4; ++k) {
+                    const float relx = q[k].x - p.x, rely = q[k].y - p.y;
+                    d2[k] = relx * relx + rely * rely;
+                }
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const uint32_t j = j0 + k;
+                    if (j < lim && j != i && d2[k] <= reach2) {
+                        const float cd = r + __ldg(radius + j);
+                        if (d2[k] <= cd * cd * 1.000002f) mask |= 1u << (j - base);
+                    }
+                }
             }
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const uint32_t j = j0 + k;
-                if (j >= b || j == i || d2[k] > reach2) continue;
+            while (mask) {
+                const uint32_t j = base + (uint32_t)(__ffs(mask) - 1);
+                mask &= mask - 1u;
                 const float rj = __ldg(radius + j);
                 float4 pc = pc0;
                 if (TYPED) pc = P.pair[mat * P.nmat + __ldg(type + j)];
-                const float cd = r + rj;
-                if (d2[k] <= cd * cd * 1.000002f && sqrtf(d2[k]) < cd) {
-                    const float2 f = pair_force(p, q[k], v, __ldg(vel + j), w, __ldg(omega + j),
-                                                r, rj, pc, P.dt, moment, pr);
-                    if (j >= b2) { f2.x += f.x; f2.y += f.y; }
-                    else if (j >= b1) { f1.x += f.x; f1.y += f.y; }
-                    else { f0.x += f.x; f0.y += f.y; }
-                }
+                const float2 f = pair_force(p, __ldg(pos + j), v, __ldg(vel + j), w, __ldg(omega + j),
+                                            r, rj, pc, P.dt, moment, pr);
+                if (j >= b2) { f2.x += f.x; f2.y += f.y; }
+                else if (j >= b1) { f1.x += f.x; f1.y += f.y; }
+                else { f0.x += f.x; f0.y += f.y; }
             }
         }
         force.x += f0.x; force.y += f0.y;

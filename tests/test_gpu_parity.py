@@ -211,3 +211,14 @@ def test_step_one_million_matches_oracle(f32):
     ref = f32.run(sc.sys, sc.state(), 4)
     for k in FINAL_KEYS:
         assert same(out[k], ref[k]), k
+
+
+def test_step_with_sixteen_million_cells_matches_oracle(f32):
+    """A 4096 x 4096 grid (16.8M cells, more than the cell scan's blocks
+    cover at two cells per thread) with a slow gas, so that the incremental
+    sort runs on such a grid: 30 steps against the oracle."""
+    sc = scenes.agitated_gas(n=30000, seed=23, vel_std=0.2, omega_std=50.0, grid=(4096, 4096))
+    out = gpu_run(sc.sys, sc.state(), 30, chunks=[1, 29])
+    ref = f32.run(sc.sys, sc.state(), 30)
+    for k in FINAL_KEYS:
+        assert same(out[k], ref[k]), k
