@@ -259,6 +259,31 @@ class Simulation:
     def kernels_per_step(self) -> int:
         return int(load().dem_kernels_per_step(self._h))
 
+    # -- adjoint (dem_adj_forward / dem_adj_backward) ------------------------
+    def adjoint_forward(self, nsteps: int, every: int, stream=None) -> None:
+        """`nsteps` steps as ``step``, keeping a checkpoint every `every` steps
+        (needs flags with CTX_ACCEL)."""
+        check(load().dem_adj_forward(self._h, int(nsteps), int(every), _stream(stream)))
+
+    def adjoint_backward(self, lam_pos, lam_vel, lam_omega, stream=None):
+        """Reverse pass of the last ``adjoint_forward``.  lam_* are contiguous
+        float32 CUDA tensors in particle-id order holding the cotangents of
+        the final pos (n, 2), vel (n, 2) and omega (n,); on return they hold
+        those of the initial state.  Returns the coefficient gradients as a
+        (specimens, 7) float64 array: pair normal stiffness, pair shear
+        stiffness, pair dashpot, pair friction, floor dashpot, floor friction,
+        floor shear stiffness."""
+        import ctypes as C
+        ns = getattr(self, "num_specimens", 1)
+        for t in (lam_pos, lam_vel, lam_omega):
+            if not (t.is_cuda and t.is_contiguous() and t.dtype.itemsize == 4):
+                raise ValueError("cotangents must be contiguous float32 CUDA tensors")
+        grad = (C.c_double * (_lib.ADJ_NUM_COEF * ns))()
+        check(load().dem_adj_backward(self._h, lam_pos.data_ptr(), lam_vel.data_ptr(),
+                                      lam_omega.data_ptr(), grad, _stream(stream)))
+        import numpy as np
+        return np.array(list(grad)).reshape(ns, _lib.ADJ_NUM_COEF)
+
     def cells(self, stream=None):
         """(cellStart, cellEnd) of the last step's reorder as int32 CUDA tensors."""
         import torch
@@ -287,7 +312,16 @@ class Batch(Simulation):
         check(load().dem_batch_create(arr, len(specs), flags, C.byref(h)))
         super().__init__(specs[0][0], total, flags, _handle=h)
         self.specs = specs
+        self.num_specimens = len(specs)
         self.materials_max = max(len(sys.materials) for sys, _ in specs)
+
+    def set_systems(self, systems) -> None:
+        """New parameters for every specimen (same grids and counts)."""
+        arr = (_lib.DemSystem * len(systems))()
+        for k, sys in enumerate(systems):
+            arr[k] = sys.to_c(int(self.specs[k][1]))
+        check(load().dem_batch_set_systems(self._h, arr, len(systems)))
+        self.specs = [(sys, n) for sys, (_, n) in zip(systems, self.specs)]
 
     def slots(self, s: int):
         import ctypes as C

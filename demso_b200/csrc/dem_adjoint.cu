@@ -15,8 +15,12 @@
 //     Jacobian of the contact law comes from forward-mode duals evaluated on
 //     the recorded float values, so every branch (contact, dashpot, stick or
 //     slip, walls) is the one the forward took ("frozen contact set");
-//   coefficient gradients are summed in double, per block and then in a
-//     fixed order, so they are deterministic.
+//   coefficient gradients are summed in double: per warp over the slots of
+//     one specimen, into per-slot accumulators, then per specimen in a fixed
+//     order, so they are deterministic.
+// A batch (dem_batch_create) is differentiated the same way, each slot
+// reading its specimen's parameters; the coefficient gradients come out per
+// specimen.
 // The state adjoints live in particle-id order between steps.
 #include <algorithm>
 #include <cmath>
@@ -51,34 +55,43 @@ struct StepRec {
     uint2* cells;
 };
 
-__device__ __forceinline__ void block_add_coef(const double (&v)[kCoef], double* __restrict__ out) {
-    __shared__ double red[kAdjThreads / 32][kCoef];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+// Adds a thread's coefficient cotangents to the per-slot accumulators
+// acc[k * n + slot]: the values of a warp are reduced over runs of equal
+// `seg` (slots of one specimen are contiguous) in a fixed pattern, and the
+// first lane of each run adds the run's sum to its own slot.  Every slot is
+// always summed by the same lanes in the same order, so the result does not
+// depend on scheduling.
+__device__ __forceinline__ void warp_add_coef(const double (&v)[kCoef], uint32_t seg, uint32_t i,
+                                              uint32_t n, double* __restrict__ acc) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t prev = __shfl_up_sync(0xffffffffu, seg, 1);
+    const bool head = i < n && (lane == 0 || prev != seg);
 #pragma unroll
     for (int k = 0; k < kCoef; ++k) {
         double x = v[k];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-        if (lane == 0) red[warp][k] = x;
-    }
-    __syncthreads();
-    if (threadIdx.x < kCoef) {
-        double s = 0.0;
-        for (int w = 0; w < kAdjThreads / 32; ++w) s += red[w][threadIdx.x];
-        out[blockIdx.x * kCoef + threadIdx.x] += s;
+        for (int o = 1; o < 32; o <<= 1) {
+            const double y = __shfl_down_sync(0xffffffffu, x, o);
+            const uint32_t so = __shfl_down_sync(0xffffffffu, seg, o);
+            if (lane + o < 32 && so == seg) x += y;
+        }
+        if (head && x != 0.0) acc[(size_t)k * n + i] += x;
     }
 }
 
 // Reverse of integrate_one (particles_kernel.cuh:580-627) for one particle.
 __global__ void __launch_bounds__(kAdjThreads)
-adj_integrate_kernel(KParams P, StepRec rec, uint32_t n, const float2* __restrict__ lamXin,
-                     const float2* __restrict__ lamVin, const float* __restrict__ lamWin,
-                     float2* __restrict__ lx, float2* __restrict__ lv, float* __restrict__ lw,
-                     float2* __restrict__ lamF, float* __restrict__ lamM,
-                     double* __restrict__ coefPartial) {
+adj_integrate_kernel(KParams P0, const KParams* __restrict__ table,
+                     const uint32_t* __restrict__ spec, StepRec rec, uint32_t n,
+                     const float2* __restrict__ lamXin, const float2* __restrict__ lamVin,
+                     const float* __restrict__ lamWin, float2* __restrict__ lx,
+                     float2* __restrict__ lv, float* __restrict__ lw, float2* __restrict__ lamF,
+                     float* __restrict__ lamM, double* __restrict__ acc) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double coef[kCoef] = {0, 0, 0, 0, 0, 0, 0};
+    const uint32_t seg = i < n ? (table ? spec[i] : 0u) : 0xffffffffu;
     if (i < n) {
+        const KParams& P = table ? table[seg] : P0;
         const uint32_t id = rec.id[i];
         const float r = rec.radius[i], m = rec.mass[i];
         const float I = inertia_of(m, r);
@@ -136,19 +149,21 @@ adj_integrate_kernel(KParams P, StepRec rec, uint32_t n, const float2* __restric
         lamF[i] = make_float2(lV1.x * P.dt / m, lV1.y * P.dt / m);
         lamM[i] = lW * P.dt / I;
     }
-    block_add_coef(coef, coefPartial);
+    warp_add_coef(coef, seg, i, n, acc);
 }
 
 // Contacts of particle i in recorded step `rec`: adds the state cotangents
 // of i and, once per pair (i < j), the coefficient cotangents.
 __global__ void __launch_bounds__(kAdjThreads)
-adj_pairs_kernel(KParams P, StepRec rec, uint32_t n, const float2* __restrict__ lamF,
+adj_pairs_kernel(KParams P0, const KParams* __restrict__ table, const uint32_t* __restrict__ spec,
+                 StepRec rec, uint32_t n, const float2* __restrict__ lamF,
                  const float* __restrict__ lamM, float2* __restrict__ lx,
-                 float2* __restrict__ lv, float* __restrict__ lw,
-                 double* __restrict__ coefPartial) {
+                 float2* __restrict__ lv, float* __restrict__ lw, double* __restrict__ acc) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double coef[kCoef] = {0, 0, 0, 0, 0, 0, 0};
+    const uint32_t seg = i < n ? (table ? spec[i] : 0u) : 0xffffffffu;
     if (i < n) {
+        const KParams& P = table ? table[seg] : P0;
         const float2 p = rec.pos[i], v = rec.vel[i];
         const float w = rec.omega[i], r = rec.radius[i];
         const float2 lFi = lamF[i];
@@ -209,7 +224,7 @@ adj_pairs_kernel(KParams P, StepRec rec, uint32_t n, const float2* __restrict__ 
         lv[i] = make_float2(u.x + gvx, u.y + gvy);
         lw[i] += gw;
     }
-    block_add_coef(coef, coefPartial);
+    warp_add_coef(coef, seg, i, n, acc);
 }
 
 __global__ void adj_scatter_kernel(const uint32_t* __restrict__ id, uint32_t n,
@@ -224,14 +239,31 @@ __global__ void adj_scatter_kernel(const uint32_t* __restrict__ id, uint32_t n,
     lamW[k] = lw[i];
 }
 
-// Sum of the per-block coefficient partials in a fixed order.
-__global__ void adj_coef_sum_kernel(const double* __restrict__ partial, uint32_t blocks,
-                                    double* __restrict__ out) {
-    const int k = threadIdx.x;
-    if (k >= kCoef) return;
-    double s = 0.0;
-    for (uint32_t b = 0; b < blocks; ++b) s += partial[(size_t)b * kCoef + k];
-    out[k] = s;
+// Per specimen s: the sum of acc[k * n + slot] over its slots
+// [first[s], first[s + 1]), in a fixed order (strided per thread, then a
+// fixed-shape block reduction).
+constexpr int kSumThreads = 256;
+__global__ void __launch_bounds__(kSumThreads)
+adj_coef_sum_kernel(const double* __restrict__ acc, uint32_t n, const uint32_t* __restrict__ first,
+                    double* __restrict__ out) {
+    __shared__ double red[kSumThreads / 32];
+    const uint32_t s = blockIdx.x;
+    const uint32_t a = first ? first[s] : 0u, b = first ? first[s + 1] : n;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = 0; k < kCoef; ++k) {
+        double x = 0.0;
+        for (uint32_t j = a + threadIdx.x; j < b; j += kSumThreads) x += acc[(size_t)k * n + j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) red[warp] = x;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int w = 0; w < kSumThreads / 32; ++w) t += red[w];
+            out[(size_t)s * kCoef + k] = t;
+        }
+        __syncthreads();
+    }
 }
 
 }  // namespace
@@ -256,25 +288,26 @@ StepRec carve_step(void* base, uint32_t n, uint32_t numCells) {
     return r;
 }
 
-cudaError_t adj_backward_step(const KParams& P, void* recBase, uint32_t n, uint32_t numCells,
-                              float2* lamX, float2* lamV, float* lamW, float2* tlx, float2* tlv,
-                              float* tlw, float2* lamF, float* lamM, double* coefPartial,
-                              cudaStream_t st) {
+cudaError_t adj_backward_step(const KParams& P, const KParams* table, const uint32_t* spec,
+                              void* recBase, uint32_t n, uint32_t numCells, float2* lamX,
+                              float2* lamV, float* lamW, float2* tlx, float2* tlv, float* tlw,
+                              float2* lamF, float* lamM, double* acc, cudaStream_t st) {
     const StepRec rec = carve_step(recBase, n, numCells);
     const unsigned b = blocks_for(n, kAdjThreads);
-    adj_integrate_kernel<<<b, kAdjThreads, 0, st>>>(P, rec, n, lamX, lamV, lamW, tlx, tlv, tlw,
-                                                    lamF, lamM, coefPartial);
-    adj_pairs_kernel<<<b, kAdjThreads, 0, st>>>(P, rec, n, lamF, lamM, tlx, tlv, tlw,
-                                                coefPartial);
+    adj_integrate_kernel<<<b, kAdjThreads, 0, st>>>(P, table, spec, rec, n, lamX, lamV, lamW, tlx,
+                                                    tlv, tlw, lamF, lamM, acc);
+    adj_pairs_kernel<<<b, kAdjThreads, 0, st>>>(P, table, spec, rec, n, lamF, lamM, tlx, tlv, tlw,
+                                                acc);
     adj_scatter_kernel<<<b, kAdjThreads, 0, st>>>(rec.id, n, tlx, tlv, tlw, lamX, lamV, lamW);
     return cudaGetLastError();
 }
 
-cudaError_t adj_sum_coef(const double* partial, uint32_t n, double* out, cudaStream_t st) {
-    adj_coef_sum_kernel<<<1, 32, 0, st>>>(partial, blocks_for(n, kAdjThreads), out);
+cudaError_t adj_sum_coef(const double* acc, uint32_t n, const uint32_t* first, uint32_t numSpecimens,
+                         double* out, cudaStream_t st) {
+    adj_coef_sum_kernel<<<numSpecimens, kSumThreads, 0, st>>>(acc, n, first, out);
     return cudaGetLastError();
 }
 
-uint32_t adj_partial_blocks(uint32_t n) { return blocks_for(n, kAdjThreads); }
+size_t adj_acc_bytes(uint32_t n) { return sizeof(double) * kCoef * (size_t)n; }
 
 }  // namespace dem

@@ -674,6 +674,41 @@ extern "C" int dem_set_system(DemContext* c, const DemSystem* sys) {
     return DEM_OK;
 }
 
+extern "C" int dem_batch_set_systems(DemContext* c, const DemSystem* specs,
+                                     uint32_t numSpecimens) {
+    if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    if (!c->nspec) return fail(DEM_ERR_INVALID_ARG, "not a batch; use dem_set_system");
+    if (!specs || numSpecimens != c->nspec)
+        return fail(DEM_ERR_INVALID_ARG, "need %u specimens", c->nspec);
+    std::vector<KParams> table(c->nspec);
+    for (uint32_t s = 0; s < c->nspec; ++s) {
+        int rc = validate(&specs[s]);
+        if (rc) return rc;
+        const KParams& old = c->hTable[s];
+        if (specs[s].gridSize[0] != old.gx || specs[s].gridSize[1] != old.gy)
+            return fail(DEM_ERR_INVALID_ARG, "specimen %u: grid size is fixed at dem_batch_create", s);
+        if (specs[s].numParticles != c->partOff[s + 1] - c->partOff[s])
+            return fail(DEM_ERR_INVALID_ARG, "specimen %u: particle count is fixed", s);
+        if ((specs[s].numMaterials > 1) != (old.nmat > 1))
+            return fail(DEM_ERR_INVALID_ARG, "specimen %u: material layout is fixed", s);
+        table[s] = make_kparams(&specs[s], specs[s].numParticles);
+        table[s].cellOff = old.cellOff;
+        set_rmax(table[s], c->rmax);
+        bool attract = false;
+        for (uint32_t m = 0; m < table[s].nmat; ++m) attract = attract || table[s].at[m] != 0.0f;
+        if (attract && c->P.at[0] == 0.0f)
+            return fail(DEM_ERR_INVALID_ARG, "specimen %u: attraction was off at create", s);
+    }
+    DEM_TRY_CUDA(cudaMemcpy(c->dTable, table.data(), sizeof(KParams) * c->nspec,
+                            cudaMemcpyHostToDevice),
+                 "batch table");
+    c->hTable.swap(table);
+    // keys depend on the boxes; recompute them and sort from scratch
+    c->keysValid = false;
+    c->haveOrder = false;
+    return DEM_OK;
+}
+
 extern "C" int dem_set_state(DemContext* c, uint32_t n, const float* pos, const float* vel,
                              const float* theta, const float* omega, const float* radius,
                              const float* mass, const uint32_t* id, const uint32_t* type, int host,
@@ -1006,12 +1041,15 @@ bool has_attraction_host(const KParams& P) {
 
 int adj_check_context(DemContext* c) {
     if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
-    if (c->nspec) return fail(DEM_ERR_INVALID_ARG, "the adjoint takes a single scene, not a batch");
     if (c->typed) return fail(DEM_ERR_INVALID_ARG, "the adjoint takes a single material");
     if (!(c->flags & DEM_CTX_ACCEL)) return fail(DEM_ERR_INVALID_ARG, "create the context with DEM_CTX_ACCEL");
-    if (c->sys.gridSize[0] < 3 || c->sys.gridSize[1] < 3)
-        return fail(DEM_ERR_INVALID_ARG, "the adjoint needs at least 3 cells per axis");
-    if (has_attraction_host(c->P)) return fail(DEM_ERR_INVALID_ARG, "the adjoint has no attraction law");
+    const uint32_t ns = c->nspec ? c->nspec : 1u;
+    for (uint32_t s = 0; s < ns; ++s) {
+        const KParams& P = c->nspec ? c->hTable[s] : c->P;
+        if (P.gx < 3 || P.gy < 3)
+            return fail(DEM_ERR_INVALID_ARG, "the adjoint needs at least 3 cells per axis");
+        if (has_attraction_host(P)) return fail(DEM_ERR_INVALID_ARG, "the adjoint has no attraction law");
+    }
     return DEM_OK;
 }
 
@@ -1056,9 +1094,10 @@ extern "C" int dem_adj_backward(DemContext* c, float* lamPos, float* lamVel, flo
     cudaStream_t st = (cudaStream_t)stream;
     const uint32_t n = c->n;
     const size_t stepBytes = adj_step_bytes(n, c->numCells);
-    const uint32_t pblocks = adj_partial_blocks(n);
+    const uint32_t ns = c->nspec ? c->nspec : 1u;
     const size_t tmpBytes = 2 * al256(8ull * n) + 2 * al256(4ull * n) + al256(8ull * n) +
-                            al256(8ull * DEM_ADJ_NUM_COEF * pblocks) + 256;
+                            al256(adj_acc_bytes(n)) + al256(8ull * DEM_ADJ_NUM_COEF * ns) +
+                            al256(4ull * (ns + 1));
     char* rec = nullptr;
     char* tmp = nullptr;
     DEM_TRY_CUDA(cudaMalloc(&rec, stepBytes * c->adjEvery), "cudaMalloc adjoint record");
@@ -1073,10 +1112,13 @@ extern "C" int dem_adj_backward(DemContext* c, float* lamPos, float* lamVel, flo
     float* tlw = reinterpret_cast<float*>(q); q += al256(4ull * n);
     float* lamM = reinterpret_cast<float*>(q); q += al256(4ull * n);
     float2* lamF = reinterpret_cast<float2*>(q); q += al256(8ull * n);
-    double* partial = reinterpret_cast<double*>(q); q += al256(8ull * DEM_ADJ_NUM_COEF * pblocks);
-    double* sum = reinterpret_cast<double*>(q);
+    double* acc = reinterpret_cast<double*>(q); q += al256(adj_acc_bytes(n));
+    double* sum = reinterpret_cast<double*>(q); q += al256(8ull * DEM_ADJ_NUM_COEF * ns);
+    uint32_t* first = c->nspec ? reinterpret_cast<uint32_t*>(q) : nullptr;
     rc = DEM_OK;
-    e = cudaMemsetAsync(partial, 0, 8ull * DEM_ADJ_NUM_COEF * pblocks, st);
+    e = cudaMemsetAsync(acc, 0, adj_acc_bytes(n), st);
+    if (e == cudaSuccess && first)
+        e = cudaMemcpyAsync(first, c->partOff.data(), 4ull * (ns + 1), cudaMemcpyHostToDevice, st);
     const size_t snap = snapshot_bytes(n);
     for (int w = (int)c->adjWindows - 1; w >= 0 && rc == DEM_OK && e == cudaSuccess; --w) {
         Snapshot s = carve_snapshot(static_cast<char*>(c->adjCheck) + snap * w, n);
@@ -1085,7 +1127,8 @@ extern "C" int dem_adj_backward(DemContext* c, float* lamPos, float* lamVel, flo
         if (rc) break;
         const uint32_t k = std::min(c->adjEvery, c->adjSteps - (uint32_t)w * c->adjEvery);
         if (!c->keysValid) {
-            e = launch_calc_hash(c->P, c->dyn[0].pos, c->keys, nullptr, n, st);
+            e = c->nspec ? launch_calc_hash_batched(c->dTable, c->spec, c->dyn[0].pos, c->keys, n, st)
+                         : launch_calc_hash(c->P, c->dyn[0].pos, c->keys, nullptr, n, st);
             c->keysValid = true;
             c->haveOrder = false;
         }
@@ -1096,14 +1139,15 @@ extern "C" int dem_adj_backward(DemContext* c, float* lamPos, float* lamVel, flo
         }
         for (uint32_t t = 0; t < k && rc == DEM_OK; ++t) rc = step_recorded(c, st, rec + stepBytes * t);
         for (int t = (int)k - 1; t >= 0 && rc == DEM_OK && e == cudaSuccess; --t)
-            e = adj_backward_step(c->P, rec + stepBytes * t, n, c->numCells,
+            e = adj_backward_step(c->P, c->nspec ? c->dTable : nullptr, c->spec,
+                                  rec + stepBytes * t, n, c->numCells,
                                   reinterpret_cast<float2*>(lamPos),
                                   reinterpret_cast<float2*>(lamVel), lamOmega, tlx, tlv, tlw, lamF,
-                                  lamM, partial, st);
+                                  lamM, acc, st);
     }
-    if (rc == DEM_OK && e == cudaSuccess) e = adj_sum_coef(partial, n, sum, st);
+    if (rc == DEM_OK && e == cudaSuccess) e = adj_sum_coef(acc, n, first, ns, sum, st);
     if (rc == DEM_OK && e == cudaSuccess)
-        e = cudaMemcpyAsync(grad, sum, 8ull * DEM_ADJ_NUM_COEF, cudaMemcpyDeviceToHost, st);
+        e = cudaMemcpyAsync(grad, sum, 8ull * DEM_ADJ_NUM_COEF * ns, cudaMemcpyDeviceToHost, st);
     if (rc == DEM_OK && e == cudaSuccess) e = cudaStreamSynchronize(st);
     cudaFree(rec);
     cudaFree(tmp);

@@ -88,11 +88,16 @@ cudaError_t launch_unpack_cells(const uint2* cellRange, uint32_t numCells, uint3
 
 // Adjoint (dem_adjoint.cu).
 size_t adj_step_bytes(uint32_t n, uint32_t numCells);
-cudaError_t adj_backward_step(const KParams& P, void* recBase, uint32_t n, uint32_t numCells,
-                              float2* lamX, float2* lamV, float* lamW, float2* tlx, float2* tlv,
-                              float* tlw, float2* lamF, float* lamM, double* coefPartial,
-                              cudaStream_t st);
-cudaError_t adj_sum_coef(const double* partial, uint32_t n, double* out, cudaStream_t st);
-uint32_t adj_partial_blocks(uint32_t n);
+// table/spec: the batch's specimen table and slot -> specimen map, or null
+// for a single scene (then P).
+cudaError_t adj_backward_step(const KParams& P, const KParams* table, const uint32_t* spec,
+                              void* recBase, uint32_t n, uint32_t numCells, float2* lamX,
+                              float2* lamV, float* lamW, float2* tlx, float2* tlv, float* tlw,
+                              float2* lamF, float* lamM, double* acc, cudaStream_t st);
+// Per-specimen coefficient gradients (first: numSpecimens + 1 slot offsets,
+// or null for one specimen of n slots).
+cudaError_t adj_sum_coef(const double* acc, uint32_t n, const uint32_t* first, uint32_t numSpecimens,
+                         double* out, cudaStream_t st);
+size_t adj_acc_bytes(uint32_t n);
 
 }  // namespace dem

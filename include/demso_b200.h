@@ -199,6 +199,11 @@ int dem_batch_create(const DemSystem* specs, uint32_t numSpecimens, uint32_t fla
 /* Slots [*firstSlot, *firstSlot + *count) of the state hold specimen s (fixed
  * for the life of the batch). */
 int dem_batch_specimen(DemContext* ctx, uint32_t specimen, uint32_t* firstSlot, uint32_t* count);
+/* Replaces every specimen's parameters (box, gravity, time step, wall and
+ * contact coefficients) of a batch; grid sizes, particle counts and the
+ * material layout stay those of dem_batch_create.  The next dem_step sorts
+ * from scratch.  No reference counterpart. */
+int dem_batch_set_systems(DemContext* ctx, const DemSystem* specs, uint32_t numSpecimens);
 
 /* Copies out the current state in its current (cell-sorted) order, plus loc
  * (indexed by id) and, when requested at create time, pressure/acc/alpha of
@@ -247,8 +252,9 @@ int dem_profile_end(DemContext* ctx, float* ms, uint32_t* steps);
 /* ---------------------------------------------------------------------------
  * Adjoint (no counterpart in the reference): reverse-mode gradients of a
  * scalar loss of the final state with respect to the initial state and the
- * contact coefficients, for a single-material scene (not a batch) created
- * with DEM_CTX_ACCEL and at least 3 cells per axis.
+ * contact coefficients, for a context (a scene or a batch) of one material
+ * per specimen, without attraction, created with DEM_CTX_ACCEL and with at
+ * least 3 cells per axis.
  *
  * dem_adj_forward runs nsteps steps exactly as dem_step and keeps the state
  * every `every` steps (device memory held by the context).  The caller then
@@ -259,11 +265,13 @@ int dem_profile_end(DemContext* ctx, float* ms, uint32_t* steps);
  * contact set).  lamPos/lamVel/lamOmega are device arrays in particle-id
  * order: on entry the cotangents of the final pos (2n), vel (2n) and omega
  * (n), on return those of the initial state.  grad (host, DEM_ADJ_NUM_COEF
- * doubles) receives dL/d of: pair normal stiffness, pair shear stiffness,
+ * doubles per specimen; one specimen for a single scene) receives, for each
+ * specimen, dL/d of its: pair normal stiffness, pair shear stiffness,
  * pair dashpot, pair friction (the series/mean values of
  * particles_kernel.cuh:269-275), then the floor's dashpot (the material's
  * normalDamping), friction and series shear stiffness
- * (particles_kernel.cuh:419-421).  Coefficient sums are in double.  After
+ * (particles_kernel.cuh:419-421).  Coefficient sums are in double, in a
+ * fixed order (deterministic).  After
  * dem_adj_backward the context holds the state at the end of the first
  * window; set the state again before stepping on.
  * ------------------------------------------------------------------------- */

@@ -193,3 +193,74 @@ class AdjointLoss:
                         (gout * dv.to(torch.float64)).to(torch.float32))
 
         return F
+
+
+def batch_adjoint(systems_and_scenes, steps, every):
+    """Batched adjoint over specimens [(System, Scene)]: the per-specimen
+    loss of ``loss_of`` (mean x-displacement of the specimen + its kinetic
+    energy), summed.  Returns (per-specimen coefficient gradients (S, 7),
+    per-specimen (dpos, dvel, domega) cotangents of the initial state in each
+    specimen's own particle order)."""
+    import torch
+    import demso_b200 as D
+    specs = [sc for _, sc in systems_and_scenes]
+    b = D.Batch([(sys, sc.n) for sys, sc in systems_and_scenes],
+                flags=D.CTX_PRESSURE | D.CTX_ACCEL)
+    st = scenes.concat_specimens(specs)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int32) if a.dtype == np.uint32
+                                   else np.ascontiguousarray(a).copy())
+    b.set_state(t(st["pos"]), t(st["vel"]), t(st["theta"]), t(st["omega"]), t(st["radius"]),
+                t(st["mass"]), t(st["id"]))
+    L = D.load()
+    stream = torch.cuda.current_stream().cuda_stream
+    D.check(L.dem_adj_forward(b.handle, steps, every, stream))
+    final = {k: v.numpy() for k, v in b.get_state("cpu").items() if v is not None}
+    order = np.argsort(final["id"].view(np.uint32))
+    n = st["pos"].shape[0]
+    m = st["mass"]
+    r = st["radius"]
+    offs = np.cumsum([0] + [sc.n for sc in specs])
+    lam_pos = np.zeros((n, 2), np.float32)
+    for s in range(len(specs)):
+        lam_pos[offs[s]:offs[s + 1], 0] = np.float32(1.0 / specs[s].n)
+    lam_vel = (m[:, None] * final["vel"][order]).astype(np.float32)
+    lam_om = (inertia(m, r) * final["omega"][order]).astype(np.float32)
+    dp, dv, dw = (torch.from_numpy(a).cuda() for a in (lam_pos, lam_vel, lam_om))
+    grad = (C.c_double * (NUM_COEF * len(specs)))()
+    D.check(L.dem_adj_backward(b.handle, dp.data_ptr(), dv.data_ptr(), dw.data_ptr(), grad, stream))
+    torch.cuda.synchronize()
+    b.close()
+    g = np.array(list(grad)).reshape(len(specs), NUM_COEF)
+    dp, dv, dw = dp.cpu().numpy(), dv.cpu().numpy(), dw.cpu().numpy()
+    per = [(dp[offs[s]:offs[s + 1]], dv[offs[s]:offs[s + 1]], dw[offs[s]:offs[s + 1]])
+           for s in range(len(specs))]
+    return g, per
+
+
+def single_adjoint(sys, sc, steps, every):
+    """The same loss and cotangents as batch_adjoint for one specimen in its
+    own context, in the specimen's particle (array) order."""
+    import torch
+    import demso_b200 as D
+    n = sc.n
+    ids = np.arange(n, dtype=np.uint32)
+    sim = D.Simulation(sys, capacity=n, flags=D.CTX_PRESSURE | D.CTX_ACCEL)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int32) if a.dtype == np.uint32
+                                   else np.ascontiguousarray(a).copy())
+    sim.set_state(t(sc.pos), t(sc.vel), t(sc.theta), t(sc.omega), t(sc.radius), t(sc.mass), t(ids))
+    L = D.load()
+    stream = torch.cuda.current_stream().cuda_stream
+    D.check(L.dem_adj_forward(sim.handle, steps, every, stream))
+    final = {k: v.numpy() for k, v in sim.get_state("cpu").items() if v is not None}
+    order = np.argsort(final["id"].view(np.uint32))
+    lam_pos = np.zeros((n, 2), np.float32)
+    lam_pos[:, 0] = np.float32(1.0 / n)
+    lam_vel = (sc.mass[:, None] * final["vel"][order]).astype(np.float32)
+    lam_om = (inertia(sc.mass, sc.radius) * final["omega"][order]).astype(np.float32)
+    dp, dv, dw = (torch.from_numpy(a).cuda() for a in (lam_pos, lam_vel, lam_om))
+    grad = (C.c_double * NUM_COEF)()
+    D.check(L.dem_adj_backward(sim.handle, dp.data_ptr(), dv.data_ptr(), dw.data_ptr(), grad,
+                               stream))
+    torch.cuda.synchronize()
+    sim.close()
+    return np.array(list(grad)), (dp.cpu().numpy(), dv.cpu().numpy(), dw.cpu().numpy())
