@@ -2,8 +2,7 @@
 // callers that cannot allocate device memory.
 //
 // Some callers of a sort like this cannot call cudaMalloc or take scratch
-// from an allocator: code that runs while its stream is being captured into
-// a CUDA graph, step loops that must not stall on the device-wide
+// from an allocator: step loops that must not stall on the device-wide
 // synchronisation cudaMalloc/cudaFree can imply, and host programs whose own
 // memory manager owns every device allocation and hands out no scratch.  This
 // variant takes its scratch from a fixed array in the library's device

@@ -110,10 +110,10 @@ int dem_sort_particles(uint32_t* gridParticleHash, uint32_t* gridParticleIndex,
                        size_t scratchBytes, void* stream);
 
 /* No counterpart in the reference: dem_sort_particles for callers that
- * cannot allocate device memory -- code running while its stream is being
- * captured into a CUDA graph, loops that must not stall on the device-wide
- * synchronisation an allocation can cause, and host programs whose memory
- * manager owns all device memory.  Same stable in-place sort and result as
+ * cannot allocate device memory -- step loops that must not stall on the
+ * device-wide synchronisation that cudaMalloc/cudaFree can cause, and host
+ * programs whose own memory manager owns every device allocation and hands
+ * out no scratch.  Same stable in-place sort and result as
  * dem_sort_particles, but the scratch is a fixed array inside the library
  * (about 2.6 MB, held on every GPU that loads the library until exit), so at
  * most 262,144 pairs per call; larger calls fail with DEM_ERR_CAPACITY.

@@ -1,8 +1,9 @@
 """dem_sort_particles_static: the sort for callers that cannot allocate.
 
-Callers that run while their stream is being captured into a CUDA graph, or
-whose memory manager owns all device memory, cannot hand the sort scratch
-memory; this entry point uses a fixed array inside the library instead.  The
+Callers whose step loop must not stall on the device-wide synchronisation of
+an allocation, or whose own memory manager owns all device memory, cannot
+hand the sort scratch memory; this entry point uses a fixed array inside the
+library instead.  The
 test calls it through the C ABI and checks that it gives exactly the result
 of dem_sort_particles (caller scratch) -- the sort is integer work, so the
 tolerance is zero -- on two calls in a row that share the fixed array, and
