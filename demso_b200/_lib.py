@@ -11,7 +11,7 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libdemso_b200.so")
 
-DEM_MAX_MATERIALS = 8
+DEM_MAX_MATERIALS = 10
 STATUS = {0: "DEM_OK", 1: "DEM_ERR_INVALID_ARG", 2: "DEM_ERR_CUDA", 3: "DEM_ERR_OOB",
           4: "DEM_ERR_TIMEOUT", 5: "DEM_ERR_NO_MEMORY", 6: "DEM_ERR_CAPACITY"}
 CTX_PRESSURE = 1
@@ -40,6 +40,21 @@ class DemSystem(C.Structure):
                 ("boundaryShearStiffness", C.c_float), ("numMaterials", C.c_uint32),
                 ("materials", DemMaterial * DEM_MAX_MATERIALS)]
 
+
+class DemDsmlInfo(C.Structure):
+    _fields_ = [("numParticles", C.c_uint32), ("numTypes", C.c_uint32),
+                ("numFollowed", C.c_uint32), ("imageHeight", C.c_uint32),
+                ("numRectangles", C.c_uint32), ("numTriangles", C.c_uint32),
+                ("numSingles", C.c_uint32), ("controlledType", C.c_int32),
+                ("timeStep", C.c_float), ("simDuration", C.c_float)]
+
+
+class DemDsmlType(C.Structure):
+    _fields_ = [("id", C.c_char * 64), ("name", C.c_char * 128), ("mass", C.c_float),
+                ("radius", C.c_float), ("color", C.c_float * 3)]
+
+
+DSML_NO_JITTER = 1  # DEM_DSML_NO_JITTER
 
 # (name, restype, argtypes)
 _P = C.c_void_p
@@ -76,6 +91,14 @@ SIGNATURES = [
     ("dem_adj_backward", C.c_int, [_P, _P, _P, _P, C.POINTER(C.c_double), _P]),
     ("dem_scene_rsa", C.c_int, [_U, _P, C.c_float, C.c_float, C.c_uint64, _U, _U, _P,
                                 C.POINTER(_U)]),
+    ("dem_dsml_load", C.c_int, [C.c_char_p, C.c_uint64, _U, C.POINTER(_P)]),
+    ("dem_dsml_parse", C.c_int, [C.c_char_p, C.c_size_t, C.c_uint64, _U, C.POINTER(_P)]),
+    ("dem_dsml_free", None, [_P]),
+    ("dem_dsml_info", C.c_int, [_P, C.POINTER(DemDsmlInfo)]),
+    ("dem_dsml_system", C.c_int, [_P, _SYS]),
+    ("dem_dsml_state", C.c_int, [_P] + [_P] * 8),
+    ("dem_dsml_followed", C.c_int, [_P, _P]),
+    ("dem_dsml_type", C.c_int, [_P, _U, C.POINTER(DemDsmlType)]),
 ]
 
 _lib = None

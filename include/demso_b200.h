@@ -39,7 +39,7 @@
 extern "C" {
 #endif
 
-#define DEM_ABI_VERSION 1
+#define DEM_ABI_VERSION 2
 
 #define DEM_OK 0
 #define DEM_ERR_INVALID_ARG 1 /* bad pointer, size, grid (not a power of two) */
@@ -49,7 +49,7 @@ extern "C" {
 #define DEM_ERR_NO_MEMORY 5   /* device allocation failed */
 #define DEM_ERR_CAPACITY 6    /* more particles/cells than the context holds */
 
-#define DEM_MAX_MATERIALS 8
+#define DEM_MAX_MATERIALS 10  /* MAX_PARTICLES_TYPES (main.cuh:33) */
 
 /* Per-material contact coefficients: the reference's ParticleProperties
  * (main.cuh:39-54) minus radius/mass/inertia/colour.  Pair values follow the
@@ -283,6 +283,47 @@ int dem_adj_backward(DemContext* ctx, float* lamPos, float* lamVel, float* lamOm
 /* ---------------------------------------------------------------------------
  * Scene generation (host only, no GPU needed)
  * ------------------------------------------------------------------------- */
+
+/* .dsml scenes: the reference's input format (DEMParser, parser.cpp:49-377;
+ * DEMSimulation::loadFromFile, DEMSimulation.cpp:45-60) and its scene
+ * construction (PrepareSim, main.cu:54-369, with createRectanglesD and
+ * createTrianglesD, particles_kernel.cuh:43-111).  Particles are numbered
+ * single particles first, then rectangles, then triangles; every particle
+ * carries its type's radius and mass; the materials are the particle types in
+ * file order.  Rectangle lattice points are jittered by (N(0,1) - 0.5) / 100
+ * of the spacing from a generator seeded by `seed` (the reference seeds
+ * cuRAND with time(NULL)); DEM_DSML_NO_JITTER uses a zero deviate.  Errors
+ * (DEM_ERR_INVALID_ARG) carry the reference's parse messages.  The step has
+ * no control particle (the reference built with USE_BIG_PARTICLE 0): a
+ * <controlled> tag is reported (its type) but creates nothing. */
+#define DEM_DSML_NO_JITTER 1u
+typedef struct DemDsml DemDsml;
+typedef struct DemDsmlInfo {
+    uint32_t numParticles, numTypes, numFollowed, imageHeight;
+    uint32_t numRectangles, numTriangles, numSingles;
+    int32_t controlledType;  /* -1 without a <controlled> tag */
+    float timeStep;          /* <timestep> */
+    float simDuration;       /* <simduration> in seconds; -1 = run forever */
+} DemDsmlInfo;
+typedef struct DemDsmlType {
+    char id[64], name[128];
+    float mass, radius;
+    float color[3];          /* 0..255 from color="rrggbb" (white by default) */
+} DemDsmlType;
+int dem_dsml_load(const char* path, uint64_t seed, uint32_t flags, DemDsml** out);
+int dem_dsml_parse(const char* text, size_t length, uint64_t seed, uint32_t flags, DemDsml** out);
+void dem_dsml_free(DemDsml* scene);
+int dem_dsml_info(const DemDsml* scene, DemDsmlInfo* info);
+/* The scene's DemSystem, with the reference's grid rule (main.cu:218-236). */
+int dem_dsml_system(const DemDsml* scene, DemSystem* sys);
+/* The initial state into host arrays of numParticles entries (pos and vel:
+ * two per particle); NULL outputs are skipped. */
+int dem_dsml_state(const DemDsml* scene, float* pos, float* vel, float* theta, float* omega,
+                   float* radius, float* mass, uint32_t* id, uint32_t* type);
+/* The followed particle ids (numFollowed entries): single particles marked
+ * follow="true", then the <follow> entries of <parameters>. */
+int dem_dsml_followed(const DemDsml* scene, uint32_t* ids);
+int dem_dsml_type(const DemDsml* scene, uint32_t type, DemDsmlType* out);
 
 /* Seeded random sequential placement of n non-overlapping disks of the given
  * radii in [0,Lx]x[0,Ly] (host arrays; pos receives 2n floats in the order of

@@ -17,7 +17,7 @@
 #define DEMSO_ORACLE_H
 #include <stdint.h>
 
-#define ORC_MAX_MATERIALS 8
+#define ORC_MAX_MATERIALS 10
 
 typedef struct OrcSystem {
     double Lx, Ly;           /* cubeDimension (main.cuh:112) */

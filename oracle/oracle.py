@@ -5,13 +5,15 @@ reference arms import this module, and only as the checker or the timed CPU
 baseline.  The product path (the ``demso_b200`` package and its CUDA
 library) never imports or calls anything here.
 
-Three oracles are wrapped:
+Four oracles are wrapped:
 
 * ``PortOracle`` -- ``dem_oracle.c``, our CPU restatement of the reference's
   step (particles_kernel.cuh / functions.cu / main.cu), in float
   (``libdem_oracle_f32.so``) or double (``libdem_oracle_f64.so``).
 * ``TangentOracle`` -- ``dem_tangent.cpp``, the forward-mode derivative of
   the same step (the FP64 oracle of the adjoint).
+* ``RefDsml`` -- ``_ref/libdsml_ref.so``, the reference's own scene-file
+  parser, with the block generators of ``_ref/libdemso_ref.so``.
 * ``RefHarness`` -- ``_ref/libdemso_ref.so``, the reference's own
   ``src/particles_kernel.cuh`` compiled for the host by oracle/Makefile (only
   when the reference tree was present at build time).
@@ -31,7 +33,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-MAX_MATERIALS = 8
+MAX_MATERIALS = 10
 
 _u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
 _f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
@@ -450,3 +452,109 @@ class RefHarness:
                          b["loc2"], b["acc"].reshape(-1), b["alpha"], b["pressure"], b["hash"],
                          b["index"], b["cellStart"], b["cellEnd"])
         return b
+
+
+# ---------------------------------------------------------------------------
+# Reference scene parser and block generators (host builds)
+# ---------------------------------------------------------------------------
+def dsml_ref_available() -> bool:
+    return (os.path.isfile(os.path.join(OUT, "libdsml_ref.so"))
+            and os.path.isfile(os.path.join(OUT, "libdemso_ref.so")))
+
+
+class RefDsml:
+    """The reference's own .dsml parser (src/parser.cpp, src/DEMSimulation.cpp)
+    and block generator kernels (createRectanglesD with a zero normal deviate,
+    createTrianglesD), built for the host by oracle/Makefile.  ``load``
+    returns the parsed scene and the particles the reference would create,
+    in PrepareSim's order (main.cu:246-325): single particles, rectangles,
+    triangles.  The parser is handed a copy without color attributes (it
+    overflows its colour buffers, parser.cpp:120-134)."""
+
+    def __init__(self):
+        self.p = C.CDLL(os.path.join(OUT, "libdsml_ref.so"))
+        self.k = C.CDLL(os.path.join(OUT, "libdemso_ref.so"))
+        dp = C.POINTER(C.c_double)
+        ip = C.POINTER(C.c_int)
+        self.p.ref_dsml_load.argtypes = [C.c_char_p, C.c_char_p, C.c_int]
+        self.p.ref_dsml_counts.argtypes = [ip]
+        self.p.ref_dsml_params.argtypes = [dp]
+        self.p.ref_dsml_type.argtypes = [C.c_int, dp, C.c_char_p, C.c_int]
+        self.p.ref_dsml_rect.argtypes = [C.c_int, dp, ip]
+        self.p.ref_dsml_tri.argtypes = [C.c_int, dp, ip]
+        self.p.ref_dsml_single.argtypes = [C.c_int, dp]
+        self.p.ref_dsml_followed.argtypes = [ip, ip]
+        u = C.c_uint32
+        f = C.c_float
+        self.k.ref_create_rectangles.argtypes = [_f32p, _u32p, _u32p, _u32p, f, f, f, f, u, u, u,
+                                                 u, _u32p]
+        self.k.ref_create_triangles.argtypes = [_f32p, _u32p, _u32p, _u32p, f, f, f, u, u, u,
+                                                _u32p]
+
+    def load(self, path: str, tmpdir: str):
+        import re
+        text = open(path, "rb").read()
+        text = re.sub(rb"\scolor=\"[^\"]*\"", b"", text)
+        tmp = os.path.join(tmpdir, "ref_nocolor.dsml")
+        open(tmp, "wb").write(text)
+        err = C.create_string_buffer(512)
+        if self.p.ref_dsml_load(tmp.encode(), err, 512):
+            return {"error": err.value.decode()}
+        c = (C.c_int * 7)()
+        self.p.ref_dsml_counts(c)
+        nt, nr, ntri, ns, nfs, nfp, _ = list(c)
+        par = (C.c_double * 9)()
+        self.p.ref_dsml_params(par)
+        out = {"params": list(par), "types": [], "followed": []}
+        for t in range(nt):
+            v = (C.c_double * 11)()
+            name = C.create_string_buffer(128)
+            self.p.ref_dsml_type(t, v, name, 128)
+            out["types"].append({"id": name.value.decode(), "values": list(v)[:8]})
+        fs = (C.c_int * max(nfs, 1))()
+        fp = (C.c_int * max(nfp, 1))()
+        self.p.ref_dsml_followed(fs, fp)
+        out["followed"] = list(fs)[:nfs] + list(fp)[:nfp]
+        pos, ids, types = [], [], []
+        start = 0
+        for i in range(ns):
+            v = (C.c_double * 7)()
+            self.p.ref_dsml_single(i, v)
+            pos.append(np.array([[v[0], v[1]]], np.float32))
+            types.append(np.array([int(v[6])], np.uint32))
+            ids.append(np.array([start], np.uint32))
+            start += 1
+        for i in range(nr):
+            v = (C.c_double * 6)()
+            tv = (C.c_int * 16)()
+            k = self.p.ref_dsml_rect(i, v, tv)
+            nx, ny = int(v[4]), int(v[5])
+            m = nx * ny
+            p = np.zeros(2 * m, np.float32)
+            idv = np.zeros(m, np.uint32)
+            loc = np.zeros(m, np.uint32)
+            ty = np.zeros(m, np.uint32)
+            vec = np.array(list(tv)[:k], np.uint32)
+            self.k.ref_create_rectangles(p, idv, loc, ty, v[0], v[1], v[2], v[3], nx, ny, start,
+                                         k, vec)
+            pos.append(p.reshape(-1, 2)); ids.append(idv); types.append(ty)
+            start += m
+        for i in range(ntri):
+            v = (C.c_double * 4)()
+            tv = (C.c_int * 16)()
+            k = self.p.ref_dsml_tri(i, v, tv)
+            N = int(v[3])
+            m = N * (N + 1) // 2
+            p = np.zeros(2 * m, np.float32)
+            idv = np.zeros(m, np.uint32)
+            loc = np.zeros(m, np.uint32)
+            ty = np.zeros(m, np.uint32)
+            vec = np.array(list(tv)[:k], np.uint32)
+            self.k.ref_create_triangles(p, idv, loc, ty, v[0], v[1], v[2], N, start, k, vec)
+            pos.append(p.reshape(-1, 2)); ids.append(idv); types.append(ty)
+            start += m
+        cat = lambda a, dt: np.concatenate(a) if a else np.zeros(0, dt)
+        out["pos"] = cat(pos, np.float32).reshape(-1, 2)
+        out["id"] = cat(ids, np.uint32)
+        out["type"] = cat(types, np.uint32)
+        return out

@@ -243,4 +243,37 @@ void ref_run(uint32_t nsteps,
     }
 }
 
+/* The reference's block generators, one "CUDA thread" per particle:
+ * createRectanglesD (particles_kernel.cuh:43-74) with the cuRAND stand-in's
+ * zero normal deviate, and createTrianglesD (:76-111) with space and height
+ * formed as PrepareSim forms them (main.cu:306-307). */
+void ref_create_rectangles(float* pos, uint32_t* id, uint32_t* loc, uint32_t* type, float sx,
+                           float sy, float ex, float ey, uint32_t nx, uint32_t ny,
+                           uint32_t startID, uint32_t ntypes, uint32_t* typeVec) {
+    const float2 start = make_float2(sx, sy);
+    const float2 len = make_float2(ex - sx, ey - sy);
+    for (uint y = 0; y < ny; ++y)
+        for (uint x = 0; x < nx; ++x) {
+            threadIdx = make_uint3(0, 0, 0);
+            blockIdx = make_uint3(x, y, 0);
+            blockDim = dim3(1, 1, 1);
+            gridDim = dim3(nx, ny, 1);
+            createRectanglesD(reinterpret_cast<float2*>(pos), id, loc, type, start, len,
+                              make_uint2(nx, ny), startID, ntypes, typeVec, 0ul);
+        }
+}
+
+void ref_create_triangles(float* pos, uint32_t* id, uint32_t* loc, uint32_t* type, float px,
+                          float py, float width, uint32_t N, uint32_t startID, uint32_t ntypes,
+                          uint32_t* typeVec) {
+    const uint32_t count = N * (N + 1) / 2;
+    float space = width / (N - 1);
+    float height = space * sqrt(3) / 2;
+    for (uint i = 0; i < count; ++i) {
+        set_thread(i, count);
+        createTrianglesD(reinterpret_cast<float2*>(pos), id, loc, type, make_float2(px, py), N,
+                         ntypes, typeVec, space, height, startID, count);
+    }
+}
+
 }  /* extern "C" */

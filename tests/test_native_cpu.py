@@ -40,7 +40,7 @@ def test_binding_covers_header():
 
 def test_abi_version_and_struct_sizes():
     lib = _lib.load()
-    assert lib.dem_abi_version() == 1
+    assert lib.dem_abi_version() == 2
     # DemSystem: 4 + 8 + 8 + 4 + 8 + 4 + 4 + 4 + 8 * 24 bytes
     assert C.sizeof(_lib.DemSystem) == 44 + 8 * 24
     assert C.sizeof(_lib.DemMaterial) == 24
