@@ -41,8 +41,8 @@ def test_binding_covers_header():
 def test_abi_version_and_struct_sizes():
     lib = _lib.load()
     assert lib.dem_abi_version() == 2
-    # DemSystem: 4 + 8 + 8 + 4 + 8 + 4 + 4 + 4 + 8 * 24 bytes
-    assert C.sizeof(_lib.DemSystem) == 44 + 8 * 24
+    # DemSystem: 4 + 8 + 8 + 4 + 8 + 4 + 4 + 4 bytes + DEM_MAX_MATERIALS * 24
+    assert C.sizeof(_lib.DemSystem) == 44 + _lib.DEM_MAX_MATERIALS * 24
     assert C.sizeof(_lib.DemMaterial) == 24
 
 
@@ -62,7 +62,7 @@ def test_validate_system():
     s = _sys().to_c()
     s.numMaterials = 0
     assert lib.dem_validate_system(s) == 1
-    s.numMaterials = 9
+    s.numMaterials = _lib.DEM_MAX_MATERIALS + 1
     assert lib.dem_validate_system(s) == 1
     s = _sys().to_c()
     s.cubeDimension[0] = 0.0
