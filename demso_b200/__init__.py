@@ -259,6 +259,28 @@ class Simulation:
     def kernels_per_step(self) -> int:
         return int(load().dem_kernels_per_step(self._h))
 
+    def render(self, params, image=None, stream=None):
+        """The disk splat of the current state (dem_render) into a CUDA uint8
+        tensor of shape (imageDIMy, imageDIMx, 4), row 0 at the bottom."""
+        import ctypes as C
+        import torch
+        if image is None:
+            image = torch.empty((params.imageDIMy, params.imageDIMx, 4), dtype=torch.uint8,
+                                device="cuda")
+        check(load().dem_render(self._h, C.byref(params), image.data_ptr(), _stream(stream)))
+        return image
+
+    def followed(self, ids, stream=None):
+        """Rows of dem_get_followed for the given particle ids: an (n, 12)
+        float32 array (id and type as integer bits)."""
+        import numpy as np
+        ids = np.ascontiguousarray(ids, dtype=np.uint32)
+        rows = np.zeros((ids.size, 12), np.float32)
+        if ids.size:
+            check(load().dem_get_followed(self._h, ids.ctypes.data, ids.size, rows.ctypes.data,
+                                          _stream(stream)))
+        return rows
+
     # -- adjoint (dem_adj_forward / dem_adj_backward) ------------------------
     def adjoint_forward(self, nsteps: int, every: int, stream=None) -> None:
         """`nsteps` steps as ``step``, keeping a checkpoint every `every` steps

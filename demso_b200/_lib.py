@@ -56,6 +56,12 @@ class DemDsmlType(C.Structure):
 
 DSML_NO_JITTER = 1  # DEM_DSML_NO_JITTER
 
+
+class DemRenderParams(C.Structure):
+    _fields_ = [("imageDIMx", C.c_uint32), ("imageDIMy", C.c_uint32), ("bgColor", C.c_uint32),
+                ("viewRotations", C.c_uint32), ("colorByPressure", C.c_uint32),
+                ("maxPressure", C.c_float), ("color", (C.c_float * 3) * DEM_MAX_MATERIALS)]
+
 # (name, restype, argtypes)
 _P = C.c_void_p
 _U = C.c_uint32
@@ -91,6 +97,9 @@ SIGNATURES = [
     ("dem_adj_backward", C.c_int, [_P, _P, _P, _P, C.POINTER(C.c_double), _P]),
     ("dem_scene_rsa", C.c_int, [_U, _P, C.c_float, C.c_float, C.c_uint64, _U, _U, _P,
                                 C.POINTER(_U)]),
+    ("dem_render_particles", C.c_int, [_SYS, _P, _P, _P, _P, _P, _U,
+                                       C.POINTER(DemRenderParams), _P, _P, _P]),
+    ("dem_render", C.c_int, [_P, C.POINTER(DemRenderParams), _P, _P]),
     ("dem_dsml_load", C.c_int, [C.c_char_p, C.c_uint64, _U, C.POINTER(_P)]),
     ("dem_dsml_parse", C.c_int, [C.c_char_p, C.c_size_t, C.c_uint64, _U, C.POINTER(_P)]),
     ("dem_dsml_free", None, [_P]),

@@ -301,6 +301,9 @@ struct DemContext {
     std::vector<KParams> hTable;
     uint32_t* spec = nullptr;
     std::vector<uint32_t> partOff;
+    // dem_render's per-pixel owner scratch
+    uint32_t* renderOwner = nullptr;
+    size_t renderOwnerWords = 0;
     bool keysValid = false;  // keys[] holds the cell of every particle of the current state
     bool haveOrder = false;  // the last step recorded its movers: incremental sort possible
     float rmax = INFINITY;   // largest radius of the current state (culling bound)
@@ -646,6 +649,7 @@ extern "C" int dem_destroy(DemContext* c) {
     if (c->bodyStream) cudaStreamDestroy(c->bodyStream);
     cudaFree(c->followRows);
     cudaFree(c->adjCheck);
+    cudaFree(c->renderOwner);
     cudaFree(c->dTable);
     cudaFree(c->spec);
     cudaFree(c->incScratch);
@@ -923,6 +927,62 @@ extern "C" int dem_get_followed(DemContext* c, const uint32_t* ids, uint32_t cou
                      "followed copy");
         DEM_TRY_CUDA(cudaStreamSynchronize(st), "followed sync");
     }
+    return DEM_OK;
+}
+
+namespace {
+int check_render(const DemRenderParams* rp) {
+    if (!rp) return fail(DEM_ERR_INVALID_ARG, "render parameters are NULL");
+    if (rp->imageDIMx == 0 || rp->imageDIMy == 0 ||
+        (uint64_t)rp->imageDIMx * rp->imageDIMy > (1ull << 30))
+        return fail(DEM_ERR_INVALID_ARG, "image %u x %u", rp->imageDIMx, rp->imageDIMy);
+    if (rp->colorByPressure && !(rp->maxPressure > 0.0f))
+        return fail(DEM_ERR_INVALID_ARG, "maxPressure must be > 0 to colour by pressure");
+    return DEM_OK;
+}
+}  // namespace
+
+extern "C" int dem_render_particles(const DemSystem* sys, const float* pos, const float* theta,
+                                    const uint32_t* type, const float* radius,
+                                    const float* pressure, uint32_t n, const DemRenderParams* rp,
+                                    uint32_t* owner, void* image, void* stream) {
+    int rc = validate(sys);
+    if (rc) return rc;
+    rc = check_render(rp);
+    if (rc) return rc;
+    if (!owner || !image || (n && (!pos || !radius || (rp->viewRotations && !theta))))
+        return fail(DEM_ERR_INVALID_ARG, "dem_render_particles: NULL buffer");
+    if (sys->numMaterials > 1 && n && !type)
+        return fail(DEM_ERR_INVALID_ARG, "dem_render_particles: several materials need `type`");
+    DEM_TRY_CUDA(launch_render(*rp, sys->cubeDimension[0], sys->cubeDimension[1],
+                               reinterpret_cast<const float2*>(pos), theta,
+                               sys->numMaterials > 1 ? type : nullptr, radius, pressure, n, owner,
+                               static_cast<uchar4*>(image), (cudaStream_t)stream),
+                 "render");
+    return DEM_OK;
+}
+
+extern "C" int dem_render(DemContext* c, const DemRenderParams* rp, void* image, void* stream) {
+    if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    if (c->nspec) return fail(DEM_ERR_INVALID_ARG, "dem_render takes a single scene");
+    int rc = check_render(rp);
+    if (rc) return rc;
+    if (!image) return fail(DEM_ERR_INVALID_ARG, "dem_render: NULL image");
+    const size_t words = (size_t)rp->imageDIMx * rp->imageDIMy;
+    if (c->renderOwnerWords < words) {
+        cudaFree(c->renderOwner);
+        c->renderOwner = nullptr;
+        c->renderOwnerWords = 0;
+        DEM_TRY_CUDA(cudaMalloc(&c->renderOwner, 4 * words), "cudaMalloc render scratch");
+        c->renderOwnerWords = words;
+    }
+    const int a = c->cur;
+    DEM_TRY_CUDA(launch_render(*rp, c->sys.cubeDimension[0], c->sys.cubeDimension[1],
+                               c->dyn[0].pos, c->dyn[0].theta, c->typed ? c->stat[a].type : nullptr,
+                               c->stat[a].radius,
+                               (c->flags & DEM_CTX_PRESSURE) ? c->pressure : nullptr, c->n,
+                               c->renderOwner, static_cast<uchar4*>(image), (cudaStream_t)stream),
+                 "render");
     return DEM_OK;
 }
 

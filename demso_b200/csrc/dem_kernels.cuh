@@ -100,4 +100,11 @@ cudaError_t adj_sum_coef(const double* acc, uint32_t n, const uint32_t* first, u
                          double* out, cudaStream_t st);
 size_t adj_acc_bytes(uint32_t n);
 
+// Disk splat of n particles into a DIMx x DIMy uchar4 image (dem_render.cu);
+// owner: DIMx * DIMy words of scratch.
+cudaError_t launch_render(const DemRenderParams& rp, float Lx, float Ly, const float2* pos,
+                          const float* theta, const uint32_t* type, const float* radius,
+                          const float* pressure, uint32_t n, uint32_t* owner, uchar4* image,
+                          cudaStream_t st);
+
 }  // namespace dem

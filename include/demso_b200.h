@@ -250,6 +250,36 @@ int dem_profile_begin(DemContext* ctx, uint32_t maxSteps);
 int dem_profile_end(DemContext* ctx, float* ms, uint32_t* steps);
 
 /* ---------------------------------------------------------------------------
+ * Headless output
+ * ------------------------------------------------------------------------- */
+
+/* Disk splat of the particles (plotParticles, functions.cu:557-599 ->
+ * plotSpheresD, particles_kernel.cuh:629-718) into a device buffer of
+ * imageDIMx * imageDIMy uchar4 pixels (RGBA, row y = 0 at the bottom of the
+ * box), instead of the reference's GL pixel buffer.  Pixels, shading and
+ * colours follow the reference; where its threads race (overlapping disks,
+ * orientation lines over other disks) the result is deterministic: the
+ * particle with the highest index colours a shared pixel and lines are drawn
+ * after all disks. */
+typedef struct DemRenderParams {
+    uint32_t imageDIMx, imageDIMy;
+    uint32_t bgColor;          /* every byte of the background (cudaMemset value) */
+    uint32_t viewRotations;    /* draw each particle's orientation line */
+    uint32_t colorByPressure;  /* colour by pressure / maxPressure on the reference's colour bar */
+    float maxPressure;
+    float color[DEM_MAX_MATERIALS][3];  /* per material, 0..255 */
+} DemRenderParams;
+/* Per-stage form: caller buffers; `owner` is device scratch of
+ * imageDIMx * imageDIMy words; type and pressure may be NULL. */
+int dem_render_particles(const DemSystem* sys, const float* pos, const float* theta,
+                         const uint32_t* type, const float* radius, const float* pressure,
+                         uint32_t numParticles, const DemRenderParams* params, uint32_t* owner,
+                         void* image, void* stream);
+/* The context's current state; the owner scratch is held by the context
+ * (allocated on the first call, or when the image grows). */
+int dem_render(DemContext* ctx, const DemRenderParams* params, void* image, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Adjoint (no counterpart in the reference): reverse-mode gradients of a
  * scalar loss of the final state with respect to the initial state and the
  * contact coefficients, for a context (a scene or a batch) of one material

@@ -558,3 +558,46 @@ class RefDsml:
         out["id"] = cat(ids, np.uint32)
         out["type"] = cat(types, np.uint32)
         return out
+
+
+# ---------------------------------------------------------------------------
+# Headless outputs (dem_render.c)
+# ---------------------------------------------------------------------------
+class RenderOracle:
+    """CPU disk splat (orc_render) and the output.csv line (orc_followed_line)."""
+
+    def __init__(self):
+        path = os.path.join(OUT, "libdem_render.so")
+        if not os.path.isfile(path):
+            build()
+        self.lib = C.CDLL(path)
+        u = C.c_uint32
+        f = C.c_float
+        self.lib.orc_render.argtypes = [u, u, u, C.c_int, C.c_int, f, _f32p, f, f, _f32p,
+                                        _f32p, C.c_void_p, _f32p, C.c_void_p, u,
+                                        np.ctypeslib.ndpointer(dtype=np.uint8,
+                                                               flags="C_CONTIGUOUS")]
+        self.lib.orc_followed_line.argtypes = [f, _f32p, u, C.c_char_p, C.c_size_t]
+        self.lib.orc_followed_line.restype = C.c_size_t
+
+    def render(self, dimx, dimy, bg, view_rotations, by_pressure, max_pressure, colors, Lx, Ly,
+               pos, theta, type_, radius, pressure):
+        n = int(np.asarray(radius).size)
+        img = np.zeros((dimy, dimx, 4), np.uint8)
+        col = np.ascontiguousarray(colors, dtype=np.float32).reshape(-1)
+        t = None if type_ is None else np.ascontiguousarray(type_, dtype=np.uint32)
+        pr = None if pressure is None else np.ascontiguousarray(pressure, dtype=np.float32)
+        self.lib.orc_render(dimx, dimy, bg, int(view_rotations), int(by_pressure), max_pressure,
+                            col, Lx, Ly, np.ascontiguousarray(pos, dtype=np.float32).reshape(-1),
+                            np.ascontiguousarray(theta, dtype=np.float32),
+                            t.ctypes.data if t is not None else None,
+                            np.ascontiguousarray(radius, dtype=np.float32),
+                            pr.ctypes.data if pr is not None else None, n, img.reshape(-1))
+        return img
+
+    def followed_line(self, elapsed, rows) -> str:
+        rows = np.ascontiguousarray(rows, dtype=np.float32).reshape(-1)
+        buf = C.create_string_buffer(64 + 256 * (rows.size // 12 + 1))
+        k = self.lib.orc_followed_line(np.float32(elapsed), rows, rows.size // 12, buf,
+                                       len(buf))
+        return buf.raw[:k].decode()

@@ -1,0 +1,120 @@
+"""Headless outputs and .dsml scenes on the GPU: the disk splat against the
+CPU restatement pixel for pixel (type colours, pressure colours, lines, the
+per-stage form); a .dsml scene of every block kind stepped against the
+oracle; the runner's output.csv against the C formatter of the reference's
+line."""
+import os
+
+import numpy as np
+import pytest
+
+from demso_b200 import dsml, output, scenes
+from helpers import gpu_run, same
+from oracle.oracle import PortOracle, RenderOracle
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FIXTURE = os.path.join(HERE, "golden", "dsml", "blocks.dsml")
+COLORS = [(255, 40, 10), (20, 200, 90), (60, 80, 250), (255, 255, 255), (128, 0, 128)]
+
+
+def _sim(sc, steps):
+    import torch
+    import demso_b200 as D
+    sim = D.Simulation(sc.sys, capacity=sc.n, flags=D.CTX_PRESSURE | D.CTX_ACCEL)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int32) if a.dtype == np.uint32
+                                   else np.ascontiguousarray(a))
+    st = sc.state()
+    sim.set_state(t(st["pos"]), t(st["vel"]), t(st["theta"]), t(st["omega"]), t(st["radius"]),
+                  t(st["mass"]), t(st["id"]), t(st["type"]) if st["type"] is not None else None)
+    sim.step(steps)
+    return sim
+
+
+@pytest.mark.parametrize("by_pressure", [False, True])
+def test_render_matches_the_cpu_splat(by_pressure):
+    sc = scenes.agitated_gas(n=3000, seed=21, n_mat=3, vel_std=0.3)
+    sim = _sim(sc, 25)
+    st = {k: (None if v is None else v.numpy()) for k, v in sim.get_state("cpu").items()}
+    mp = float(st["pressure"].max()) if by_pressure else 1.0
+    p = output.render_params(sc.sys.Lx, sc.sys.Ly, COLORS[:3], image_height=600,
+                             color_by_pressure=by_pressure, max_pressure=mp)
+    gpu = sim.render(p).cpu().numpy()
+    sim.close()
+    ref = RenderOracle().render(p.imageDIMx, p.imageDIMy, 0, True, by_pressure, mp, COLORS[:3],
+                                sc.sys.Lx, sc.sys.Ly, st["pos"], st["theta"],
+                                st["type"].view(np.uint32), st["radius"], st["pressure"])
+    assert gpu.shape == ref.shape
+    assert np.array_equal(gpu, ref), int(np.count_nonzero(np.any(gpu != ref, axis=2)))
+    assert np.count_nonzero(gpu[..., 3]) > 0.2 * gpu.shape[0] * gpu.shape[1]
+
+
+def test_per_stage_render_with_caller_scratch():
+    import ctypes as C
+    import torch
+    import demso_b200 as D
+    rng = np.random.default_rng(5)
+    n = 500
+    pos = rng.uniform(0.0, 1.0, size=(n, 2)).astype(np.float32)
+    pos[:5] = [[-0.1, 0.5], [1.2, 0.5], [0.5, -0.05], [0.999, 0.999], [0.0, 0.0]]
+    theta = rng.uniform(0, 6.3, size=n).astype(np.float32)
+    radius = rng.uniform(0.005, 0.03, size=n).astype(np.float32)
+    typ = rng.integers(0, 2, size=n).astype(np.uint32)
+    sys = scenes.agitated_gas(n=64, seed=1, n_mat=2).sys
+    sys.Lx = sys.Ly = 1.0
+    p = output.render_params(1.0, 1.0, COLORS[:2], image_height=301, bg=17)
+    dev = lambda a: torch.from_numpy(a.view(np.int32) if a.dtype == np.uint32 else a).cuda()
+    img = torch.empty((p.imageDIMy, p.imageDIMx, 4), dtype=torch.uint8, device="cuda")
+    owner = torch.empty(p.imageDIMx * p.imageDIMy, dtype=torch.int32, device="cuda")
+    d = [dev(a) for a in (pos, theta, typ, radius)]
+    D.check(D.load().dem_render_particles(sys.to_c(n), d[0].data_ptr(), d[1].data_ptr(),
+                                          d[2].data_ptr(), d[3].data_ptr(), None, n,
+                                          C.byref(p), owner.data_ptr(), img.data_ptr(),
+                                          D._stream()))
+    ref = RenderOracle().render(p.imageDIMx, p.imageDIMy, 17, True, False, 1.0, COLORS[:2], 1.0,
+                                1.0, pos, theta, typ, radius, None)
+    assert np.array_equal(img.cpu().numpy(), ref)
+
+
+def test_dsml_scene_steps_like_the_oracle():
+    """The test scene (three types, one attracting; rectangles, a triangle,
+    single particles) for 300 steps: bit for bit against the oracle."""
+    s = dsml.load(FIXTURE, seed=3)
+    steps = 300
+    out = gpu_run(s.system, s.state(), steps, chunks=[1, 99, 200])
+    ref = PortOracle("f32").run(s.system, s.state(), steps)
+    for k in ("pos", "vel", "theta", "omega", "radius", "mass", "id", "type"):
+        assert same(out[k], ref[k]), k
+
+
+def test_runner_writes_the_reference_csv(tmp_path):
+    """output.csv from the runner equals, line for line, the C formatter of
+    the reference's line applied to an independent run's followed rows; the
+    frames are PPM images of the scene's size."""
+    from demso_b200 import run as R
+    csv = tmp_path / "output.csv"
+    frames = tmp_path / "frames"
+    res = R.run(FIXTURE, steps=60, seed=3, csv=str(csv), frames=str(frames), frame_every=30)
+    assert res["followed"] == [0, 2, 7, 40] and res["followed_out_of_range"] == []
+    lines = csv.read_text().splitlines(keepends=True)
+    assert len(lines) == 60
+    s = dsml.load(FIXTURE, seed=3)
+    import torch
+    import demso_b200 as D
+    sim = D.Simulation(s.system, capacity=s.n, flags=D.CTX_PRESSURE | D.CTX_ACCEL)
+    st = s.state()
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int32) if a.dtype == np.uint32
+                                   else np.ascontiguousarray(a))
+    sim.set_state(t(st["pos"]), t(st["vel"]), t(st["theta"]), t(st["omega"]), t(st["radius"]),
+                  t(st["mass"]), t(st["id"]), t(st["type"]))
+    ro = RenderOracle()
+    for k in range(1, 61):
+        sim.step(1)
+        rows = sim.followed([0, 2, 7, 40])
+        assert lines[k - 1] == ro.followed_line(output.elapsed_time(s.time_step, k), rows), k
+    sim.close()
+    names = sorted(os.listdir(frames))
+    assert names == ["frame_0000000.ppm", "frame_0000030.ppm", "frame_0000060.ppm"]
+    head = open(frames / names[-1], "rb").read(32)
+    assert head.startswith(b"P6\n720 480\n255\n")
