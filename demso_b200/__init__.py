@@ -259,6 +259,33 @@ class Simulation:
     def kernels_per_step(self) -> int:
         return int(load().dem_kernels_per_step(self._h))
 
+    def set_control(self, pos, radius, material=0, vel=(0.0, 0.0), theta=0.0, omega=0.0,
+                    drift=(0.0, 0.0), wrap_y=None, wrap_x=None, stream=None) -> None:
+        """The control particle (dem_set_control); ``wrap_y`` = (below, to) and
+        ``wrap_x`` = (above, to), None for no wrap.  ``set_control(None, 0)``
+        removes it."""
+        import ctypes as C
+        if pos is None:
+            check(load().dem_set_control(self._h, None, _stream(stream)))
+            return
+        c = _lib.DemControl()
+        c.pos[0], c.pos[1] = pos
+        c.vel[0], c.vel[1] = vel
+        c.theta, c.omega, c.radius, c.material = theta, omega, radius, material
+        c.drift[0], c.drift[1] = drift
+        nan = float("nan")
+        c.wrapYBelow, c.wrapYTo = wrap_y if wrap_y is not None else (nan, nan)
+        c.wrapXAbove, c.wrapXTo = wrap_x if wrap_x is not None else (nan, nan)
+        check(load().dem_set_control(self._h, C.byref(c), _stream(stream)))
+
+    def control(self, stream=None):
+        """(position (x, y), reaction (fx, fy, moment) of the last step)."""
+        import ctypes as C
+        c = _lib.DemControl()
+        r = (C.c_float * 3)()
+        check(load().dem_get_control(self._h, C.byref(c), r, _stream(stream)))
+        return (c.pos[0], c.pos[1]), (r[0], r[1], r[2])
+
     def render(self, params, image=None, stream=None):
         """The disk splat of the current state (dem_render) into a CUDA uint8
         tensor of shape (imageDIMy, imageDIMx, 4), row 0 at the bottom."""

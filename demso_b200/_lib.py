@@ -57,6 +57,13 @@ class DemDsmlType(C.Structure):
 DSML_NO_JITTER = 1  # DEM_DSML_NO_JITTER
 
 
+class DemControl(C.Structure):
+    _fields_ = [("pos", C.c_float * 2), ("vel", C.c_float * 2), ("theta", C.c_float),
+                ("omega", C.c_float), ("radius", C.c_float), ("material", C.c_uint32),
+                ("drift", C.c_double * 2), ("wrapYBelow", C.c_double), ("wrapYTo", C.c_double),
+                ("wrapXAbove", C.c_double), ("wrapXTo", C.c_double)]
+
+
 class DemRenderParams(C.Structure):
     _fields_ = [("imageDIMx", C.c_uint32), ("imageDIMy", C.c_uint32), ("bgColor", C.c_uint32),
                 ("viewRotations", C.c_uint32), ("colorByPressure", C.c_uint32),
@@ -97,6 +104,8 @@ SIGNATURES = [
     ("dem_adj_backward", C.c_int, [_P, _P, _P, _P, C.POINTER(C.c_double), _P]),
     ("dem_scene_rsa", C.c_int, [_U, _P, C.c_float, C.c_float, C.c_uint64, _U, _U, _P,
                                 C.POINTER(_U)]),
+    ("dem_set_control", C.c_int, [_P, C.POINTER(DemControl), _P]),
+    ("dem_get_control", C.c_int, [_P, C.POINTER(DemControl), C.POINTER(C.c_float), _P]),
     ("dem_render_particles", C.c_int, [_SYS, _P, _P, _P, _P, _P, _U,
                                        C.POINTER(DemRenderParams), _P, _P, _P]),
     ("dem_render", C.c_int, [_P, C.POINTER(DemRenderParams), _P, _P]),

@@ -301,6 +301,14 @@ struct DemContext {
     std::vector<KParams> hTable;
     uint32_t* spec = nullptr;
     std::vector<uint32_t> partOff;
+    // the control particle (dem_set_control): device state, reaction vectors
+    // (3 n floats), block partials and the reaction of the last step
+    bool ctlOn = false;
+    void* ctlBlock = nullptr;
+    ControlDev* dCtl = nullptr;
+    float* ctlVec = nullptr;
+    float* ctlPartials = nullptr;
+    float* ctlOut = nullptr;
     // dem_render's per-pixel owner scratch
     uint32_t* renderOwner = nullptr;
     size_t renderOwnerWords = 0;
@@ -431,12 +439,17 @@ cudaError_t enqueue_sort_phase(DemContext* c, int kind, cudaStream_t st, int* la
 // Collide + integrate + next hash over the sorted set made by the sort phase.
 cudaError_t enqueue_step_kernel(DemContext* c, cudaStream_t st, int* launches) {
     const int b = c->cur ^ 1;
+    ControlArgs ctl{};
+    if (c->ctlOn) ctl = ControlArgs{c->dCtl, c->ctlVec, c->ctlVec + c->capacity,
+                                    c->ctlVec + 2ull * c->capacity};
     cudaError_t e = launch_step(c->P, c->dyn[1], c->stat[b], c->skey[b], c->cells[b], c->dyn[0],
                                 c->keys, (c->flags & DEM_CTX_PRESSURE) ? c->pressure : nullptr,
                                 (c->flags & DEM_CTX_ACCEL) ? c->acc : nullptr,
                                 (c->flags & DEM_CTX_ACCEL) ? c->alpha : nullptr, c->errFlag, c->n,
-                                sink_of(c), st, c->nspec ? c->dTable : nullptr, c->spec);
+                                sink_of(c), st, c->nspec ? c->dTable : nullptr, c->spec, ctl);
     if (launches) ++*launches;
+    if (e == cudaSuccess && c->ctlOn)
+        e = launch_control_post(ctl, c->dCtl, c->n, c->ctlPartials, c->ctlOut, st, launches);
     return e;
 }
 
@@ -461,7 +474,7 @@ int build_graph(DemContext* c, int what, int parity) {
     e = cudaGraphInstantiate(slot, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(e, "graph instantiate");
-    if (what == 1) c->launchesPerStep = launches + 1;  // + the step kernel
+    if (what == 1) c->launchesPerStep = launches + 1 + (c->ctlOn ? 2 : 0);  // + the step graph
     return DEM_OK;
 }
 
@@ -650,6 +663,7 @@ extern "C" int dem_destroy(DemContext* c) {
     cudaFree(c->followRows);
     cudaFree(c->adjCheck);
     cudaFree(c->renderOwner);
+    cudaFree(c->ctlBlock);
     cudaFree(c->dTable);
     cudaFree(c->spec);
     cudaFree(c->incScratch);
@@ -971,6 +985,7 @@ extern "C" int dem_render(DemContext* c, const DemRenderParams* rp, void* image,
     const size_t words = (size_t)rp->imageDIMx * rp->imageDIMy;
     if (c->renderOwnerWords < words) {
         cudaFree(c->renderOwner);
+    cudaFree(c->ctlBlock);
         c->renderOwner = nullptr;
         c->renderOwnerWords = 0;
         DEM_TRY_CUDA(cudaMalloc(&c->renderOwner, 4 * words), "cudaMalloc render scratch");
@@ -983,6 +998,84 @@ extern "C" int dem_render(DemContext* c, const DemRenderParams* rp, void* image,
                                (c->flags & DEM_CTX_PRESSURE) ? c->pressure : nullptr, c->n,
                                c->renderOwner, static_cast<uchar4*>(image), (cudaStream_t)stream),
                  "render");
+    return DEM_OK;
+}
+
+extern "C" int dem_set_control(DemContext* c, const DemControl* ctl, void* stream) {
+    if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    (void)stream;
+    if (!ctl) {
+        if (c->ctlOn) {
+            c->ctlOn = false;
+            drop_graphs(c);
+        }
+        return DEM_OK;
+    }
+    if (c->nspec) return fail(DEM_ERR_INVALID_ARG, "the control particle takes a single scene");
+    if (ctl->material >= c->sys.numMaterials || (!c->typed && ctl->material != 0))
+        return fail(DEM_ERR_INVALID_ARG, "control material %u (the context has %u)", ctl->material,
+                    c->typed ? c->sys.numMaterials : 1u);
+    if (!(ctl->radius > 0.0f) || !std::isfinite(ctl->radius))
+        return fail(DEM_ERR_INVALID_ARG, "control radius must be positive and finite");
+    if (!c->ctlBlock) {
+        const size_t cap = c->capacity ? c->capacity : 1;
+        const size_t blocks = (cap + 511) / 512 + 1;
+        const size_t bytes = al256(sizeof(ControlDev)) + al256(12 * cap) + al256(12 * blocks) + 256;
+        DEM_TRY_CUDA(cudaMalloc(&c->ctlBlock, bytes), "cudaMalloc control particle");
+        DEM_TRY_CUDA(cudaMemset(c->ctlBlock, 0, bytes), "clear control particle");
+        char* q = static_cast<char*>(c->ctlBlock);
+        c->dCtl = reinterpret_cast<ControlDev*>(q); q += al256(sizeof(ControlDev));
+        c->ctlVec = reinterpret_cast<float*>(q); q += al256(12 * cap);
+        c->ctlPartials = reinterpret_cast<float*>(q); q += al256(12 * blocks);
+        c->ctlOut = reinterpret_cast<float*>(q);
+    }
+    ControlDev d;
+    d.pos = make_float2(ctl->pos[0], ctl->pos[1]);
+    d.vel = make_float2(ctl->vel[0], ctl->vel[1]);
+    d.theta = ctl->theta;
+    d.omega = ctl->omega;
+    d.radius = ctl->radius;
+    d.mat = ctl->material;
+    d.drift[0] = ctl->drift[0];
+    d.drift[1] = ctl->drift[1];
+    d.wrapYBelow = ctl->wrapYBelow;
+    d.wrapYTo = ctl->wrapYTo;
+    d.wrapXAbove = ctl->wrapXAbove;
+    d.wrapXTo = ctl->wrapXTo;
+    DEM_TRY_CUDA(cudaMemcpy(c->dCtl, &d, sizeof(d), cudaMemcpyHostToDevice), "set control");
+    if (!c->ctlOn) {
+        c->ctlOn = true;
+        drop_graphs(c);
+    }
+    return DEM_OK;
+}
+
+extern "C" int dem_get_control(DemContext* c, DemControl* ctl, float* reaction, void* stream) {
+    if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    if (!c->ctlOn) return fail(DEM_ERR_INVALID_ARG, "no control particle");
+    cudaStream_t st = (cudaStream_t)stream;
+    ControlDev d;
+    DEM_TRY_CUDA(cudaMemcpyAsync(&d, c->dCtl, sizeof(d), cudaMemcpyDeviceToHost, st), "get control");
+    float r[3] = {0, 0, 0};
+    DEM_TRY_CUDA(cudaMemcpyAsync(r, c->ctlOut, sizeof(r), cudaMemcpyDeviceToHost, st), "get reaction");
+    DEM_TRY_CUDA(cudaStreamSynchronize(st), "sync");
+    if (ctl) {
+        ctl->pos[0] = d.pos.x;
+        ctl->pos[1] = d.pos.y;
+        ctl->vel[0] = d.vel.x;
+        ctl->vel[1] = d.vel.y;
+        ctl->theta = d.theta;
+        ctl->omega = d.omega;
+        ctl->radius = d.radius;
+        ctl->material = d.mat;
+        ctl->drift[0] = d.drift[0];
+        ctl->drift[1] = d.drift[1];
+        ctl->wrapYBelow = d.wrapYBelow;
+        ctl->wrapYTo = d.wrapYTo;
+        ctl->wrapXAbove = d.wrapXAbove;
+        ctl->wrapXTo = d.wrapXTo;
+    }
+    if (reaction) memcpy(reaction, r, sizeof(r));
     return DEM_OK;
 }
 
@@ -1102,6 +1195,7 @@ bool has_attraction_host(const KParams& P) {
 int adj_check_context(DemContext* c) {
     if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
     if (c->typed) return fail(DEM_ERR_INVALID_ARG, "the adjoint takes a single material");
+    if (c->ctlOn) return fail(DEM_ERR_INVALID_ARG, "the adjoint has no control particle");
     if (!(c->flags & DEM_CTX_ACCEL)) return fail(DEM_ERR_INVALID_ARG, "create the context with DEM_CTX_ACCEL");
     const uint32_t ns = c->nspec ? c->nspec : 1u;
     for (uint32_t s = 0; s < ns; ++s) {

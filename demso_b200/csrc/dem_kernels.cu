@@ -429,7 +429,7 @@ __device__ __forceinline__ void finish_particle(
 // collideD + integrateSystemD + calcHashD of the next step for one particle.
 // The acceleration stays in registers instead of a round trip through HBM;
 // the arithmetic is the same expressions in the same order.
-template <bool TYPED, bool ATTRACT, bool CULL>
+template <bool TYPED, bool ATTRACT, bool CULL, bool CONTROL = false>
 __device__ __forceinline__ void step_particle(const KParams& P, uint32_t i, DynSet in,
                                               StatSet inS,
                                               const uint32_t* __restrict__ sortedKey,
@@ -438,7 +438,8 @@ __device__ __forceinline__ void step_particle(const KParams& P, uint32_t i, DynS
                                               float* __restrict__ pressure,
                                               float2* __restrict__ acc,
                                               float* __restrict__ alpha,
-                                              uint32_t* __restrict__ errFlag, MoverSinkArgs sink) {
+                                              uint32_t* __restrict__ errFlag, MoverSinkArgs sink,
+                                              ControlArgs ctl = ControlArgs{}) {
     Dyn s;
     s.p = in.pos[i];
     s.v = in.vel[i];
@@ -463,20 +464,94 @@ __device__ __forceinline__ void step_particle(const KParams& P, uint32_t i, DynS
                                                in.omega, inS.radius, inS.type,
                                                PackedCells{cellRange}, f, moment, pr);
     }
+    if (CONTROL) {
+        // particles_kernel.cuh:520-541: the contact (and attraction) with the
+        // control particle after the 3x3 cells; its force is added once, the
+        // reaction is stored for the reduction
+        const ControlDev c = *ctl.c;
+        const float4 pc = TYPED ? P.pair[mat * P.nmat + c.mat] : P.pair[0];
+        float mc = 0.0f;
+        float2 fc = pair_force(s.p, c.pos, s.v, c.vel, s.w, c.omega, r, c.radius, pc, P.dt, mc,
+                               pr);
+        if (ATTRACT) {
+            const float2 fa = pair_attract(s.p, c.pos, r, c.radius, P.at[mat], P.at[c.mat], pr);
+            fc.x += fa.x;
+            fc.y += fa.y;
+        }
+        f.x += fc.x;
+        f.y += fc.y;
+        moment += mc;
+        ctl.fx[i] = -fc.x;
+        ctl.fy[i] = -fc.y;
+        ctl.fm[i] = -mc / r * c.radius;
+    }
     finish_particle<TYPED>(P, i, s, f, moment, pr, r, mat, key, in, inS, cellRange, out, nextHash,
                            pressure, acc, alpha, errFlag, sink);
 }
 
-template <bool TYPED, bool ATTRACT, bool CULL>
+template <bool TYPED, bool ATTRACT, bool CULL, bool CONTROL>
 __global__ void __launch_bounds__(kCollideThreads, 8)
 step_kernel(KParams P, DynSet in, StatSet inS, const uint32_t* __restrict__ sortedKey,
             const uint2* __restrict__ cellRange, DynSet out, uint32_t* __restrict__ nextHash,
             float* __restrict__ pressure, float2* __restrict__ acc, float* __restrict__ alpha,
-            uint32_t* __restrict__ errFlag, uint32_t n, MoverSinkArgs sink) {
+            uint32_t* __restrict__ errFlag, uint32_t n, MoverSinkArgs sink, ControlArgs ctl) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    step_particle<TYPED, ATTRACT, CULL>(P, i, in, inS, sortedKey, cellRange, out, nextHash,
-                                        pressure, acc, alpha, errFlag, sink);
+    step_particle<TYPED, ATTRACT, CULL, CONTROL>(P, i, in, inS, sortedKey, cellRange, out,
+                                                 nextHash, pressure, acc, alpha, errFlag, sink,
+                                                 ctl);
+}
+
+// reduceVecD (particles_kernel.cuh:551-578) for the three reaction vectors,
+// launched as collide launches it (functions.cu:486-488): blocks of
+// min(512, n) threads, a shared-memory tree that halves the block size.
+constexpr int kControlThreads = 512;
+__global__ void __launch_bounds__(kControlThreads)
+control_reduce_kernel(ControlArgs ctl, uint32_t n, float* __restrict__ partials) {
+    __shared__ float cache[3][kControlThreads];
+    const uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = threadIdx.x;
+    const bool in = index < n;
+    cache[0][t] = in ? ctl.fx[index] : 0.0f;
+    cache[1][t] = in ? ctl.fy[index] : 0.0f;
+    cache[2][t] = in ? ctl.fm[index] : 0.0f;
+    __syncthreads();
+    for (int i = blockDim.x / 2; i != 0; i /= 2) {
+        if (t < i) {
+            cache[0][t] += cache[0][t + i];
+            cache[1][t] += cache[1][t + i];
+            cache[2][t] += cache[2][t + i];
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        partials[blockIdx.x] = cache[0][0];
+        partials[gridDim.x + blockIdx.x] = cache[1][0];
+        partials[2 * gridDim.x + blockIdx.x] = cache[2][0];
+    }
+}
+
+// the host's sum of the block results in block order (functions.cu:511-519),
+// then the host's move of the control particle (main.cu:511-514): float +=
+// double, and the wraps
+__global__ void control_sum_move_kernel(ControlDev* __restrict__ c,
+                                        const float* __restrict__ partials, uint32_t blocks,
+                                        float* __restrict__ out) {
+    float sx = 0.0f, sy = 0.0f, sm = 0.0f;
+    for (uint32_t b = 0; b < blocks; ++b) {
+        sx += partials[b];
+        sy += partials[blocks + b];
+        sm += partials[2 * blocks + b];
+    }
+    out[0] = sx;
+    out[1] = sy;
+    out[2] = sm;
+    float2 p = c->pos;
+    p.x = (float)((double)p.x + c->drift[0]);
+    p.y = (float)((double)p.y + c->drift[1]);
+    if ((double)p.y < c->wrapYBelow) p.y = (float)c->wrapYTo;
+    if ((double)p.x > c->wrapXAbove) p.x = (float)c->wrapXTo;
+    c->pos = p;
 }
 
 // Batched form: particle slot i belongs to specimen spec[i] (slots of a
@@ -673,7 +748,7 @@ cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t
                         const uint2* cellRange, DynSet out, uint32_t* nextHash, float* pressure,
                         float2* acc, float* alpha, uint32_t* errFlag, uint32_t n,
                         MoverSinkArgs sink, cudaStream_t st, const KParams* table,
-                        const uint32_t* spec) {
+                        const uint32_t* spec, ControlArgs ctl) {
     if (n == 0) return cudaSuccess;
     const bool typed = inS.type != nullptr && P.nmat > 1;
     const bool attract = has_attraction(P);
@@ -685,11 +760,14 @@ cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t
             step_kernel_batched<T, A, C><<<b, kCollideThreads, 0, st>>>(                       \
                 table, spec, in, inS, sortedKey, cellRange, out, nextHash, pressure, acc, alpha, \
                 errFlag, n, sink);                                                             \
+        else if (ctl.c)                                                                        \
+            step_kernel<T, A, C, true><<<b, kCollideThreads, 0, st>>>(                         \
+                P, in, inS, sortedKey, cellRange, out, nextHash, pressure, acc, alpha, errFlag, \
+                n, sink, ctl);                                                                 \
         else                                                                                   \
-            step_kernel<T, A, C><<<b, kCollideThreads, 0, st>>>(P, in, inS, sortedKey,         \
-                                                                cellRange, out, nextHash,      \
-                                                                pressure, acc, alpha, errFlag, \
-                                                                n, sink);                      \
+            step_kernel<T, A, C, false><<<b, kCollideThreads, 0, st>>>(                        \
+                P, in, inS, sortedKey, cellRange, out, nextHash, pressure, acc, alpha, errFlag, \
+                n, sink, ctl);                                                                 \
     } while (0)
     if (typed) {
         if (attract) DEM_STEP(true, true, false);
@@ -701,6 +779,16 @@ cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t
         else DEM_STEP(false, false, false);
     }
 #undef DEM_STEP
+    return cudaGetLastError();
+}
+
+cudaError_t launch_control_post(ControlArgs ctl, ControlDev* c, uint32_t n, float* partials,
+                                float* out, cudaStream_t st, int* launches) {
+    const uint32_t threads = n < (uint32_t)kControlThreads ? (n ? n : 1u) : (uint32_t)kControlThreads;
+    const uint32_t blocks = n ? (n + threads - 1) / threads : 0u;
+    if (blocks) control_reduce_kernel<<<blocks, threads, 0, st>>>(ctl, n, partials);
+    control_sum_move_kernel<<<1, 1, 0, st>>>(c, partials, blocks, out);
+    if (launches) *launches += blocks ? 2 : 1;
     return cudaGetLastError();
 }
 

@@ -70,11 +70,33 @@ struct MoverSinkArgs {
     uint32_t* ctrl;
     uint32_t moverCap;
 };
+// The control ("big") particle of the reference built with USE_BIG_PARTICLE 1
+// (device memory, read by the step kernel and moved by control_move_kernel).
+struct ControlDev {
+    float2 pos, vel;
+    float theta, omega, radius;
+    uint32_t mat;
+    double drift[2];
+    double wrapYBelow, wrapYTo, wrapXAbove, wrapXTo;  // NaN: no wrap
+};
+// Step-kernel outputs of the control particle: per-particle reaction
+// vectors (-f.x, -f.y, -m / r * rControl), or c == null when there is none.
+struct ControlArgs {
+    const ControlDev* c;
+    float* fx;
+    float* fy;
+    float* fm;
+};
 cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t* sortedKey,
                         const uint2* cellRange, DynSet out, uint32_t* nextHash, float* pressure,
                         float2* acc, float* alpha, uint32_t* errFlag, uint32_t n,
                         MoverSinkArgs sink, cudaStream_t st, const KParams* table = nullptr,
-                        const uint32_t* spec = nullptr);
+                        const uint32_t* spec = nullptr, ControlArgs ctl = ControlArgs{});
+// After the step kernel: the reaction sums (reduceVecD's blocks, then their
+// sum in block order: out[0..2] = force x, force y, moment) and the control
+// particle's move.  partials: 3 * ceil(n / min(512, n)) floats.
+cudaError_t launch_control_post(ControlArgs ctl, ControlDev* c, uint32_t n, float* partials,
+                                float* out, cudaStream_t st, int* launches);
 
 // Reorder with interleaved (start, end) cell ranges; resets the ranges first.
 cudaError_t launch_reorder_packed(uint2* cellRange, DynSet sorted, StatSet sortedS,

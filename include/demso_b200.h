@@ -249,6 +249,34 @@ int dem_get_followed(DemContext* ctx, const uint32_t* ids, uint32_t count, float
 int dem_profile_begin(DemContext* ctx, uint32_t maxSteps);
 int dem_profile_end(DemContext* ctx, float* ms, uint32_t* steps);
 
+/* The control ("big") particle of the reference built with USE_BIG_PARTICLE
+ * 1 (main.cuh:29): a kinematic disk of `material` that every particle meets
+ * after its 3x3 neighbour cells (particles_kernel.cuh:520-541: contact, and
+ * attraction where a material attracts).  The reaction on it -- the sums of
+ * -f.x, -f.y and -m / r * radius over the particles -- is reduced on the
+ * device as the reference reduces it (reduceVecD over blocks of
+ * min(512, n), functions.cu:486-519, then the block sums in order), with no
+ * per-step copy to the host.  After every step the particle moves as the
+ * reference's host moves it (main.cu:511-514): pos += drift (float += double),
+ * then y < wrapYBelow -> wrapYTo and x > wrapXAbove -> wrapXTo (NaN: no
+ * wrap); the reference's values are drift (0, -0.005), wrapY (-1, 10.5),
+ * wrapX (Lx + 0.5, -0.5), start (5, 9.5), vel 0.  The control particle
+ * takes a single scene (not a batch); a single-material context needs
+ * material 0.  Off by default; no reference counterpart as a function. */
+typedef struct DemControl {
+    float pos[2], vel[2];
+    float theta, omega, radius;
+    uint32_t material;
+    double drift[2];
+    double wrapYBelow, wrapYTo;
+    double wrapXAbove, wrapXTo;
+} DemControl;
+/* Sets (or, with NULL, removes) the control particle. */
+int dem_set_control(DemContext* ctx, const DemControl* control, void* stream);
+/* Its current state and the reaction (fx, fy, moment) of the last step;
+ * synchronises `stream`.  Either output may be NULL. */
+int dem_get_control(DemContext* ctx, DemControl* control, float* reaction, void* stream);
+
 /* ---------------------------------------------------------------------------
  * Headless output
  * ------------------------------------------------------------------------- */

@@ -229,10 +229,38 @@ static R2 attract_spheres(const Sys* s, R2 pA, R2 pB, REAL rA, REAL rB, uint32_t
 /* functions.cu:441 (pressure <- 0) and particles_kernel.cuh:459-549 with
  * USE_BIG_PARTICLE 0: 3x3 neighbour cells, y outer, x inner; each cell's
  * subtotal (collideCell, :346-385) is added to the running force. */
+static void collide_impl(const OrcSystem* os, uint32_t n, const REAL* pos, const REAL* vel,
+                         const REAL* omega, const REAL* radius, const REAL* mass,
+                         const uint32_t* type, const uint32_t* cellStart, const uint32_t* cellEnd,
+                         REAL* acc, REAL* alpha, float* pressure, const OrcControl* ctl,
+                         REAL* fx, REAL* fy, REAL* fm);
+
 void orc_collide(const OrcSystem* os, uint32_t n, const REAL* pos, const REAL* vel,
                  const REAL* omega, const REAL* radius, const REAL* mass, const uint32_t* type,
                  const uint32_t* cellStart, const uint32_t* cellEnd, REAL* acc, REAL* alpha,
                  float* pressure) {
+    collide_impl(os, n, pos, vel, omega, radius, mass, type, cellStart, cellEnd, acc, alpha,
+                 pressure, NULL, NULL, NULL, NULL);
+}
+
+/* particles_kernel.cuh:459-549 with USE_BIG_PARTICLE 1 and USE_ATOMIC 0: after
+ * the 3x3 cells, the contact (and attraction) with the control particle is
+ * added to the force and moment, and -f.x, -f.y and -m / rA * rControl are
+ * stored per particle for the reduction. */
+void orc_collide_control(const OrcSystem* os, uint32_t n, const REAL* pos, const REAL* vel,
+                         const REAL* omega, const REAL* radius, const REAL* mass,
+                         const uint32_t* type, const uint32_t* cellStart,
+                         const uint32_t* cellEnd, REAL* acc, REAL* alpha, float* pressure,
+                         const OrcControl* ctl, REAL* fx, REAL* fy, REAL* fm) {
+    collide_impl(os, n, pos, vel, omega, radius, mass, type, cellStart, cellEnd, acc, alpha,
+                 pressure, ctl, fx, fy, fm);
+}
+
+static void collide_impl(const OrcSystem* os, uint32_t n, const REAL* pos, const REAL* vel,
+                         const REAL* omega, const REAL* radius, const REAL* mass,
+                         const uint32_t* type, const uint32_t* cellStart, const uint32_t* cellEnd,
+                         REAL* acc, REAL* alpha, float* pressure, const OrcControl* ctl,
+                         REAL* fx, REAL* fy, REAL* fm) {
     Sys s = load_sys(os);
     for (uint32_t i = 0; i < n; ++i) {
         R2 p = ld2(pos, i), v = ld2(vel, i);
@@ -263,6 +291,22 @@ void orc_collide(const OrcSystem* os, uint32_t n, const REAL* pos, const REAL* v
                 force.x += fc.x;
                 force.y += fc.y;
             }
+        }
+        if (ctl) {
+            REAL mc = 0;
+            const R2 cp = r2((REAL)ctl->pos[0], (REAL)ctl->pos[1]);
+            const REAL cr = (REAL)ctl->radius;
+            R2 f = collide_spheres(&s, p, cp, v, r2((REAL)ctl->vel[0], (REAL)ctl->vel[1]), w,
+                                   (REAL)ctl->omega, r, cr, mi, ctl->mat, &mc, &pr);
+            const R2 fa = attract_spheres(&s, p, cp, r, cr, mi, ctl->mat, &pr);
+            f.x += fa.x;
+            f.y += fa.y;
+            force.x += f.x;
+            force.y += f.y;
+            moment += mc;
+            fx[i] = -f.x;
+            fy[i] = -f.y;
+            fm[i] = -mc / r * cr;
         }
         REAL m = mass[i];
         st2(acc, i, r2(force.x / m, force.y / m));
@@ -378,3 +422,37 @@ void orc_step(const OrcSystem* os, uint32_t n,
 }
 
 int orc_real_bytes(void) { return (int)sizeof(REAL); }
+
+/* reduceVecD (particles_kernel.cuh:551-578) over blocks of
+ * min(512, n) entries as collide launches it (functions.cu:486-488), then the
+ * host's sum of the block results in block order (functions.cu:511-519), in
+ * float. */
+float orc_control_reduce(uint32_t n, const float* v) {
+    if (n == 0) return 0.0f;
+    const uint32_t threads = n < 512u ? n : 512u;
+    const uint32_t blocks = (n % threads != 0) ? n / threads + 1 : n / threads;
+    float* cache = (float*)malloc(sizeof(float) * threads);
+    float sum = 0.0f;
+    for (uint32_t b = 0; b < blocks; ++b) {
+        for (uint32_t t = 0; t < threads; ++t) {
+            const uint32_t idx = b * threads + t;
+            cache[t] = idx < n ? v[idx] : 0.0f;
+        }
+        for (uint32_t i = threads / 2; i != 0; i /= 2)
+            for (uint32_t t = 0; t < i; ++t) cache[t] += cache[t + i];
+        sum += cache[0];
+    }
+    free(cache);
+    return sum;
+}
+
+/* main.cu:511-514: the host moves the control particle after each step, in
+ * double rounded to float as `float += double` does. */
+void orc_control_move(OrcControl* c) {
+    c->pos[0] = (float)((double)(float)c->pos[0] + c->drift[0]);
+    c->pos[1] = (float)((double)(float)c->pos[1] + c->drift[1]);
+    if (c->wrapYBelow == c->wrapYBelow && (float)c->pos[1] < c->wrapYBelow)
+        c->pos[1] = (float)c->wrapYTo;
+    if (c->wrapXAbove == c->wrapXAbove && (double)(float)c->pos[0] > c->wrapXAbove)
+        c->pos[0] = (float)c->wrapXTo;
+}

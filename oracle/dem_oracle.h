@@ -31,4 +31,17 @@ typedef struct OrcSystem {
     double mat[ORC_MAX_MATERIALS][6];
 } OrcSystem;
 
+/* The control ("big") particle of the reference built with
+ * USE_BIG_PARTICLE 1: a kinematic disk of material `mat` touching every
+ * particle (particles_kernel.cuh:520-541), moved by the host after each step
+ * (main.cu:511-514 with drift (0, -0.005), wrapY (-1 -> 10.5) and wrapX
+ * (Lx + 0.5 -> -0.5)).  A wrap is off when its threshold is NaN. */
+typedef struct OrcControl {
+    double pos[2], vel[2];
+    double theta, omega, radius;
+    uint32_t mat, reserved;
+    double drift[2];
+    double wrapYBelow, wrapYTo, wrapXAbove, wrapXTo;
+} OrcControl;
+
 #endif

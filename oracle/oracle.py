@@ -94,6 +94,29 @@ def _orc_system(s: System) -> _OrcSystem:
     return o
 
 
+class OrcControl(C.Structure):
+    """The control particle (dem_oracle.h)."""
+    _fields_ = [("pos", C.c_double * 2), ("vel", C.c_double * 2), ("theta", C.c_double),
+                ("omega", C.c_double), ("radius", C.c_double), ("mat", C.c_uint32),
+                ("reserved", C.c_uint32), ("drift", C.c_double * 2), ("wrapYBelow", C.c_double),
+                ("wrapYTo", C.c_double), ("wrapXAbove", C.c_double), ("wrapXTo", C.c_double)]
+
+
+def orc_control(ctl: dict) -> OrcControl:
+    """dict keys: pos, vel, theta, omega, radius, mat, drift, wrap_y (below, to) and
+    wrap_x (above, to); missing wraps are off."""
+    c = OrcControl()
+    c.pos[0], c.pos[1] = ctl["pos"]
+    c.vel[0], c.vel[1] = ctl.get("vel", (0.0, 0.0))
+    c.theta, c.omega = ctl.get("theta", 0.0), ctl.get("omega", 0.0)
+    c.radius, c.mat = ctl["radius"], int(ctl.get("mat", 0))
+    c.drift[0], c.drift[1] = ctl.get("drift", (0.0, 0.0))
+    nan = float("nan")
+    c.wrapYBelow, c.wrapYTo = ctl.get("wrap_y", (nan, nan))
+    c.wrapXAbove, c.wrapXTo = ctl.get("wrap_x", (nan, nan))
+    return c
+
+
 def build(ref_root: Optional[str] = None, quiet: bool = True) -> None:
     """Compile the oracles (and the reference host build when its tree exists)."""
     targets = ["all"]
@@ -134,6 +157,11 @@ class PortOracle:
                                   rp, rp, _f32p]
         L.orc_integrate.argtypes = [sp, u32, rp, rp, rp, rp, rp, rp, rp, rp, C.c_void_p, _f32p]
         L.orc_signature.restype = C.c_uint64
+        L.orc_collide_control.argtypes = [sp, u32, rp, rp, rp, rp, rp, C.c_void_p, _u32p, _u32p,
+                                          rp, rp, _f32p, C.POINTER(OrcControl), rp, rp, rp]
+        L.orc_control_reduce.argtypes = [u32, _f32p]
+        L.orc_control_reduce.restype = C.c_float
+        L.orc_control_move.argtypes = [C.POINTER(OrcControl)]
         L.orc_step.argtypes = [sp, u32] + [rp] * 6 + [_u32p, C.c_void_p] + [rp] * 6 + \
             [_u32p, _u32p, C.c_void_p] + [rp, rp, _f32p, _u32p, _u32p, _u32p, _u32p]
 
@@ -202,6 +230,53 @@ class PortOracle:
                              np.ascontiguousarray(cell_end, dtype=np.uint32),
                              acc.reshape(-1), alpha, pr)
         return acc, alpha, pr
+
+    def collide_control(self, sys: System, st: dict, cell_start, cell_end, ctl: OrcControl):
+        """collide with the control particle: acc, alpha, pressure and the
+        reaction vectors fx, fy, fm."""
+        pos = self._r(st["pos"])
+        n = pos.shape[0]
+        acc = np.empty((n, 2), self.dt)
+        alpha = np.empty(n, self.dt)
+        pr = np.empty(n, np.float32)
+        fx, fy, fm = (np.zeros(n, self.dt) for _ in range(3))
+        typ = self._tp(st.get("type"))
+        self.lib.orc_collide_control(C.byref(_orc_system(sys)), n, pos.reshape(-1),
+                                     self._r(st["vel"]).reshape(-1), self._r(st["omega"]),
+                                     self._r(st["radius"]), self._r(st["mass"]),
+                                     typ.ctypes.data if typ is not None else None,
+                                     np.ascontiguousarray(cell_start, dtype=np.uint32),
+                                     np.ascontiguousarray(cell_end, dtype=np.uint32),
+                                     acc.reshape(-1), alpha, pr, C.byref(ctl), fx, fy, fm)
+        return acc, alpha, pr, fx, fy, fm
+
+    def control_reduce(self, v) -> np.float32:
+        v = np.ascontiguousarray(v, dtype=np.float32)
+        return np.float32(self.lib.orc_control_reduce(v.size, v))
+
+    def control_move(self, ctl: OrcControl) -> None:
+        self.lib.orc_control_move(C.byref(ctl))
+
+    def run_control(self, sys: System, st: dict, nsteps: int, ctl: OrcControl):
+        """`nsteps` steps with the control particle, each as the reference's
+        SimLooping takes it (main.cu:431-514): hash, sort, reorder, collide
+        with the control particle and its reaction sums, integrate, then the
+        control particle's move.  Returns the final state and the reaction
+        (fx, fy, moment) of every step."""
+        cur = {k: (None if v is None else np.array(v)) for k, v in st.items()}
+        reac = []
+        for _ in range(nsteps):
+            h, ix = self.calc_hash(sys, cur["pos"])
+            h, ix = self.sort(h, ix)
+            cs, ce, srt = self.reorder(sys, h, ix, cur)
+            acc, alpha, pr, fx, fy, fm = self.collide_control(sys, srt, cs, ce, ctl)
+            reac.append((self.control_reduce(fx), self.control_reduce(fy),
+                         self.control_reduce(fm)))
+            pos, vel, th, om, pr = self.integrate(sys, srt, acc, alpha, pr)
+            cur = dict(srt)
+            cur.update(pos=pos, vel=vel, theta=th, omega=om, pressure=pr)
+            self.control_move(ctl)
+        return cur, np.array(reac, np.float32)
 
     def integrate(self, sys: System, st: dict, acc, alpha, pressure):
         """Returns new (pos, vel, theta, omega, pressure); inputs are not modified."""
@@ -316,8 +391,8 @@ class RefHarness:
     (the reference's constant-memory symbols), so one harness per process.
     """
 
-    def __init__(self, threads: Optional[int] = None):
-        path = os.path.join(OUT, "libdemso_ref.so")
+    def __init__(self, threads: Optional[int] = None, control: bool = False):
+        path = os.path.join(OUT, "libdemso_ref_ctrl.so" if control else "libdemso_ref.so")
         if not os.path.isfile(path):
             raise FileNotFoundError("reference host build missing: " + path)
         self.lib = C.CDLL(path)
@@ -338,6 +413,11 @@ class RefHarness:
         L.ref_run.argtypes = [u32] + [_f32p] * 4 + [_u32p] * 3 + [_f32p] * 4 + [_u32p] * 3 + \
             [_f32p, _f32p, _f32p, _u32p, _u32p, _u32p, _u32p]
         L.ref_max_particles.restype = C.c_int
+        if control:
+            f = C.c_float
+            L.ref_set_control.argtypes = [f, f, f, f, f, f, f, f, _f32p]
+            L.ref_set_control.restype = C.c_int
+            L.ref_control_vectors.argtypes = [_f32p, _f32p, _f32p]
         self.threads = L.ref_set_threads(int(threads or 0))
         self.sys = None
         self.n = 0
@@ -357,6 +437,19 @@ class RefHarness:
         if rc != 0:
             raise ValueError("ref_setup failed: %d" % rc)
         self.sys, self.n = sys, n
+
+    def set_control(self, pos, vel, theta, omega, radius, mass, material):
+        """The control particle (control build only), of reference type n."""
+        row = np.ascontiguousarray(material.row(), dtype=np.float32)
+        rc = self.lib.ref_set_control(pos[0], pos[1], vel[0], vel[1], theta, omega, radius, mass,
+                                      row)
+        if rc != 0:
+            raise ValueError("ref_set_control failed")
+
+    def control_vectors(self):
+        fx, fy, fm = (np.empty(self.n, np.float32) for _ in range(3))
+        self.lib.ref_control_vectors(fx, fy, fm)
+        return fx, fy, fm
 
     def calc_hash(self, pos):
         pos = np.ascontiguousarray(pos, dtype=np.float32)

@@ -39,7 +39,11 @@
 typedef unsigned int uint;
 
 #define MAIN_CUH 1
+#ifdef REF_CONTROL
+#define USE_BIG_PARTICLE 1  /* with the control particle, USE_ATOMIC 0 (main.cuh:29-30) */
+#else
 #define USE_BIG_PARTICLE 0
+#endif
 #define USE_ATOMIC 0
 #define MAX_PARTICLES_TYPES (1u << 24)
 
@@ -181,15 +185,66 @@ void ref_reorder(uint32_t* cellStart, uint32_t* cellEnd,
     }
 }
 
+#if USE_BIG_PARTICLE
+/* The control particle (main.cu:141-146, 476-494): its kinematic state and
+ * the per-particle reaction vectors collideD writes (USE_ATOMIC 0). */
+static float2 g_cPos, g_cVel;
+static float g_cTheta, g_cOmega;
+static uint g_cType;
+static std::vector<float> g_fx, g_fy, g_fm;
+
+/* Call after ref_setup: the control particle becomes type n (one past the
+ * particles) with the given radius, mass and material row. */
+int ref_set_control(float px, float py, float vx, float vy, float theta, float omega,
+                    float radius, float mass, const float* row) {
+    const uint n = sisPropD.numParticles;
+    if (n + 1 > MAX_PARTICLES_TYPES) return 1;
+    ParticleProperties& p = partPropD[n];
+    p.radius = radius;
+    p.mass = mass;
+    p.inertia = 2 * p.mass * p.radius * p.radius / 5;
+    p.normalStiffness = row[0];
+    p.shearStiffness = row[1];
+    p.normalDamping = row[2];
+    p.boundaryDamping = row[3];
+    p.frictionCoefficient = row[4];
+    p.attractCoefficient = row[5];
+    g_cPos = make_float2(px, py);
+    g_cVel = make_float2(vx, vy);
+    g_cTheta = theta;
+    g_cOmega = omega;
+    g_cType = n;
+    return 0;
+}
+
+/* The reaction vectors of the last ref_collide (n entries each). */
+void ref_control_vectors(float* fx, float* fy, float* fm) {
+    const size_t n = g_fx.size();
+    memcpy(fx, g_fx.data(), 4 * n);
+    memcpy(fy, g_fy.data(), 4 * n);
+    memcpy(fm, g_fm.data(), 4 * n);
+}
+#endif
+
 void ref_collide(float* pos, float* vel, float* acc, float* omega, float* alpha, uint32_t* type,
                  uint32_t* cellStart, uint32_t* cellEnd, float* pressure) {
     const uint n = sisPropD.numParticles;
     memset(pressure, 0, sizeof(float) * n);
+#if USE_BIG_PARTICLE
+    g_fx.assign(n, 0.0f);
+    g_fy.assign(n, 0.0f);
+    g_fm.assign(n, 0.0f);
+#endif
 #pragma omp parallel for schedule(static)
     for (long long i = 0; i < (long long)n; ++i) {
         set_thread((uint)i, n);
         collideD((float2*)pos, (float2*)vel, (float2*)acc, omega, alpha, type, cellStart,
-                 cellEnd, pressure);
+                 cellEnd,
+#if USE_BIG_PARTICLE
+                 g_cPos, g_cVel, g_cTheta, g_cOmega, g_cType, g_fx.data(), g_fy.data(),
+                 g_fm.data(),
+#endif
+                 pressure);
     }
 }
 
