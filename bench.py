@@ -354,6 +354,94 @@ def measure_adjoint(n: int = 16384, steps: int = 2000, every: int = 100):
                            torch.isfinite(dv).all().item())}
 
 
+# ------------------------------------------------------------------ config 0
+def measure_settling_pile(steps: int = 20000, cpu_sample: int = 2000):
+    """The plain 2D settling pile (4,096 disks, 20,000 steps): wall time of
+    the whole run on the GPU, beside the reference's step functions built
+    for the host (timed on `cpu_sample` of the steps, all host threads)."""
+    import torch
+    import demso_b200 as D
+    from demso_b200 import scenes
+    from oracle import oracle as O
+    sc = scenes.settling_pile()
+    sim = D.Simulation(sc.sys, capacity=sc.n, flags=D.CTX_PRESSURE)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int32) if a.dtype == np.uint32
+                                   else np.ascontiguousarray(a))
+    st = sc.state()
+    sim.set_state(t(st["pos"]), t(st["vel"]), t(st["theta"]), t(st["omega"]), t(st["radius"]),
+                  t(st["mass"]), t(st["id"]))
+    sim.step(10)
+    sim.set_state(t(st["pos"]), t(st["vel"]), t(st["theta"]), t(st["omega"]), t(st["radius"]),
+                  t(st["mass"]), t(st["id"]))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    sim.step(steps)
+    e1.record()
+    torch.cuda.synchronize()
+    sim.check()
+    gpu_s = e0.elapsed_time(e1) * 1e-3
+    sim.close()
+    out = {"workload": "plain 2D settling pile: 4096 disks, radii U[0.9, 1.1] mm, 64x64 "
+                       "jittered lattice in a 0.2 x 0.2 m box, dt 2e-6 s, %d steps" % steps,
+           "gpu_seconds": gpu_s, "gpu_steps_per_s": steps / gpu_s,
+           "gpu_particle_steps_per_s": sc.n * steps / gpu_s}
+    if O.ref_available():
+        h = O.RefHarness(threads=os.cpu_count() or 1)
+        h.setup(sc.sys, sc.radius, sc.mass, None)
+        b = h.make_buffers(sc.state())
+        h.run(b, 10)
+        t0 = time.perf_counter()
+        h.run(b, cpu_sample)
+        cpu_s = (time.perf_counter() - t0) * steps / cpu_sample
+        out.update(cpu_reference_seconds_estimate=cpu_s, cpu_threads=h.threads,
+                   cpu_sample="%d of the %d steps, scaled" % (cpu_sample, steps),
+                   gpu_over_cpu=cpu_s / gpu_s)
+    return out
+
+
+def measure_sweep(sizes, steps: int = 200, warmup: int = 50):
+    """The plain-at-scale workload at several sizes: particle-steps/s and the
+    roofline fractions of the step kernel and of the whole step."""
+    import ctypes as C
+    import torch
+    import demso_b200 as D
+    from demso_b200 import scenes
+    hbm, _ = peaks()
+    rows = []
+    for n in sizes:
+        sc = scenes.plain_at_scale(n)
+        sim = D.Simulation(sc.sys, capacity=sc.n, flags=D.CTX_PRESSURE)
+        t = lambda a: torch.from_numpy(a.view(np.int32) if a.dtype == np.uint32 else a)
+        sim.set_state(t(sc.pos), t(sc.vel), t(sc.theta), t(sc.omega), t(sc.radius), t(sc.mass),
+                      t(sc.id))
+        sim.step(warmup)
+        torch.cuda.synchronize()
+        D.check(D.load().dem_profile_begin(sim.handle, steps))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sim.step(steps)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = (C.c_float * D._lib.NUM_STAGES)()
+        k = C.c_uint32(0)
+        D.check(D.load().dem_profile_end(sim.handle, ms, C.byref(k)))
+        sim.check()
+        sim.close()
+        step_ms = e0.elapsed_time(e1) / steps
+        cells = sc.sys.num_cells
+        kern_ms = ms[2] / max(1, k.value)
+        kb = STEP_KERNEL_BYTES_PER_PARTICLE * sc.n + STEP_KERNEL_BYTES_PER_CELL * cells
+        rows.append({"n": sc.n, "grid": [sc.sys.gx, sc.sys.gy], "ms_per_step": step_ms,
+                     "value": sc.n / (step_ms * 1e-3),
+                     "sort_ms": ms[0] / max(1, k.value), "step_kernel_ms": kern_ms,
+                     "step_kernel_frac": kb / (kern_ms * 1e-3) / 1e9 / hbm,
+                     "whole_step_frac": WHOLE_STEP_BYTES(sc.n, cells) / (step_ms * 1e-3) / 1e9
+                                        / hbm})
+        del sc
+    return rows
+
+
 # ------------------------------------------------------------------ our arm
 def main():
     ap = argparse.ArgumentParser()
@@ -366,6 +454,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-pile", action="store_true")
+    ap.add_argument("--sweep", default=None,
+                    help="comma-separated sizes of the plain-at-scale sweep (e.g. "
+                         "65536,262144,1048576,4194304,16777216)")
     ap.add_argument("--direct", action="store_true",
                     help="launch each kernel directly instead of through CUDA graphs "
                          "(for per-kernel profilers; one host read-back per step)")
@@ -510,6 +602,16 @@ def main():
         except Exception as e:  # reported beside the headline, never instead of it
             batched = {"error": str(e)}
 
+    pile = None
+    if rank == 0 and world == 1 and not args.no_pile:
+        try:
+            pile = measure_settling_pile()
+        except Exception as e:  # reported beside the headline, never instead of it
+            pile = {"error": str(e)}
+    sweep = None
+    if rank == 0 and world == 1 and args.sweep:
+        sweep = measure_sweep([int(v) for v in args.sweep.split(",") if v])
+
     adjoint = None
     if rank == 0 and world == 1 and not args.no_adjoint:
         try:
@@ -536,9 +638,11 @@ def main():
                                "achieved_gbs": whole_bytes / (step_ms * 1e-3) / 1e9,
                                "frac": whole_bytes / (step_ms * 1e-3) / 1e9 / hbm},
                 "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "batched": batched,
-                "adjoint": adjoint,
+                "adjoint": adjoint, "settling_pile": pile,
                 "gpu_launches": kernels_per_step * args.steps,
                 "kernels_per_step": kernels_per_step}
+        if sweep is not None:
+            line["sweep"] = sweep
         print(json.dumps(line), flush=True)
     sim.close()
     if dist is not None:
