@@ -235,12 +235,15 @@ def measure_batched(steps: int, warmup: int, num: int = 4096, loop_sample: int =
     from demso_b200 import scenes
     specimens = scenes.specimen_batch(num=num, seed=0)
     total = sum(sc.n for sc in specimens)
-    b = D.Batch([(sc.sys, sc.n) for sc in specimens], flags=D.CTX_PRESSURE)
+    b = D.Batch([(sc.sys, sc.n) for sc in specimens], flags=D.CTX_PRESSURE | D.CTX_AUTOTUNE)
     st = scenes.concat_specimens(specimens)
     t = lambda a: torch.from_numpy(a.view(np.int32) if a.dtype == np.uint32 else a)
     b.set_state(t(st["pos"]), t(st["vel"]), t(st["theta"]), t(st["omega"]), t(st["radius"]),
                 t(st["mass"]), t(st["id"]))
     b.step(max(3, warmup))
+    while b.step_variant()["tuned"] < 0:
+        b.step(1)
+    shape = b.step_variant()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
@@ -275,6 +278,7 @@ def measure_batched(steps: int, warmup: int, num: int = 4096, loop_sample: int =
             "value": batched, "looped_plain": looped, "ratio": batched / looped,
             "unit": UNIT, "specimens": num, "particles": total, "steps": steps,
             "kernels_per_step": kernels,
+            "step_kernel_shape": [shape["threads"], shape["blocks_per_sm"]],
             "looped_sample": "%d of the %d specimens (every %d-th), %d steps each"
                              % (len(sample), num, max(1, num // loop_sample), lsteps),
             "workload": "batched: specimens with counts log-uniform in [256, 8192], square "
@@ -411,11 +415,14 @@ def measure_sweep(sizes, steps: int = 200, warmup: int = 50):
     rows = []
     for n in sizes:
         sc = scenes.plain_at_scale(n)
-        sim = D.Simulation(sc.sys, capacity=sc.n, flags=D.CTX_PRESSURE)
+        sim = D.Simulation(sc.sys, capacity=sc.n, flags=D.CTX_PRESSURE | D.CTX_AUTOTUNE)
         t = lambda a: torch.from_numpy(a.view(np.int32) if a.dtype == np.uint32 else a)
         sim.set_state(t(sc.pos), t(sc.vel), t(sc.theta), t(sc.omega), t(sc.radius), t(sc.mass),
                       t(sc.id))
         sim.step(warmup)
+        while sim.step_variant()["tuned"] < 0:
+            sim.step(1)
+        shape = sim.step_variant()
         torch.cuda.synchronize()
         D.check(D.load().dem_profile_begin(sim.handle, steps))
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -433,6 +440,7 @@ def measure_sweep(sizes, steps: int = 200, warmup: int = 50):
         kern_ms = ms[2] / max(1, k.value)
         kb = STEP_KERNEL_BYTES_PER_PARTICLE * sc.n + STEP_KERNEL_BYTES_PER_CELL * cells
         rows.append({"n": sc.n, "grid": [sc.sys.gx, sc.sys.gy], "ms_per_step": step_ms,
+                     "step_kernel_shape": [shape["threads"], shape["blocks_per_sm"]],
                      "value": sc.n / (step_ms * 1e-3),
                      "sort_ms": ms[0] / max(1, k.value), "step_kernel_ms": kern_ms,
                      "step_kernel_frac": kb / (kern_ms * 1e-3) / 1e9 / hbm,
@@ -458,6 +466,9 @@ def main():
     ap.add_argument("--sweep", default=None,
                     help="comma-separated sizes of the plain-at-scale sweep (e.g. "
                          "65536,262144,1048576,4194304,16777216)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the step kernel's default launch shape (128 threads x 8 "
+                         "blocks per SM) instead of timing the shapes on the first steps")
     ap.add_argument("--direct", action="store_true",
                     help="launch each kernel directly instead of through CUDA graphs "
                          "(for per-kernel profilers; one host read-back per step)")
@@ -488,7 +499,8 @@ def main():
     sc = scenes.plain_at_scale(args.n, seed=rank)
     n = sc.n
     sim = D.Simulation(sc.sys, capacity=n,
-                       flags=D.CTX_PRESSURE | (D.CTX_DIRECT if args.direct else 0))
+                       flags=D.CTX_PRESSURE | (D.CTX_DIRECT if args.direct else 0)
+                       | (0 if args.no_autotune else D.CTX_AUTOTUNE))
     pin = lambda a: torch.from_numpy(a.view(np.int32) if a.dtype == np.uint32 else a).pin_memory()
     host = {k: pin(getattr(sc, k)) for k in ("pos", "vel", "theta", "omega", "radius", "mass",
                                               "id")}
@@ -496,9 +508,14 @@ def main():
     sim.set_state(host["pos"], host["vel"], host["theta"], host["omega"], host["radius"],
                   host["mass"], host["id"])
     sim.step(args.warmup)
+    # the launch-shape tuner times its variants on the first 24 steps; any it
+    # still needs run here, untimed
+    while sim.step_variant()["tuned"] < 0:
+        sim.step(1)
     torch.cuda.synchronize()
     sim.check()
     kernels_per_step = sim.kernels_per_step()
+    shape = sim.step_variant()
 
     # ---- timed region (device-resident state)
     clocks = Clocks(local)
@@ -563,6 +580,7 @@ def main():
     e2e = None
     if not args.no_e2e:
         sim2 = D.Simulation(sc.sys, capacity=n, flags=D.CTX_PRESSURE | D.CTX_ACCEL)
+        sim2.set_step_variant(shape["variant"])
         out_host = {k: torch.empty_like(v).pin_memory() for k, v in host.items()}
         follow = np.array([n // 3, (2 * n) // 3], dtype=np.uint32)
         rows = np.zeros(12 * follow.size, np.float32)
@@ -640,7 +658,11 @@ def main():
                 "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "batched": batched,
                 "adjoint": adjoint, "settling_pile": pile,
                 "gpu_launches": kernels_per_step * args.steps,
-                "kernels_per_step": kernels_per_step}
+                "kernels_per_step": kernels_per_step,
+                "step_kernel_shape": {"threads": shape["threads"],
+                                      "blocks_per_sm": shape["blocks_per_sm"],
+                                      "tuned": shape["tuned"] == 1,
+                                      "tuner_median_ms": shape["median_ms"]}}
         if sweep is not None:
             line["sweep"] = sweep
         print(json.dumps(line), flush=True)

@@ -19,11 +19,13 @@ from dataclasses import dataclass, field
 from typing import Optional, Sequence
 
 from . import _lib
-from ._lib import CTX_ACCEL, CTX_DIRECT, CTX_PRESSURE, DEM_MAX_MATERIALS, DemError, check, load
+from ._lib import (CTX_ACCEL, CTX_AUTOTUNE, CTX_DIRECT, CTX_PRESSURE, DEM_MAX_MATERIALS, DemError,
+                   check, load)
 
 __all__ = ["Material", "System", "DemError", "calcHash", "sortParticles",
            "reorderDataAndFindCellStart", "collide", "integrateSystem", "Simulation", "Batch",
-           "sort_scratch_bytes", "load", "CTX_PRESSURE", "CTX_ACCEL", "CTX_DIRECT"]
+           "sort_scratch_bytes", "load", "CTX_PRESSURE", "CTX_ACCEL", "CTX_DIRECT",
+           "CTX_AUTOTUNE"]
 
 
 @dataclass
@@ -258,6 +260,20 @@ class Simulation:
 
     def kernels_per_step(self) -> int:
         return int(load().dem_kernels_per_step(self._h))
+
+    def step_variant(self) -> dict:
+        """The step kernel's launch shape (dem_get_step_variant): variant,
+        threads, blocks_per_sm, tuned (1 by the autotuner, 0 fixed, -1 still
+        timing) and the tuner's median ms per variant."""
+        from ._lib import DemStepVariant
+        import ctypes as C
+        v = DemStepVariant()
+        check(load().dem_get_step_variant(self._h, C.byref(v)))
+        return {"variant": v.variant, "threads": v.threads, "blocks_per_sm": v.blocksPerSm,
+                "tuned": v.tuned, "median_ms": [float(x) for x in v.medianMs]}
+
+    def set_step_variant(self, variant: int) -> None:
+        check(load().dem_set_step_variant(self._h, int(variant)))
 
     def set_control(self, pos, radius, material=0, vel=(0.0, 0.0), theta=0.0, omega=0.0,
                     drift=(0.0, 0.0), wrap_y=None, wrap_x=None, stream=None) -> None:

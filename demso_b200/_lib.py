@@ -17,6 +17,8 @@ STATUS = {0: "DEM_OK", 1: "DEM_ERR_INVALID_ARG", 2: "DEM_ERR_CUDA", 3: "DEM_ERR_
 CTX_PRESSURE = 1
 CTX_ACCEL = 2
 CTX_DIRECT = 4
+CTX_AUTOTUNE = 8
+STEP_VARIANTS = 4  # DEM_STEP_VARIANTS
 NUM_STAGES = 3  # DEM_NUM_STAGES: sort, reorder, collide + integrate
 ADJ_NUM_COEF = 7  # DEM_ADJ_NUM_COEF
 
@@ -64,6 +66,11 @@ class DemControl(C.Structure):
                 ("wrapXAbove", C.c_double), ("wrapXTo", C.c_double)]
 
 
+class DemStepVariant(C.Structure):
+    _fields_ = [("variant", C.c_int32), ("threads", C.c_uint32), ("blocksPerSm", C.c_uint32),
+                ("tuned", C.c_int32), ("medianMs", C.c_float * STEP_VARIANTS)]
+
+
 class DemRenderParams(C.Structure):
     _fields_ = [("imageDIMx", C.c_uint32), ("imageDIMy", C.c_uint32), ("bgColor", C.c_uint32),
                 ("viewRotations", C.c_uint32), ("colorByPressure", C.c_uint32),
@@ -97,6 +104,8 @@ SIGNATURES = [
     ("dem_get_cells", C.c_int, [_P, _P, _P, _P]),
     ("dem_check", C.c_int, [_P, _P]),
     ("dem_kernels_per_step", C.c_int, [_P]),
+    ("dem_set_step_variant", C.c_int, [_P, C.c_int32]),
+    ("dem_get_step_variant", C.c_int, [_P, C.POINTER(DemStepVariant)]),
     ("dem_get_followed", C.c_int, [_P, _P, _U, _P, _P]),
     ("dem_profile_begin", C.c_int, [_P, _U]),
     ("dem_profile_end", C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(_U)]),

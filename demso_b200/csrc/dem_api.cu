@@ -1,6 +1,7 @@
 // C ABI of the DEM step (include/demso_b200.h): argument checking, the
 // per-stage entry points, and the context that runs the fused, graph-captured
 // step on library-owned buffers.
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -335,11 +336,37 @@ struct DemContext {
     void* adjCheck = nullptr;
     size_t adjCheckBytes = 0;
     uint32_t adjSteps = 0, adjEvery = 0, adjWindows = 0;
+    // the step kernel's launch shape (step_variant_shape) and its autotuner
+    // (DEM_CTX_AUTOTUNE): the first kTuneSteps steps run the variants in turn,
+    // each timed by a pair of events, then the one with the smallest median
+    // is kept.  tuned: 1 chosen by the tuner, 0 fixed, -1 still timing.
+    int variant = 0;
+    int tuned = 0;
+    uint32_t tuneStep = 0;
+    cudaGraphExec_t tuneGraph[kStepVariants][2] = {};
+    cudaEvent_t* tuneEv = nullptr;
+    float tuneMs[kStepVariants] = {};
 };
 
 namespace {
 
+// rounds of the autotuner: every variant once per round, the first round
+// (cold instruction caches, first graph launches) not counted
+constexpr uint32_t kTuneRounds = 6;
+constexpr uint32_t kTuneSteps = kTuneRounds * kStepVariants;
+
+void drop_tune_graphs(DemContext* c) {
+    for (int v = 0; v < kStepVariants; ++v)
+        for (int p = 0; p < 2; ++p) {
+            if (c->tuneGraph[v][p]) cudaGraphExecDestroy(c->tuneGraph[v][p]);
+            c->tuneGraph[v][p] = nullptr;
+        }
+}
+
 void drop_graphs(DemContext* c) {
+    drop_tune_graphs(c);
+    // a tuning interrupted by a change of the step starts again
+    if (c->tuned < 0) c->tuneStep = 0;
     for (int k = 0; k < 2; ++k)
         for (int p = 0; p < 2; ++p) {
             if (c->sortGraph[k][p]) cudaGraphExecDestroy(c->sortGraph[k][p]);
@@ -446,14 +473,16 @@ cudaError_t enqueue_step_kernel(DemContext* c, cudaStream_t st, int* launches) {
                                 c->keys, (c->flags & DEM_CTX_PRESSURE) ? c->pressure : nullptr,
                                 (c->flags & DEM_CTX_ACCEL) ? c->acc : nullptr,
                                 (c->flags & DEM_CTX_ACCEL) ? c->alpha : nullptr, c->errFlag, c->n,
-                                sink_of(c), st, c->nspec ? c->dTable : nullptr, c->spec, ctl);
+                                sink_of(c), st, c->nspec ? c->dTable : nullptr, c->spec, ctl,
+                                c->variant);
     if (launches) ++*launches;
     if (e == cudaSuccess && c->ctlOn)
         e = launch_control_post(ctl, c->dCtl, c->n, c->ctlPartials, c->ctlOut, st, launches);
     return e;
 }
 
-// what: 0/1 = sort phase of that kind, 2 = step kernel.
+// what: 0/1 = sort phase of that kind, 2 = step kernel (of c->variant's
+// shape), 3 = the step kernel into the autotuner's graph of c->variant.
 int build_graph(DemContext* c, int what, int parity) {
     cudaGraph_t g = nullptr;
     const int saved = c->cur;
@@ -470,11 +499,72 @@ int build_graph(DemContext* c, int what, int parity) {
         return cuda_fail(e, "step capture");
     }
     if (e2 != cudaSuccess) return cuda_fail(e2, "end capture");
-    cudaGraphExec_t* slot = what < 2 ? &c->sortGraph[what][parity] : &c->stepGraph[parity];
+    cudaGraphExec_t* slot = what < 2    ? &c->sortGraph[what][parity]
+                            : what == 2 ? &c->stepGraph[parity]
+                                        : &c->tuneGraph[c->variant][parity];
     e = cudaGraphInstantiate(slot, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(e, "graph instantiate");
     if (what == 1) c->launchesPerStep = launches + 1 + (c->ctlOn ? 2 : 0);  // + the step graph
+    return DEM_OK;
+}
+
+void drop_tune_events(DemContext* c) {
+    if (!c->tuneEv) return;
+    for (uint32_t i = 0; i < 2 * kTuneSteps; ++i)
+        if (c->tuneEv[i]) cudaEventDestroy(c->tuneEv[i]);
+    delete[] c->tuneEv;
+    c->tuneEv = nullptr;
+}
+
+// Before a tuning step: the events (and, on the graph path, every variant's
+// step graph) exist.
+int tune_prepare(DemContext* c, bool graphs) {
+    if (!c->tuneEv) {
+        c->tuneEv = new (std::nothrow) cudaEvent_t[2 * kTuneSteps]();
+        if (!c->tuneEv) return fail(DEM_ERR_NO_MEMORY, "host allocation failed");
+        for (uint32_t i = 0; i < 2 * kTuneSteps; ++i)
+            DEM_TRY_CUDA(cudaEventCreate(&c->tuneEv[i]), "tuner event");
+    }
+    if (!graphs) return DEM_OK;
+    const int keep = c->variant;
+    for (int v = 0; v < kStepVariants; ++v)
+        for (int p = 0; p < 2; ++p)
+            if (!c->tuneGraph[v][p]) {
+                c->variant = v;
+                const int rc = build_graph(c, 3, p);
+                c->variant = keep;
+                if (rc) return rc;
+            }
+    return DEM_OK;
+}
+
+// After the last tuning step: the median time of each variant, the fastest
+// kept (the lower index on a tie), its graphs moved into stepGraph.
+int tune_finish(DemContext* c, bool graphs) {
+    DEM_TRY_CUDA(cudaEventSynchronize(c->tuneEv[2 * kTuneSteps - 1]), "tuner sync");
+    int best = 0;
+    for (int v = 0; v < kStepVariants; ++v) {
+        float t[kTuneRounds - 1];
+        for (uint32_t r = 1; r < kTuneRounds; ++r) {
+            const uint32_t s = r * kStepVariants + (uint32_t)v;
+            DEM_TRY_CUDA(cudaEventElapsedTime(&t[r - 1], c->tuneEv[2 * s], c->tuneEv[2 * s + 1]),
+                         "tuner time");
+        }
+        std::sort(t, t + (kTuneRounds - 1));
+        c->tuneMs[v] = t[(kTuneRounds - 1) / 2];
+        if (c->tuneMs[v] < c->tuneMs[best]) best = v;
+    }
+    c->variant = best;
+    c->tuned = 1;
+    if (graphs)
+        for (int p = 0; p < 2; ++p) {
+            if (c->stepGraph[p]) cudaGraphExecDestroy(c->stepGraph[p]);
+            c->stepGraph[p] = c->tuneGraph[best][p];
+            c->tuneGraph[best][p] = nullptr;
+        }
+    drop_tune_graphs(c);
+    drop_tune_events(c);
     return DEM_OK;
 }
 
@@ -585,6 +675,7 @@ extern "C" int dem_batch_specimen(DemContext* c, uint32_t specimen, uint32_t* fi
 }
 
 int init_context(DemContext* c, uint32_t capacity, uint32_t numCells, DemContext** out) {
+    c->tuned = (c->flags & DEM_CTX_AUTOTUNE) ? -1 : 0;
     c->capacity = capacity;
     c->numCells = numCells;
     c->keyBits = log2_u32(c->numCells);
@@ -658,6 +749,7 @@ extern "C" int dem_destroy(DemContext* c) {
     if (!c) return DEM_OK;
     drop_graphs(c);
     drop_profile(c);
+    drop_tune_events(c);
     if (c->capStream) cudaStreamDestroy(c->capStream);
     if (c->bodyStream) cudaStreamDestroy(c->bodyStream);
     cudaFree(c->followRows);
@@ -825,7 +917,24 @@ int step_direct(DemContext* c, uint32_t nsteps, cudaStream_t st) {
         DEM_TRY_CUDA(full ? enqueue_full_sort(c, a, st, nullptr) : enqueue_inc_sort(c, a, st, nullptr),
                      "sort phase");
         if (prof) DEM_TRY_CUDA(cudaEventRecord(ev[1], st), "profile event");
-        DEM_TRY_CUDA(enqueue_step_kernel(c, st, nullptr), "step kernel");
+        if (c->tuned < 0) {
+            int rc = tune_prepare(c, false);
+            if (rc) return rc;
+            const uint32_t k = c->tuneStep;
+            const int keep = c->variant;
+            c->variant = (int)(k % kStepVariants);
+            DEM_TRY_CUDA(cudaEventRecord(c->tuneEv[2 * k], st), "tuner event");
+            cudaError_t e = enqueue_step_kernel(c, st, nullptr);
+            c->variant = keep;
+            DEM_TRY_CUDA(e, "step kernel");
+            DEM_TRY_CUDA(cudaEventRecord(c->tuneEv[2 * k + 1], st), "tuner event");
+            if (++c->tuneStep == kTuneSteps) {
+                rc = tune_finish(c, false);
+                if (rc) return rc;
+            }
+        } else {
+            DEM_TRY_CUDA(enqueue_step_kernel(c, st, nullptr), "step kernel");
+        }
         if (prof) {
             DEM_TRY_CUDA(cudaEventRecord(ev[2], st), "profile event");
             c->evUsed += 3;
@@ -872,7 +981,20 @@ extern "C" int dem_step(DemContext* c, uint32_t nsteps, void* stream) {
         if (prof) DEM_TRY_CUDA(cudaEventRecord(ev[0], st), "profile event");
         DEM_TRY_CUDA(cudaGraphLaunch(c->sortGraph[kind][p], st), "graph launch");
         if (prof) DEM_TRY_CUDA(cudaEventRecord(ev[1], st), "profile event");
-        DEM_TRY_CUDA(cudaGraphLaunch(c->stepGraph[p], st), "graph launch");
+        if (c->tuned < 0) {
+            int rc = tune_prepare(c, true);
+            if (rc) return rc;
+            const uint32_t k = c->tuneStep;
+            DEM_TRY_CUDA(cudaEventRecord(c->tuneEv[2 * k], st), "tuner event");
+            DEM_TRY_CUDA(cudaGraphLaunch(c->tuneGraph[k % kStepVariants][p], st), "graph launch");
+            DEM_TRY_CUDA(cudaEventRecord(c->tuneEv[2 * k + 1], st), "tuner event");
+            if (++c->tuneStep == kTuneSteps) {
+                rc = tune_finish(c, true);
+                if (rc) return rc;
+            }
+        } else {
+            DEM_TRY_CUDA(cudaGraphLaunch(c->stepGraph[p], st), "graph launch");
+        }
         if (prof) {
             DEM_TRY_CUDA(cudaEventRecord(ev[2], st), "profile event");
             c->evUsed += 3;
@@ -881,6 +1003,36 @@ extern "C" int dem_step(DemContext* c, uint32_t nsteps, void* stream) {
         c->cur ^= 1;
         c->haveOrder = true;
     }
+    return DEM_OK;
+}
+
+extern "C" int dem_set_step_variant(DemContext* c, int32_t variant) {
+    if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    if (variant < 0 || variant >= kStepVariants)
+        return fail(DEM_ERR_INVALID_ARG, "step variant %d outside 0..%d", (int)variant,
+                    kStepVariants - 1);
+    drop_tune_graphs(c);
+    drop_tune_events(c);
+    c->tuneStep = 0;
+    c->tuned = 0;
+    if (c->variant != variant) {
+        c->variant = variant;
+        for (int p = 0; p < 2; ++p) {
+            if (c->stepGraph[p]) cudaGraphExecDestroy(c->stepGraph[p]);
+            c->stepGraph[p] = nullptr;
+        }
+    }
+    return DEM_OK;
+}
+
+extern "C" int dem_get_step_variant(DemContext* c, DemStepVariant* out) {
+    if (!c || !out) return fail(DEM_ERR_INVALID_ARG, "context or out is NULL");
+    const StepShape sh = step_variant_shape(c->ctlOn ? 0 : c->variant);
+    out->variant = c->variant;
+    out->threads = (uint32_t)sh.threads;
+    out->blocksPerSm = (uint32_t)sh.blocksPerSm;
+    out->tuned = c->tuned;
+    for (int v = 0; v < DEM_STEP_VARIANTS; ++v) out->medianMs[v] = c->tuned > 0 ? c->tuneMs[v] : 0.0f;
     return DEM_OK;
 }
 

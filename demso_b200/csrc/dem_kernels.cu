@@ -489,8 +489,11 @@ __device__ __forceinline__ void step_particle(const KParams& P, uint32_t i, DynS
                            pressure, acc, alpha, errFlag, sink);
 }
 
-template <bool TYPED, bool ATTRACT, bool CULL, bool CONTROL>
-__global__ void __launch_bounds__(kCollideThreads, 8)
+// THREADS x MINB: the block size and the blocks per SM the registers are
+// capped for (the step variants, chosen by the context's autotuner).
+template <bool TYPED, bool ATTRACT, bool CULL, bool CONTROL, int THREADS = kCollideThreads,
+          int MINB = 1024 / kCollideThreads>
+__global__ void __launch_bounds__(THREADS, MINB)
 step_kernel(KParams P, DynSet in, StatSet inS, const uint32_t* __restrict__ sortedKey,
             const uint2* __restrict__ cellRange, DynSet out, uint32_t* __restrict__ nextHash,
             float* __restrict__ pressure, float2* __restrict__ acc, float* __restrict__ alpha,
@@ -557,8 +560,9 @@ __global__ void control_sum_move_kernel(ControlDev* __restrict__ c,
 // Batched form: particle slot i belongs to specimen spec[i] (slots of a
 // specimen are contiguous and never change specimen), whose parameters --
 // box, grid, cell offset, contact coefficients -- come from a device table.
-template <bool TYPED, bool ATTRACT, bool CULL>
-__global__ void __launch_bounds__(kCollideThreads, 8)
+template <bool TYPED, bool ATTRACT, bool CULL, int THREADS = kCollideThreads,
+          int MINB = 1024 / kCollideThreads>
+__global__ void __launch_bounds__(THREADS, MINB)
 step_kernel_batched(const KParams* __restrict__ table, const uint32_t* __restrict__ spec,
                     DynSet in, StatSet inS, const uint32_t* __restrict__ sortedKey,
                     const uint2* __restrict__ cellRange, DynSet out,
@@ -748,26 +752,36 @@ cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t
                         const uint2* cellRange, DynSet out, uint32_t* nextHash, float* pressure,
                         float2* acc, float* alpha, uint32_t* errFlag, uint32_t n,
                         MoverSinkArgs sink, cudaStream_t st, const KParams* table,
-                        const uint32_t* spec, ControlArgs ctl) {
+                        const uint32_t* spec, ControlArgs ctl, int variant) {
     if (n == 0) return cudaSuccess;
+    if (variant < 0 || variant >= kStepVariants) return cudaErrorInvalidValue;
     const bool typed = inS.type != nullptr && P.nmat > 1;
     const bool attract = has_attraction(P);
-    const unsigned b = blocks_for(n, kCollideThreads);
     const bool cull = table ? true : P.cull != 0u;
-#define DEM_STEP(T, A, C)                                                                      \
+#define DEM_STEP_T(T, A, C, TH, MB)                                                            \
     do {                                                                                       \
+        const unsigned b = blocks_for(n, TH);                                                  \
         if (table)                                                                             \
-            step_kernel_batched<T, A, C><<<b, kCollideThreads, 0, st>>>(                       \
+            step_kernel_batched<T, A, C, TH, MB><<<b, TH, 0, st>>>(                            \
                 table, spec, in, inS, sortedKey, cellRange, out, nextHash, pressure, acc, alpha, \
                 errFlag, n, sink);                                                             \
         else if (ctl.c)                                                                        \
-            step_kernel<T, A, C, true><<<b, kCollideThreads, 0, st>>>(                         \
-                P, in, inS, sortedKey, cellRange, out, nextHash, pressure, acc, alpha, errFlag, \
-                n, sink, ctl);                                                                 \
+            step_kernel<T, A, C, true><<<blocks_for(n, kCollideThreads), kCollideThreads, 0,  \
+                                         st>>>(P, in, inS, sortedKey, cellRange, out, nextHash, \
+                                               pressure, acc, alpha, errFlag, n, sink, ctl);  \
         else                                                                                   \
-            step_kernel<T, A, C, false><<<b, kCollideThreads, 0, st>>>(                        \
+            step_kernel<T, A, C, false, TH, MB><<<b, TH, 0, st>>>(                             \
                 P, in, inS, sortedKey, cellRange, out, nextHash, pressure, acc, alpha, errFlag, \
                 n, sink, ctl);                                                                 \
+    } while (0)
+#define DEM_STEP(T, A, C)                                                                      \
+    do {                                                                                       \
+        switch (variant) {                                                                     \
+            case 1: DEM_STEP_T(T, A, C, 64, 16); break;                                        \
+            case 2: DEM_STEP_T(T, A, C, 256, 4); break;                                        \
+            case 3: DEM_STEP_T(T, A, C, 128, 6); break;                                        \
+            default: DEM_STEP_T(T, A, C, 128, 8); break;                                       \
+        }                                                                                      \
     } while (0)
     if (typed) {
         if (attract) DEM_STEP(true, true, false);
@@ -779,7 +793,17 @@ cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t
         else DEM_STEP(false, false, false);
     }
 #undef DEM_STEP
+#undef DEM_STEP_T
     return cudaGetLastError();
+}
+
+StepShape step_variant_shape(int variant) {
+    switch (variant) {
+        case 1: return StepShape{64, 16};
+        case 2: return StepShape{256, 4};
+        case 3: return StepShape{128, 6};
+        default: return StepShape{128, 8};
+    }
 }
 
 cudaError_t launch_control_post(ControlArgs ctl, ControlDev* c, uint32_t n, float* partials,

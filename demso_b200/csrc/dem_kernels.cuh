@@ -91,7 +91,17 @@ cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t
                         const uint2* cellRange, DynSet out, uint32_t* nextHash, float* pressure,
                         float2* acc, float* alpha, uint32_t* errFlag, uint32_t n,
                         MoverSinkArgs sink, cudaStream_t st, const KParams* table = nullptr,
-                        const uint32_t* spec = nullptr, ControlArgs ctl = ControlArgs{});
+                        const uint32_t* spec = nullptr, ControlArgs ctl = ControlArgs{},
+                        int variant = 0);
+// Launch shapes of the step kernel: threads per block x the blocks per SM its
+// registers are capped for (variant 0: 128 x 8, 1: 64 x 16, 2: 256 x 4,
+// 3: 128 x 6, which allows 80 registers).  All compute the same bits; the
+// control-particle step always runs variant 0's shape.
+constexpr int kStepVariants = 4;
+struct StepShape {
+    int threads, blocksPerSm;
+};
+StepShape step_variant_shape(int variant);
 // After the step kernel: the reaction sums (reduceVecD's blocks, then their
 // sum in block order: out[0..2] = force x, force y, moment) and the control
 // particle's move.  partials: 3 * ceil(n / min(512, n)) floats.

@@ -168,6 +168,8 @@ typedef struct DemContext DemContext;
 #define DEM_CTX_ACCEL 2u      /* also store acc/alpha of the last step (output rows) */
 #define DEM_CTX_DIRECT 4u     /* launch each kernel directly instead of through CUDA graphs
                                  (one host read-back per step; for per-kernel profiling) */
+#define DEM_CTX_AUTOTUNE 8u   /* choose the step kernel's launch shape on the first steps
+                                 (dem_get_step_variant) */
 
 int dem_create(const DemSystem* sys, uint32_t capacity, uint32_t flags, DemContext** out);
 int dem_destroy(DemContext* ctx);
@@ -212,8 +214,28 @@ int dem_get_state(DemContext* ctx, float* pos, float* vel, float* theta, float* 
                   float* radius, float* mass, uint32_t* id, uint32_t* type, uint32_t* loc,
                   float* pressure, float* acc, float* alpha, int host, void* stream);
 
-/* Advances `nsteps` full steps (hash, sort, reorder, collide, integrate). */
+/* Advances `nsteps` full steps (hash, sort, reorder, collide, integrate).
+ * With DEM_CTX_AUTOTUNE the context's first 24 steps run the step kernel's
+ * launch shapes in turn, each timed by CUDA events on `stream`; the step
+ * that completes the 24th waits for `stream` once and keeps the shape with
+ * the smallest median time.  Every shape computes the same bits, so the
+ * trajectory does not depend on the choice. */
 int dem_step(DemContext* ctx, uint32_t nsteps, void* stream);
+
+/* Launch shapes of the step kernel (threads per block x blocks per SM its
+ * registers are capped for): 0 = 128 x 8 (the default), 1 = 64 x 16,
+ * 2 = 256 x 4, 3 = 128 x 6. */
+#define DEM_STEP_VARIANTS 4
+typedef struct DemStepVariant {
+    int32_t variant;       /* the shape in use */
+    uint32_t threads;      /* its threads per block (128 while a control particle is set) */
+    uint32_t blocksPerSm;  /* its register cap as resident blocks per SM */
+    int32_t tuned;         /* 1 chosen by DEM_CTX_AUTOTUNE, 0 fixed, -1 still timing */
+    float medianMs[DEM_STEP_VARIANTS]; /* the tuner's median step-kernel times (0 unless tuned) */
+} DemStepVariant;
+/* Fixes the launch shape (ends any tuning in progress). */
+int dem_set_step_variant(DemContext* ctx, int32_t variant);
+int dem_get_step_variant(DemContext* ctx, DemStepVariant* out);
 
 /* Cell ranges of the last step's reorder, written to caller device buffers
  * of numCells words each in the reference's layout (either may be NULL). */
