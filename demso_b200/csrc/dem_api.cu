@@ -683,9 +683,12 @@ int init_context(DemContext* c, uint32_t capacity, uint32_t numCells, DemContext
 
     const size_t N = capacity, f4 = al256(4 * N), f8 = al256(8 * N),
                  cells8 = al256(8 * (size_t)c->numCells);
+    // the sorted positions and radii are read up to kFilterPad - 1 elements
+    // past the last particle by the step kernel's candidate filter
+    const size_t f4p = al256(4 * (N + kFilterPad)), f8p = al256(8 * (N + kFilterPad));
     size_t total = 0;
-    total += 2 * (2 * f8 + 2 * f4);              // dyn sets
-    total += 2 * (3 * f4 + (c->typed ? f4 : 0));  // static sets
+    total += 2 * (f8p + f8 + 2 * f4);            // dyn sets
+    total += 2 * (f4p + 2 * f4 + (c->typed ? f4 : 0));  // static sets
     total += 3 * f4 + 2 * f4;                    // loc, keys, perm, sorted keys x2
     total += 2 * cells8;                         // cell ranges x2
     total += f4 + f8 + f4;                       // pressure, acc, alpha
@@ -705,11 +708,11 @@ int init_context(DemContext* c, uint32_t capacity, uint32_t numCells, DemContext
     char* p = static_cast<char*>(c->block);
     auto take = [&p](size_t b) { char* q = p; p += b; return q; };
     for (int s = 0; s < 2; ++s) {
-        c->dyn[s].pos = reinterpret_cast<float2*>(take(f8));
+        c->dyn[s].pos = reinterpret_cast<float2*>(take(f8p));
         c->dyn[s].vel = reinterpret_cast<float2*>(take(f8));
         c->dyn[s].theta = reinterpret_cast<float*>(take(f4));
         c->dyn[s].omega = reinterpret_cast<float*>(take(f4));
-        c->stat[s].radius = reinterpret_cast<float*>(take(f4));
+        c->stat[s].radius = reinterpret_cast<float*>(take(f4p));
         c->stat[s].mass = reinterpret_cast<float*>(take(f4));
         c->stat[s].id = reinterpret_cast<uint32_t*>(take(f4));
         c->stat[s].type = c->typed ? reinterpret_cast<uint32_t*>(take(f4)) : nullptr;

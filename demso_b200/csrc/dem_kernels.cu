@@ -215,7 +215,7 @@ __device__ __forceinline__ void collide_one(const KParams& P, uint32_t i, int2 g
 //
 // Each interval is walked twice, in chunks of 32 candidates: a lean filter
 // sets one bit per candidate whose squared distance is within
-// (rA + rB)^2 (1 + 2e-6) -- a superset of the contacts -- and the contact
+// (rA + rB)^2 (1 + 2e-6), up to rounding -- a superset of the contacts -- and the contact
 // law then runs on the set bits in increasing index.  The law's own
 // `dist < rA + rB` test rejects the few non-contacts among them with a +0
 // force, which changes no sum, so every contact is met in the same
@@ -240,7 +240,6 @@ __device__ __forceinline__ bool collide_rows(const KParams& P, uint32_t i, int2 
                                              const uint2* __restrict__ cells, float2& force,
                                              float& moment, float& pr) {
     int y0 = -1, y1 = 1, x0 = -1, x1 = 1;
-    float reach2 = INFINITY;
     if (p.x > P.cullMargin && p.x < P.Lx - P.cullMargin && p.y > P.cullMargin &&
         p.y < P.Ly - P.cullMargin) {
         const float reach = (r + P.rmax) * 1.0001f + P.cullMargin;
@@ -249,8 +248,6 @@ __device__ __forceinline__ bool collide_rows(const KParams& P, uint32_t i, int2 
         if (X0 + P.cellW - p.x > reach) x1 = 0;
         if (p.y - Y0 > reach) y0 = 0;
         if (Y0 + P.cellH - p.y > reach) y1 = 0;
-        const float rr = (r + P.rmax) * 1.0001f;
-        reach2 = rr * rr;
     }
     if (g.x + x0 < 0 || g.x + x1 >= (int)P.gx) return false;
     force = make_float2(0.0f, 0.0f);
@@ -278,32 +275,38 @@ __device__ __forceinline__ bool collide_rows(const KParams& P, uint32_t i, int2 
         const uint32_t b2 = x1 - x0 >= 2 ? (s2 != 0xffffffffu ? s2 : max(max(e1, e0), a))
                                          : 0xffffffffu;
         float2 f0 = make_float2(0.0f, 0.0f), f1 = f0, f2 = f0;
-        // filter: a bit per candidate that may touch (d2 within (r + rj)^2 (1 + 2e-6));
-        // then the contact law on the set bits in index order
+        // filter: a bit per candidate that may touch, then the contact law on
+        // the set bits in index order.  Groups of 4 candidates are read whole
+        // (the arrays are padded by kFilterPad), the bits past the interval
+        // and the particle's own bit are cleared per chunk.  The test
+        // d2 <= cd^2 (1 + 2e-6) uses fused multiply-adds: d2 and the bound
+        // differ from the law's separately rounded values by under 4e-7
+        // relative, so a rejected candidate still has sqrtf(d2) >= rA + rB in
+        // the law's arithmetic (the law itself is unchanged).
 #pragma unroll 1
         for (uint32_t base = a; base < b; base += 32u) {
-            const uint32_t lim = min(b, base + 32u);
+            const uint32_t cnt = min(b - base, 32u);
             uint32_t mask = 0u;
 #pragma unroll 1
-            for (uint32_t j0 = base; j0 < lim; j0 += 4) {
+            for (uint32_t k0 = 0; k0 < cnt; k0 += 4) {
                 float2 q[4];
-                float d2[4];
-#pragma unroll
-                for (int k = 0; k < 4; ++k) q[k] = __ldg(pos + min(j0 + k, lim - 1));
+                float rq[4];
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
-                    const float relx = q[k].x - p.x, rely = q[k].y - p.y;
-                    d2[k] = relx * relx + rely * rely;
+                    q[k] = __ldg(pos + base + k0 + k);
+                    rq[k] = __ldg(radius + base + k0 + k);
                 }
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
-                    const uint32_t j = j0 + k;
-                    if (j < lim && j != i && d2[k] <= reach2) {
-                        const float cd = r + __ldg(radius + j);
-                        if (d2[k] <= cd * cd * 1.000002f) mask |= 1u << (j - base);
-                    }
+                    const float dx = q[k].x - p.x, dy = q[k].y - p.y;
+                    const float d2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
+                    const float cd = r + rq[k];
+                    const float cd2 = __fmul_rn(cd, cd);
+                    if (d2 <= __fmaf_rn(cd2, 2e-6f, cd2)) mask |= 1u << (k0 + k);
                 }
             }
+            if (cnt < 32u) mask &= (1u << cnt) - 1u;
+            if (i - base < 32u) mask &= ~(1u << (i - base));
             while (mask) {
                 const uint32_t j = base + (uint32_t)(__ffs(mask) - 1);
                 mask &= mask - 1u;

@@ -98,6 +98,9 @@ cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t
 // 3: 128 x 6, which allows 80 registers).  All compute the same bits; the
 // control-particle step always runs variant 0's shape.
 constexpr int kStepVariants = 4;
+// Elements of padding after the sorted positions and radii of a context:
+// the step kernel's candidate filter reads whole groups of 4 candidates.
+constexpr uint32_t kFilterPad = 4;
 struct StepShape {
     int threads, blocksPerSm;
 };
