@@ -175,19 +175,43 @@ __global__ void arrivals_scatter_kernel(const uint4* __restrict__ movers,
     }
 }
 
+// One particle's fields, read in one round of independent loads.
+struct ParticleRec {
+    float2 pos, vel;
+    float theta, omega, radius, mass;
+    uint32_t id, type;
+};
+
+__device__ __forceinline__ ParticleRec load_particle(uint32_t src, DynSet from, StatSet fromS) {
+    ParticleRec r;
+    r.pos = from.pos[src];
+    r.vel = from.vel[src];
+    r.theta = from.theta[src];
+    r.omega = from.omega[src];
+    r.radius = fromS.radius[src];
+    r.mass = fromS.mass[src];
+    r.id = fromS.id[src];
+    r.type = fromS.type ? fromS.type[src] : 0u;
+    return r;
+}
+
+__device__ __forceinline__ void store_particle(const ParticleRec& r, uint32_t dst, DynSet to,
+                                               StatSet toS, uint32_t* __restrict__ loc) {
+    to.pos[dst] = r.pos;
+    to.vel[dst] = r.vel;
+    to.theta[dst] = r.theta;
+    to.omega[dst] = r.omega;
+    toS.radius[dst] = r.radius;
+    toS.mass[dst] = r.mass;
+    toS.id[dst] = r.id;
+    loc[r.id] = dst;
+    if (toS.type) toS.type[dst] = r.type;
+}
+
 __device__ __forceinline__ void move_particle(uint32_t src, uint32_t dst, DynSet from,
                                               StatSet fromS, DynSet to, StatSet toS,
                                               uint32_t* __restrict__ loc) {
-    to.pos[dst] = from.pos[src];
-    to.vel[dst] = from.vel[src];
-    to.theta[dst] = from.theta[src];
-    to.omega[dst] = from.omega[src];
-    toS.radius[dst] = fromS.radius[src];
-    toS.mass[dst] = fromS.mass[src];
-    const uint32_t id = fromS.id[src];
-    toS.id[dst] = id;
-    loc[id] = dst;
-    if (toS.type) toS.type[dst] = fromS.type[src];
+    store_particle(load_particle(src, from, fromS), dst, to, toS, loc);
 }
 
 // A mover goes after the arrivals of its new cell with smaller index, and
@@ -216,7 +240,9 @@ __global__ void place_movers_kernel(const uint4* __restrict__ movers,
     }
 }
 
-// A stayer keeps its rank among the stayers of its cell.
+// A stayer keeps its rank among the stayers of its cell.  The particle's
+// fields are read together with its keys, before its destination is known,
+// so that a thread waits on two rounds of loads instead of three.
 __global__ void __launch_bounds__(kThreads)
 place_stayers_kernel(uint32_t n, const uint32_t* __restrict__ keys,
                      const uint32_t* __restrict__ prevSortedKey,
@@ -227,7 +253,9 @@ place_stayers_kernel(uint32_t n, const uint32_t* __restrict__ keys,
     if (i == 0) ctrl[kCtrlMovers] = 0u;  // movers were consumed by the previous kernels
     if (i >= n) return;
     const uint32_t o = prevSortedKey[i];
-    if (keys[i] != o) return;
+    const uint32_t k = keys[i];
+    const ParticleRec rec = load_particle(i, from, fromS);
+    if (k != o) return;
     const uint32_t os = prevCells[o].x;
     const uint32_t sb = stayBase[o];
     uint32_t rank = i - os;
@@ -237,7 +265,7 @@ place_stayers_kernel(uint32_t n, const uint32_t* __restrict__ keys,
     }
     const uint32_t dst = (sb & ~kHasLeavers) + rank;
     newSortedKey[dst] = o;
-    move_particle(i, dst, from, fromS, to, toS, loc);
+    store_particle(rec, dst, to, toS, loc);
 }
 
 // Full path, after the radix sort: cell ranges from the sorted keys, the

@@ -86,6 +86,46 @@ struct PackedCells {
     __device__ __forceinline__ uint2 get(uint32_t h) const { return __ldg(range + h); }
 };
 
+// Packed pairs of IEEE single-precision operations (PTX f32x2, round to
+// nearest even, sm_100): each lane of the result is the same correctly
+// rounded value as the scalar operation.
+__device__ __forceinline__ float2 f32x2_add(float2 a, float2 b) {
+    float2 d;
+    asm("{.reg .b64 ra, rb, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+__device__ __forceinline__ float2 f32x2_sub(float2 a, float2 b) {
+    float2 d;
+    asm("{.reg .b64 ra, rb, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "sub.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+__device__ __forceinline__ float2 f32x2_mul(float2 a, float2 b) {
+    float2 d;
+    asm("{.reg .b64 ra, rb, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mul.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+__device__ __forceinline__ float2 f32x2_fma(float2 a, float2 b, float2 c) {
+    float2 d;
+    asm("{.reg .b64 ra, rb, rc, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+        "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return d;
+}
+
 // Contact test and force of one candidate j (the reference's collideSpheres
 // and, with ATTRACT, attractSpheres) added to the cell subtotal fc.
 template <bool TYPED, bool ATTRACT>
@@ -276,33 +316,37 @@ __device__ __forceinline__ bool collide_rows(const KParams& P, uint32_t i, int2 
                                          : 0xffffffffu;
         float2 f0 = make_float2(0.0f, 0.0f), f1 = f0, f2 = f0;
         // filter: a bit per candidate that may touch, then the contact law on
-        // the set bits in index order.  Groups of 4 candidates are read whole
+        // the set bits in index order.  Groups of 8 candidates are read whole
         // (the arrays are padded by kFilterPad), the bits past the interval
-        // and the particle's own bit are cleared per chunk.  The test
-        // d2 <= cd^2 (1 + 2e-6) uses fused multiply-adds: d2 and the bound
-        // differ from the law's separately rounded values by under 4e-7
-        // relative, so a rejected candidate still has sqrtf(d2) >= rA + rB in
-        // the law's arithmetic (the law itself is unchanged).
+        // and the particle's own bit are cleared per chunk.  Two candidates
+        // share each packed f32x2 operation.  d2 is the law's own
+        // rn(rn(dx^2) + rn(dy^2)); the bound cd^2 (1 + 2e-6) is a fused
+        // multiply-add, within 2e-7 relative of the exact value, so a
+        // rejected candidate still has sqrtf(d2) >= rA + rB in the law's
+        // arithmetic (the law itself is unchanged).
 #pragma unroll 1
         for (uint32_t base = a; base < b; base += 32u) {
             const uint32_t cnt = min(b - base, 32u);
             uint32_t mask = 0u;
 #pragma unroll 1
-            for (uint32_t k0 = 0; k0 < cnt; k0 += 4) {
-                float2 q[4];
-                float rq[4];
+            for (uint32_t k0 = 0; k0 < cnt; k0 += 8) {
+                float2 q[8];
+                float rq[8];
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
+                for (int k = 0; k < 8; ++k) {
                     q[k] = __ldg(pos + base + k0 + k);
                     rq[k] = __ldg(radius + base + k0 + k);
                 }
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const float dx = q[k].x - p.x, dy = q[k].y - p.y;
-                    const float d2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
-                    const float cd = r + rq[k];
-                    const float cd2 = __fmul_rn(cd, cd);
-                    if (d2 <= __fmaf_rn(cd2, 2e-6f, cd2)) mask |= 1u << (k0 + k);
+                for (int k = 0; k < 8; k += 2) {
+                    const float2 da = f32x2_sub(q[k], p), db = f32x2_sub(q[k + 1], p);
+                    const float2 sa = f32x2_mul(da, da), sb = f32x2_mul(db, db);
+                    const float d2a = sa.x + sa.y, d2b = sb.x + sb.y;
+                    const float2 cd = f32x2_add(make_float2(r, r), make_float2(rq[k], rq[k + 1]));
+                    const float2 c2 = f32x2_mul(cd, cd);
+                    const float2 bound = f32x2_fma(c2, make_float2(2e-6f, 2e-6f), c2);
+                    if (d2a <= bound.x) mask |= 1u << (k0 + k);
+                    if (d2b <= bound.y) mask |= 2u << (k0 + k);
                 }
             }
             if (cnt < 32u) mask &= (1u << cnt) - 1u;

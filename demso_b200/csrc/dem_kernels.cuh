@@ -99,8 +99,8 @@ cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t
 // control-particle step always runs variant 0's shape.
 constexpr int kStepVariants = 4;
 // Elements of padding after the sorted positions and radii of a context:
-// the step kernel's candidate filter reads whole groups of 4 candidates.
-constexpr uint32_t kFilterPad = 4;
+// the step kernel's candidate filter reads whole groups of 8 candidates.
+constexpr uint32_t kFilterPad = 8;
 struct StepShape {
     int threads, blocksPerSm;
 };
