@@ -422,14 +422,14 @@ integrate_kernel(KParams P, float2* __restrict__ pos, float2* __restrict__ vel,
 }
 
 // collide_one/rows/staged done: acceleration, integration, next hash, mover
-// record (shared tail of step_kernel).
+// record (shared tail of step_kernel).  `m` and `s.th` were read with the
+// particle's other fields before the collide, so no load waits here.
 template <bool TYPED>
 __device__ __forceinline__ void finish_particle(
-    const KParams& P, uint32_t i, Dyn& s, float2 f, float moment, float pr, float r, uint32_t mat,
-    uint32_t key, DynSet in, StatSet inS, const uint2* __restrict__ cellRange, DynSet out,
+    const KParams& P, uint32_t i, Dyn& s, float2 f, float moment, float pr, float r, float m,
+    uint32_t mat, uint32_t key, const uint2* __restrict__ cellRange, DynSet out,
     uint32_t* __restrict__ nextHash, float* __restrict__ pressure, float2* __restrict__ acc,
     float* __restrict__ alpha, uint32_t* __restrict__ errFlag, MoverSinkArgs sink) {
-    const float m = inS.mass[i];
     // F/m and M/I as the reference divides them.  Without contacts F and M
     // are +0 (sums that start at +0 never become -0), and +0 divided by a
     // positive finite mass or inertia is exactly +0, so the divisions are
@@ -448,7 +448,6 @@ __device__ __forceinline__ void finish_particle(
     }
     if (acc) acc[i] = a;
     if (alpha) alpha[i] = al;
-    s.th = in.theta[i];
     integrate_one(P, s, a, al, r, m, mat, pr);
     out.pos[i] = s.p;
     out.vel[i] = s.v;
@@ -491,7 +490,9 @@ __device__ __forceinline__ void step_particle(const KParams& P, uint32_t i, DynS
     s.p = in.pos[i];
     s.v = in.vel[i];
     s.w = in.omega[i];
+    s.th = in.theta[i];
     const float r = inS.radius[i];
+    const float m = inS.mass[i];
     const uint32_t mat = TYPED ? inS.type[i] : 0u;
     // the sort key of particle i is calcGridPos of this very position, wrapped
     const uint32_t key = sortedKey[i];
@@ -532,7 +533,7 @@ __device__ __forceinline__ void step_particle(const KParams& P, uint32_t i, DynS
         ctl.fy[i] = -fc.y;
         ctl.fm[i] = -mc / r * c.radius;
     }
-    finish_particle<TYPED>(P, i, s, f, moment, pr, r, mat, key, in, inS, cellRange, out, nextHash,
+    finish_particle<TYPED>(P, i, s, f, moment, pr, r, m, mat, key, cellRange, out, nextHash,
                            pressure, acc, alpha, errFlag, sink);
 }
 
