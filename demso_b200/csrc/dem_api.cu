@@ -317,6 +317,9 @@ struct DemContext {
     bool haveOrder = false;  // the last step recorded its movers: incremental sort possible
     float rmax = INFINITY;   // largest radius of the current state (culling bound)
     cudaStream_t capStream = nullptr, bodyStream = nullptr;
+    // capture-time fork of the sort phase: the full path's branch
+    cudaStream_t forkStream = nullptr;
+    cudaEvent_t forkEv = nullptr, joinEv = nullptr;
     // Each step is two graph launches: the sort phase sortGraph[kind][parity]
     // (kind 0 = full radix sort, 1 = incremental sort with the full sort as a
     // device-chosen fallback), then the step kernel stepGraph[parity].
@@ -397,11 +400,17 @@ cudaError_t enqueue_full_sort(DemContext* c, int a, cudaStream_t st, int* launch
                         launches);
 }
 
-cudaError_t enqueue_inc_sort(DemContext* c, int a, cudaStream_t st, int* launches) {
+cudaError_t enqueue_inc_tail(DemContext* c, int a, cudaStream_t st, int* launches) {
     const int b = a ^ 1;
-    return enqueue_incremental(c->inc, c->n, c->keys, c->skey[a], c->cells[a], c->skey[b],
-                               c->cells[b], c->dyn[0], c->stat[a], c->dyn[1], c->stat[b], c->loc,
-                               st, launches);
+    return enqueue_incremental_tail(c->inc, c->n, c->keys, c->skey[a], c->cells[a], c->skey[b],
+                                    c->cells[b], c->dyn[0], c->stat[a], c->dyn[1], c->stat[b],
+                                    c->loc, st, launches);
+}
+
+// The incremental sort launched directly (the host chose it).
+cudaError_t enqueue_inc_sort(DemContext* c, int a, cudaStream_t st, int* launches) {
+    cudaError_t e = enqueue_incremental_head(c->inc, c->cells[a], 0, false, st, launches);
+    return e == cudaSuccess ? enqueue_inc_tail(c, a, st, launches) : e;
 }
 
 // Adds an IF node on `h` at the current capture point of `st` and captures
@@ -436,7 +445,12 @@ cudaError_t add_if(DemContext* c, cudaStream_t st, cudaGraphConditionalHandle h,
 // Sort phase of one step: the state (dyn[0], stat[cur]) is sorted into
 // (dyn[1], stat[cur^1]) with its cell ranges.  kind 0: full radix sort;
 // kind 1: incremental sort, or the full sort when the last step's movers did
-// not fit (chosen on the device by conditional nodes).
+// not fit.  In kind 1 the incremental kernels are plain graph nodes that
+// return at once when the full path is due, and the full path is the body of
+// one conditional node on a branch beside them, forked after the first
+// incremental kernel (which sets its condition): when the node does not run
+// its body, evaluating it overlaps the incremental kernels instead of adding
+// to the step.  The two branches never both do work in one step.
 cudaError_t enqueue_sort_phase(DemContext* c, int kind, cudaStream_t st, int* launches) {
     const int a = c->cur;
     if (kind == 0) return enqueue_full_sort(c, a, st, launches);
@@ -445,22 +459,22 @@ cudaError_t enqueue_sort_phase(DemContext* c, int kind, cudaStream_t st, int* la
     cudaError_t e = cudaStreamGetCaptureInfo(st, &status, nullptr, &g, nullptr, nullptr);
     if (e != cudaSuccess) return e;
     if (status != cudaStreamCaptureStatusActive) return cudaErrorStreamCaptureUnsupported;
-    cudaGraphConditionalHandle hFast, hFull;
-    e = cudaGraphConditionalHandleCreate(&hFast, g, 0, cudaGraphCondAssignDefault);
-    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hFull, g, 0, cudaGraphCondAssignDefault);
-    if (e == cudaSuccess) e = enqueue_choose_path(c->inc, hFast, hFull, st);
-    if (launches) ++*launches;
-    int fastLaunches = 0, fullLaunches = 0;
-    if (e == cudaSuccess)
-        e = add_if(c, st, hFast, [&](cudaStream_t bs) {
-            return enqueue_inc_sort(c, a, bs, &fastLaunches);
-        });
-    if (e == cudaSuccess)
-        e = add_if(c, st, hFull, [&](cudaStream_t bs) {
-            return enqueue_full_sort(c, a, bs, &fullLaunches);
-        });
-    if (launches) *launches += fastLaunches;  // the usual path
-    return e;
+    cudaGraphConditionalHandle hFull;
+    e = cudaGraphConditionalHandleCreate(&hFull, g, 0, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) e = enqueue_incremental_head(c->inc, c->cells[a], hFull, true, st, launches);
+    if (e != cudaSuccess) return e;
+    e = cudaEventRecord(c->forkEv, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->forkStream, c->forkEv, 0);
+    if (e != cudaSuccess) return e;
+    int fullLaunches = 0;
+    e = add_if(c, c->forkStream, hFull, [&](cudaStream_t bs) {
+        return enqueue_full_sort(c, a, bs, &fullLaunches);
+    });
+    cudaError_t ej = cudaEventRecord(c->joinEv, c->forkStream);
+    if (e == cudaSuccess) e = ej;
+    if (e == cudaSuccess) e = enqueue_inc_tail(c, a, st, launches);
+    ej = cudaStreamWaitEvent(st, c->joinEv, 0);  // join the branch even after an error
+    return e == cudaSuccess ? ej : e;
 }
 
 // Collide + integrate + next hash over the sorted set made by the sort phase.
@@ -736,7 +750,14 @@ int init_context(DemContext* c, uint32_t capacity, uint32_t numCells, DemContext
         e = cudaMemset(c->cells[s], 0xff, 8 * (size_t)c->numCells);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->capStream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->bodyStream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->forkStream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->forkEv, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->joinEv, cudaEventDisableTiming);
     if (e != cudaSuccess) {
+        if (c->joinEv) cudaEventDestroy(c->joinEv);
+        if (c->forkEv) cudaEventDestroy(c->forkEv);
+        if (c->forkStream) cudaStreamDestroy(c->forkStream);
+        if (c->bodyStream) cudaStreamDestroy(c->bodyStream);
         if (c->capStream) cudaStreamDestroy(c->capStream);
         cudaFree(c->incScratch);
         cudaFree(c->sortScratch);
@@ -755,6 +776,9 @@ extern "C" int dem_destroy(DemContext* c) {
     drop_tune_events(c);
     if (c->capStream) cudaStreamDestroy(c->capStream);
     if (c->bodyStream) cudaStreamDestroy(c->bodyStream);
+    if (c->forkStream) cudaStreamDestroy(c->forkStream);
+    if (c->forkEv) cudaEventDestroy(c->forkEv);
+    if (c->joinEv) cudaEventDestroy(c->joinEv);
     cudaFree(c->followRows);
     cudaFree(c->adjCheck);
     cudaFree(c->renderOwner);

@@ -82,10 +82,22 @@ __device__ __forceinline__ unsigned long long cell_counts(const uint2* __restric
     return (unsigned long long)cnt | ((unsigned long long)ac << 32);
 }
 
+// Every kernel of the incremental path returns at once when the last step
+// asked for the full path.  The first one reads that request
+// (ctrl[kCtrlNeedFull]), keeps it for the others in ctrl[kCtrlPath] (the full
+// path, which may run beside them, clears the request) and passes it to the
+// graph's conditional node that runs the full path.
 __global__ void __launch_bounds__(kThreads)
 cells_reduce_kernel(const uint2* __restrict__ prevCells, const uint32_t* __restrict__ leavers,
                     const uint32_t* __restrict__ arrCnt, uint32_t numCells, uint32_t items,
-                    unsigned long long* __restrict__ partials) {
+                    unsigned long long* __restrict__ partials, uint32_t* __restrict__ ctrl,
+                    cudaGraphConditionalHandle full, int setFull) {
+    const bool needFull = ctrl[kCtrlNeedFull] != 0u;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctrl[kCtrlPath] = needFull ? 1u : 0u;
+        if (setFull) cudaGraphSetConditional(full, needFull ? 1u : 0u);
+    }
+    if (needFull) return;
     __shared__ unsigned long long warpTot[kThreads / 32];
     const size_t base = (size_t)blockIdx.x * kThreads * items;
     unsigned long long s = 0;
@@ -100,7 +112,9 @@ cells_reduce_kernel(const uint2* __restrict__ prevCells, const uint32_t* __restr
 }
 
 __global__ void __launch_bounds__(kTopThreads)
-cells_top_kernel(unsigned long long* __restrict__ partials, uint32_t np) {
+cells_top_kernel(unsigned long long* __restrict__ partials, uint32_t np,
+                 const uint32_t* __restrict__ ctrl) {
+    if (ctrl[kCtrlPath]) return;
     __shared__ unsigned long long warpTot[kTopThreads / 32];
     unsigned long long v[kTopItems];
     unsigned long long s = 0;
@@ -128,7 +142,8 @@ cells_apply_kernel(const uint2* __restrict__ prevCells, uint32_t* __restrict__ l
                    uint32_t numCells, uint32_t items,
                    const unsigned long long* __restrict__ partials,
                    uint2* __restrict__ newCells, uint32_t* __restrict__ stayBase,
-                   uint2* __restrict__ arrInfo) {
+                   uint2* __restrict__ arrInfo, const uint32_t* __restrict__ ctrl) {
+    if (ctrl[kCtrlPath]) return;
     __shared__ unsigned long long warpTot[kThreads / 32];
     const size_t base = (size_t)blockIdx.x * kThreads * items;
     unsigned long long carry = partials[blockIdx.x];
@@ -167,6 +182,7 @@ __global__ void arrivals_scatter_kernel(const uint4* __restrict__ movers,
                                         const uint32_t* __restrict__ ctrl, uint32_t cap,
                                         const uint2* __restrict__ arrInfo,
                                         uint32_t* __restrict__ arrSlots) {
+    if (ctrl[kCtrlPath]) return;
     const uint32_t count = min(ctrl[kCtrlMovers], cap);
     for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < count;
          m += gridDim.x * blockDim.x) {
@@ -224,6 +240,7 @@ __global__ void place_movers_kernel(const uint4* __restrict__ movers,
                                     uint32_t* __restrict__ newSortedKey, DynSet from,
                                     StatSet fromS, DynSet to, StatSet toS,
                                     uint32_t* __restrict__ loc) {
+    if (ctrl[kCtrlPath]) return;
     const uint32_t count = min(ctrl[kCtrlMovers], cap);
     for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < count;
          m += gridDim.x * blockDim.x) {
@@ -249,6 +266,7 @@ place_stayers_kernel(uint32_t n, const uint32_t* __restrict__ keys,
                      const uint2* __restrict__ prevCells, const uint32_t* __restrict__ stayBase,
                      uint32_t* __restrict__ newSortedKey, DynSet from, StatSet fromS, DynSet to,
                      StatSet toS, uint32_t* __restrict__ loc, uint32_t* __restrict__ ctrl) {
+    if (ctrl[kCtrlPath]) return;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) ctrl[kCtrlMovers] = 0u;  // movers were consumed by the previous kernels
     if (i >= n) return;
@@ -290,14 +308,6 @@ full_reorder_kernel(uint32_t n, const uint32_t* __restrict__ hash,
     move_particle(index[i], i, from, fromS, to, toS, loc);
 }
 
-__global__ void choose_path_kernel(const uint32_t* __restrict__ ctrl,
-                                   cudaGraphConditionalHandle fast,
-                                   cudaGraphConditionalHandle full) {
-    const bool needFull = ctrl[kCtrlNeedFull] != 0u;
-    cudaGraphSetConditional(fast, needFull ? 0u : 1u);
-    cudaGraphSetConditional(full, needFull ? 1u : 0u);
-}
-
 }  // namespace
 
 size_t incsort_bytes(uint32_t n, uint32_t numCells, uint32_t* moverCapOut) {
@@ -328,21 +338,32 @@ IncSort carve_incsort(void* base, uint32_t n, uint32_t numCells) {
     return s;
 }
 
-cudaError_t enqueue_incremental(const IncSort& s, uint32_t n, const uint32_t* keys,
-                                const uint32_t* prevSortedKey, const uint2* prevCells,
-                                uint32_t* newSortedKey, uint2* newCells, DynSet from,
-                                StatSet fromS, DynSet to, StatSet toS, uint32_t* loc,
-                                cudaStream_t st, int* launches) {
+cudaError_t enqueue_incremental_head(const IncSort& s, const uint2* prevCells,
+                                     cudaGraphConditionalHandle full, bool setFull,
+                                     cudaStream_t st, int* launches) {
+    const uint32_t C = s.numCells;
+    const size_t nb = cell_blocks(C);
+    if (nb > kMaxScanBlocks) return cudaErrorInvalidValue;
+    cells_reduce_kernel<<<(unsigned)nb, kThreads, 0, st>>>(prevCells, s.leavers, s.arrCnt, C,
+                                                           cell_items(C), s.partials, s.ctrl,
+                                                           full, setFull ? 1 : 0);
+    if (launches) ++*launches;
+    return cudaGetLastError();
+}
+
+cudaError_t enqueue_incremental_tail(const IncSort& s, uint32_t n, const uint32_t* keys,
+                                     const uint32_t* prevSortedKey, const uint2* prevCells,
+                                     uint32_t* newSortedKey, uint2* newCells, DynSet from,
+                                     StatSet fromS, DynSet to, StatSet toS, uint32_t* loc,
+                                     cudaStream_t st, int* launches) {
     const uint32_t C = s.numCells;
     const uint32_t items = cell_items(C);
     const size_t nb = cell_blocks(C);
     if (nb > kMaxScanBlocks) return cudaErrorInvalidValue;
-    cells_reduce_kernel<<<(unsigned)nb, kThreads, 0, st>>>(prevCells, s.leavers, s.arrCnt, C,
-                                                           items, s.partials);
-    cells_top_kernel<<<1, kTopThreads, 0, st>>>(s.partials, (uint32_t)nb);
+    cells_top_kernel<<<1, kTopThreads, 0, st>>>(s.partials, (uint32_t)nb, s.ctrl);
     cells_apply_kernel<<<(unsigned)nb, kThreads, 0, st>>>(prevCells, s.leavers, s.arrCnt, s.arrLo,
                                                           C, items, s.partials, newCells,
-                                                          s.stayBase, s.arrInfo);
+                                                          s.stayBase, s.arrInfo, s.ctrl);
     const unsigned mb = std::min<unsigned>(blocks_for(s.moverCap, kThreads), 296u);
     arrivals_scatter_kernel<<<mb, kThreads, 0, st>>>(s.movers, s.ctrl, s.moverCap, s.arrInfo,
                                                      s.arrSlots);
@@ -354,7 +375,7 @@ cudaError_t enqueue_incremental(const IncSort& s, uint32_t n, const uint32_t* ke
             n, keys, prevSortedKey, prevCells, s.stayBase, newSortedKey, from, fromS, to, toS,
             loc, s.ctrl);
     }
-    if (launches) *launches += 6;
+    if (launches) *launches += 5;
     return cudaGetLastError();
 }
 
@@ -381,12 +402,6 @@ cudaError_t enqueue_full(const IncSort& s, uint32_t n, uint32_t keyBits, uint32_
     if (e == cudaSuccess) e = fill_u32(s.arrLo, 0u, s.numCells, st, launches);
     if (e == cudaSuccess) e = fill_u32(s.ctrl, 0u, 2, st, launches);
     if (e != cudaSuccess) return e;
-    return cudaGetLastError();
-}
-
-cudaError_t enqueue_choose_path(const IncSort& s, cudaGraphConditionalHandle fast,
-                                cudaGraphConditionalHandle full, cudaStream_t st) {
-    choose_path_kernel<<<1, 1, 0, st>>>(s.ctrl, fast, full);
     return cudaGetLastError();
 }
 

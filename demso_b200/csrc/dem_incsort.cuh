@@ -21,8 +21,9 @@
 // reference.  When the mover list overflows, an arrival group or a leaving
 // cell is larger than kMaxGroup, or there is no previous order (first
 // step), the full path runs instead: the onesweep radix sort, cell ranges
-// from the sorted keys, and the gather.  Graph conditional nodes choose the
-// path on the device.
+// from the sorted keys, and the gather.  The incremental kernels run
+// unconditionally and return at once when the full path is due; the full
+// path sits in a graph conditional node that the first of them switches on.
 #pragma once
 
 #include <cstdint>
@@ -35,6 +36,7 @@ namespace dem {
 
 constexpr uint32_t kCtrlNeedFull = 0;        // ctrl[0]: non-zero -> full path next step
 constexpr uint32_t kCtrlMovers = 1;          // ctrl[1]: movers recorded by the step kernel
+constexpr uint32_t kCtrlPath = 2;            // ctrl[2]: this step runs the full path
 constexpr uint32_t kHasLeavers = 0x80000000u;  // flag bit in stayBase
 
 // Buffers of the incremental path (all device memory, owned by the context).
@@ -48,19 +50,25 @@ struct IncSort {
     uint4* movers = nullptr;       // moverCap records (index, new cell, old cell, arrival slot)
     uint32_t* arrSlots = nullptr;  // moverCap
     unsigned long long* partials = nullptr;  // scan partials
-    uint32_t* ctrl = nullptr;      // kCtrlNeedFull, kCtrlMovers
+    uint32_t* ctrl = nullptr;      // kCtrlNeedFull, kCtrlMovers, kCtrlPath
 };
 
 size_t incsort_bytes(uint32_t n, uint32_t numCells, uint32_t* moverCapOut);
 IncSort carve_incsort(void* base, uint32_t n, uint32_t numCells);
 
 // Fast path: new cell ranges, sorted keys, moved state.  prev* describe the
-// order the step kernel just stepped; `keys` are the new keys.
-cudaError_t enqueue_incremental(const IncSort& s, uint32_t n, const uint32_t* keys,
-                                const uint32_t* prevSortedKey, const uint2* prevCells,
-                                uint32_t* newSortedKey, uint2* newCells, DynSet from,
-                                StatSet fromS, DynSet to, StatSet toS, uint32_t* loc,
-                                cudaStream_t st, int* launches);
+// order the step kernel just stepped; `keys` are the new keys.  `head` (the
+// first kernel) reads whether the full path is due, keeps the answer in
+// ctrl[kCtrlPath] for the kernels of `tail`, and with setFull passes it to
+// the graph conditional handle `full`.
+cudaError_t enqueue_incremental_head(const IncSort& s, const uint2* prevCells,
+                                     cudaGraphConditionalHandle full, bool setFull,
+                                     cudaStream_t st, int* launches);
+cudaError_t enqueue_incremental_tail(const IncSort& s, uint32_t n, const uint32_t* keys,
+                                     const uint32_t* prevSortedKey, const uint2* prevCells,
+                                     uint32_t* newSortedKey, uint2* newCells, DynSet from,
+                                     StatSet fromS, DynSet to, StatSet toS, uint32_t* loc,
+                                     cudaStream_t st, int* launches);
 
 // Full path: onesweep sort of `keys`, cell ranges, gather, reset of the
 // incremental counters.  `perm` and `keys` are overwritten.
@@ -68,9 +76,5 @@ cudaError_t enqueue_full(const IncSort& s, uint32_t n, uint32_t keyBits, uint32_
                          uint32_t* perm, const OnesweepScratch& os, uint32_t* errFlag,
                          uint32_t* newSortedKey, uint2* newCells, DynSet from, StatSet fromS,
                          DynSet to, StatSet toS, uint32_t* loc, cudaStream_t st, int* launches);
-
-// Sets the two conditional handles from ctrl[kCtrlNeedFull].
-cudaError_t enqueue_choose_path(const IncSort& s, cudaGraphConditionalHandle fast,
-                                cudaGraphConditionalHandle full, cudaStream_t st);
 
 }  // namespace dem
