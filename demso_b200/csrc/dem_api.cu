@@ -1331,35 +1331,13 @@ int step_recorded(DemContext* c, cudaStream_t st, char* rec) {
     const int p = c->cur, b = c->cur ^ 1;
     const int kind = c->haveOrder ? 1 : 0;
     DEM_TRY_CUDA(cudaGraphLaunch(c->sortGraph[kind][p], st), "graph launch");
-    const uint32_t n = c->n;
-    if (rec) {
-        char* q = rec;
-        auto cp = [&](const void* src, size_t bytes, size_t slot) -> cudaError_t {
-            cudaError_t e = cudaMemcpyAsync(q, src, bytes, cudaMemcpyDeviceToDevice, st);
-            q += slot;
-            return e;
-        };
-        const size_t s8 = al256(8ull * n), s4 = al256(4ull * n);
-        // layout of carve_step: pos, vel, acc, spare, omega, radius, mass, alpha, id, cells
-        DEM_TRY_CUDA(cp(c->dyn[1].pos, 8ull * n, s8), "record");
-        DEM_TRY_CUDA(cp(c->dyn[1].vel, 8ull * n, s8), "record");
-        q += s8 + s8;  // acc (after the step), spare
-        DEM_TRY_CUDA(cp(c->dyn[1].omega, 4ull * n, s4), "record");
-        DEM_TRY_CUDA(cp(c->stat[b].radius, 4ull * n, s4), "record");
-        DEM_TRY_CUDA(cp(c->stat[b].mass, 4ull * n, s4), "record");
-        q += s4;  // alpha (after the step)
-        DEM_TRY_CUDA(cp(c->stat[b].id, 4ull * n, s4), "record");
-        DEM_TRY_CUDA(cp(c->cells[b], 8ull * c->numCells, al256(8ull * c->numCells)), "record");
-    }
     DEM_TRY_CUDA(cudaGraphLaunch(c->stepGraph[p], st), "graph launch");
-    if (rec) {
-        const size_t s8 = al256(8ull * n), s4 = al256(4ull * n);
-        DEM_TRY_CUDA(cudaMemcpyAsync(rec + 2 * s8, c->acc, 8ull * n, cudaMemcpyDeviceToDevice, st),
+    // the step kernel leaves the sorted state it read intact: record it, the
+    // cell ranges and the accelerations in one launch
+    if (rec)
+        DEM_TRY_CUDA(adj_record_step(rec, c->n, c->numCells, c->dyn[1], c->stat[b], c->cells[b],
+                                     c->acc, c->alpha, st),
                      "record");
-        DEM_TRY_CUDA(cudaMemcpyAsync(rec + 4 * s8 + 3 * s4, c->alpha, 4ull * n,
-                                     cudaMemcpyDeviceToDevice, st),
-                     "record");
-    }
     c->cur ^= 1;
     c->haveOrder = true;
     return DEM_OK;

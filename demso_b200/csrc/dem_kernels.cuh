@@ -123,6 +123,12 @@ cudaError_t launch_unpack_cells(const uint2* cellRange, uint32_t numCells, uint3
 
 // Adjoint (dem_adjoint.cu).
 size_t adj_step_bytes(uint32_t n, uint32_t numCells);
+// Writes the record of one forward step at recBase in one launch: the sorted
+// state the step kernel stepped (d, s), its cell ranges and the acceleration
+// and angular acceleration it produced.
+cudaError_t adj_record_step(void* recBase, uint32_t n, uint32_t numCells, DynSet d, StatSet s,
+                            const uint2* cells, const float2* acc, const float* alpha,
+                            cudaStream_t st);
 // table/spec: the batch's specimen table and slot -> specimen map, or null
 // for a single scene (then P).
 cudaError_t adj_backward_step(const KParams& P, const KParams* table, const uint32_t* spec,
