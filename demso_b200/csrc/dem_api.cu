@@ -287,6 +287,7 @@ struct DemContext {
     uint32_t* perm = nullptr;  // radix sort values (full path)
     uint32_t* skey[2] = {};    // sorted keys of the order made when stat[p] was filled
     uint2* cells[2] = {};      // interleaved (cellStart, cellEnd) of that order
+    uint32_t* first[2] = {};   // first particle of every cell of that order (numCells + 4)
     float* pressure = nullptr;
     float2* acc = nullptr;
     float* alpha = nullptr;
@@ -396,15 +397,16 @@ MoverSinkArgs sink_of(DemContext* c) {
 cudaError_t enqueue_full_sort(DemContext* c, int a, cudaStream_t st, int* launches) {
     const int b = a ^ 1;
     return enqueue_full(c->inc, c->n, c->keyBits, c->keys, c->perm, c->ss, c->errFlag, c->skey[b],
-                        c->cells[b], c->dyn[0], c->stat[a], c->dyn[1], c->stat[b], c->loc, st,
+                        c->cells[b], c->first[b], c->dyn[0], c->stat[a], c->dyn[1], c->stat[b],
+                        c->loc, st,
                         launches);
 }
 
 cudaError_t enqueue_inc_tail(DemContext* c, int a, cudaStream_t st, int* launches) {
     const int b = a ^ 1;
     return enqueue_incremental_tail(c->inc, c->n, c->keys, c->skey[a], c->cells[a], c->skey[b],
-                                    c->cells[b], c->dyn[0], c->stat[a], c->dyn[1], c->stat[b],
-                                    c->loc, st, launches);
+                                    c->cells[b], c->first[b], c->dyn[0], c->stat[a], c->dyn[1],
+                                    c->stat[b], c->loc, st, launches);
 }
 
 // The incremental sort launched directly (the host chose it).
@@ -483,7 +485,8 @@ cudaError_t enqueue_step_kernel(DemContext* c, cudaStream_t st, int* launches) {
     ControlArgs ctl{};
     if (c->ctlOn) ctl = ControlArgs{c->dCtl, c->ctlVec, c->ctlVec + c->capacity,
                                     c->ctlVec + 2ull * c->capacity};
-    cudaError_t e = launch_step(c->P, c->dyn[1], c->stat[b], c->skey[b], c->cells[b], c->dyn[0],
+    cudaError_t e = launch_step(c->P, c->dyn[1], c->stat[b], c->skey[b], c->cells[b],
+                                c->first[b], c->dyn[0],
                                 c->keys, (c->flags & DEM_CTX_PRESSURE) ? c->pressure : nullptr,
                                 (c->flags & DEM_CTX_ACCEL) ? c->acc : nullptr,
                                 (c->flags & DEM_CTX_ACCEL) ? c->alpha : nullptr, c->errFlag, c->n,
@@ -696,7 +699,8 @@ int init_context(DemContext* c, uint32_t capacity, uint32_t numCells, DemContext
     cudaGetDevice(&c->device);
 
     const size_t N = capacity, f4 = al256(4 * N), f8 = al256(8 * N),
-                 cells8 = al256(8 * (size_t)c->numCells);
+                 cells8 = al256(8 * (size_t)c->numCells),
+                 first4 = al256(4 * ((size_t)c->numCells + 4));
     // the sorted positions and radii are read up to kFilterPad - 1 elements
     // past the last particle by the step kernel's candidate filter
     const size_t f4p = al256(4 * (N + kFilterPad)), f8p = al256(8 * (N + kFilterPad));
@@ -704,7 +708,7 @@ int init_context(DemContext* c, uint32_t capacity, uint32_t numCells, DemContext
     total += 2 * (f8p + f8 + 2 * f4);            // dyn sets
     total += 2 * (f4p + 2 * f4 + (c->typed ? f4 : 0));  // static sets
     total += 3 * f4 + 2 * f4;                    // loc, keys, perm, sorted keys x2
-    total += 2 * cells8;                         // cell ranges x2
+    total += 2 * cells8 + 2 * first4;            // cell ranges and first particles x2
     total += f4 + f8 + f4;                       // pressure, acc, alpha
     total += 256;                                // error flag
     const size_t sortBytes = onesweep_scratch_bytes(capacity, c->keyBits);
@@ -737,6 +741,7 @@ int init_context(DemContext* c, uint32_t capacity, uint32_t numCells, DemContext
     for (int s = 0; s < 2; ++s) {
         c->skey[s] = reinterpret_cast<uint32_t*>(take(f4));
         c->cells[s] = reinterpret_cast<uint2*>(take(cells8));
+        c->first[s] = reinterpret_cast<uint32_t*>(take(first4));
     }
     c->pressure = reinterpret_cast<float*>(take(f4));
     c->acc = reinterpret_cast<float2*>(take(f8));

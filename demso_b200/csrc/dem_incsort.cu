@@ -141,8 +141,9 @@ cells_apply_kernel(const uint2* __restrict__ prevCells, uint32_t* __restrict__ l
                    uint32_t* __restrict__ arrCnt, uint32_t* __restrict__ arrLo,
                    uint32_t numCells, uint32_t items,
                    const unsigned long long* __restrict__ partials,
-                   uint2* __restrict__ newCells, uint32_t* __restrict__ stayBase,
-                   uint2* __restrict__ arrInfo, const uint32_t* __restrict__ ctrl) {
+                   uint2* __restrict__ newCells, uint32_t* __restrict__ newFirst,
+                   uint32_t* __restrict__ stayBase, uint2* __restrict__ arrInfo,
+                   const uint32_t* __restrict__ ctrl) {
     if (ctrl[kCtrlPath]) return;
     __shared__ unsigned long long warpTot[kThreads / 32];
     const size_t base = (size_t)blockIdx.x * kThreads * items;
@@ -167,6 +168,8 @@ cells_apply_kernel(const uint2* __restrict__ prevCells, uint32_t* __restrict__ l
         if (valid) {
             const uint32_t start = (uint32_t)run, abase = (uint32_t)(run >> 32);
             newCells[c] = cnt ? make_uint2(start, start + cnt) : make_uint2(kEmptyCell, kEmptyCell);
+            newFirst[c] = start;
+            if (c == numCells - 1) newFirst[numCells] = start + cnt;
             stayBase[c] = (start + lo) | (lv ? kHasLeavers : 0u);
             if (ac) arrInfo[c] = make_uint2(abase, ac);
             if (lv) leavers[c] = 0u;
@@ -286,6 +289,22 @@ place_stayers_kernel(uint32_t n, const uint32_t* __restrict__ keys,
     store_particle(rec, dst, to, toS, loc);
 }
 
+// First particle of every cell c <= numCells (for an empty cell, that of the
+// next non-empty one): the lower bound of c in the sorted keys.
+__global__ void cell_first_kernel(const uint32_t* __restrict__ sortedKey, uint32_t n,
+                                  uint32_t numCells, uint32_t* __restrict__ first) {
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c <= numCells;
+         c += gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = n;
+        while (lo < hi) {
+            const uint32_t mid = lo + (hi - lo) / 2;
+            if (sortedKey[mid] < c) lo = mid + 1;
+            else hi = mid;
+        }
+        first[c] = lo;
+    }
+}
+
 // Full path, after the radix sort: cell ranges from the sorted keys, the
 // gather by the sorted indices, and the sorted keys kept for the next step.
 __global__ void __launch_bounds__(kThreads)
@@ -353,9 +372,9 @@ cudaError_t enqueue_incremental_head(const IncSort& s, const uint2* prevCells,
 
 cudaError_t enqueue_incremental_tail(const IncSort& s, uint32_t n, const uint32_t* keys,
                                      const uint32_t* prevSortedKey, const uint2* prevCells,
-                                     uint32_t* newSortedKey, uint2* newCells, DynSet from,
-                                     StatSet fromS, DynSet to, StatSet toS, uint32_t* loc,
-                                     cudaStream_t st, int* launches) {
+                                     uint32_t* newSortedKey, uint2* newCells, uint32_t* newFirst,
+                                     DynSet from, StatSet fromS, DynSet to, StatSet toS,
+                                     uint32_t* loc, cudaStream_t st, int* launches) {
     const uint32_t C = s.numCells;
     const uint32_t items = cell_items(C);
     const size_t nb = cell_blocks(C);
@@ -363,7 +382,8 @@ cudaError_t enqueue_incremental_tail(const IncSort& s, uint32_t n, const uint32_
     cells_top_kernel<<<1, kTopThreads, 0, st>>>(s.partials, (uint32_t)nb, s.ctrl);
     cells_apply_kernel<<<(unsigned)nb, kThreads, 0, st>>>(prevCells, s.leavers, s.arrCnt, s.arrLo,
                                                           C, items, s.partials, newCells,
-                                                          s.stayBase, s.arrInfo, s.ctrl);
+                                                          newFirst, s.stayBase, s.arrInfo,
+                                                          s.ctrl);
     const unsigned mb = std::min<unsigned>(blocks_for(s.moverCap, kThreads), 296u);
     arrivals_scatter_kernel<<<mb, kThreads, 0, st>>>(s.movers, s.ctrl, s.moverCap, s.arrInfo,
                                                      s.arrSlots);
@@ -381,8 +401,9 @@ cudaError_t enqueue_incremental_tail(const IncSort& s, uint32_t n, const uint32_
 
 cudaError_t enqueue_full(const IncSort& s, uint32_t n, uint32_t keyBits, uint32_t* keys,
                          uint32_t* perm, const OnesweepScratch& os, uint32_t* errFlag,
-                         uint32_t* newSortedKey, uint2* newCells, DynSet from, StatSet fromS,
-                         DynSet to, StatSet toS, uint32_t* loc, cudaStream_t st, int* launches) {
+                         uint32_t* newSortedKey, uint2* newCells, uint32_t* newFirst,
+                         DynSet from, StatSet fromS, DynSet to, StatSet toS, uint32_t* loc,
+                         cudaStream_t st, int* launches) {
     uint32_t *ko, *vo;
     cudaError_t e = onesweep_sort_pairs(keys, perm, n, keyBits, true, os, errFlag, st, &ko, &vo,
                                         launches);
@@ -395,6 +416,9 @@ cudaError_t enqueue_full(const IncSort& s, uint32_t n, uint32_t keyBits, uint32_
             n, ko, vo, newCells, newSortedKey, from, fromS, to, toS, loc);
         if (launches) ++*launches;
     }
+    cell_first_kernel<<<std::min<unsigned>(blocks_for((size_t)s.numCells + 1, kThreads), 148u * 8u),
+                        kThreads, 0, st>>>(newSortedKey, n, s.numCells, newFirst);
+    if (launches) ++*launches;
     // the incremental counters restart from zero: the step kernel of this
     // step records the movers of the next one
     e = fill_u32(s.leavers, 0u, s.numCells, st, launches);

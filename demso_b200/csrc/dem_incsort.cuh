@@ -66,15 +66,16 @@ cudaError_t enqueue_incremental_head(const IncSort& s, const uint2* prevCells,
                                      cudaStream_t st, int* launches);
 cudaError_t enqueue_incremental_tail(const IncSort& s, uint32_t n, const uint32_t* keys,
                                      const uint32_t* prevSortedKey, const uint2* prevCells,
-                                     uint32_t* newSortedKey, uint2* newCells, DynSet from,
-                                     StatSet fromS, DynSet to, StatSet toS, uint32_t* loc,
-                                     cudaStream_t st, int* launches);
+                                     uint32_t* newSortedKey, uint2* newCells, uint32_t* newFirst,
+                                     DynSet from, StatSet fromS, DynSet to, StatSet toS,
+                                     uint32_t* loc, cudaStream_t st, int* launches);
 
 // Full path: onesweep sort of `keys`, cell ranges, gather, reset of the
 // incremental counters.  `perm` and `keys` are overwritten.
 cudaError_t enqueue_full(const IncSort& s, uint32_t n, uint32_t keyBits, uint32_t* keys,
                          uint32_t* perm, const OnesweepScratch& os, uint32_t* errFlag,
-                         uint32_t* newSortedKey, uint2* newCells, DynSet from, StatSet fromS,
-                         DynSet to, StatSet toS, uint32_t* loc, cudaStream_t st, int* launches);
+                         uint32_t* newSortedKey, uint2* newCells, uint32_t* newFirst,
+                         DynSet from, StatSet fromS, DynSet to, StatSet toS, uint32_t* loc,
+                         cudaStream_t st, int* launches);
 
 }  // namespace dem

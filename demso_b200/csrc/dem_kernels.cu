@@ -277,8 +277,8 @@ __device__ __forceinline__ bool collide_rows(const KParams& P, uint32_t i, int2 
                                              const float* __restrict__ omega,
                                              const float* __restrict__ radius,
                                              const uint32_t* __restrict__ type,
-                                             const uint2* __restrict__ cells, float2& force,
-                                             float& moment, float& pr) {
+                                             const uint32_t* __restrict__ cellFirst,
+                                             float2& force, float& moment, float& pr) {
     int y0 = -1, y1 = 1, x0 = -1, x1 = 1;
     if (p.x > P.cullMargin && p.x < P.Lx - P.cullMargin && p.y > P.cullMargin &&
         p.y < P.Ly - P.cullMargin) {
@@ -297,23 +297,17 @@ __device__ __forceinline__ bool collide_rows(const KParams& P, uint32_t i, int2 
 #pragma unroll 1
     for (int dy = y0; dy <= y1; ++dy) {
         const uint32_t row = P.cellOff + (uint32_t)((g.y + dy) & (int)(P.gy - 1u)) * P.gx;
-        // the visited cells of this row: [first, last] of x0..x1; boundaries
-        // b1/b2 = first index of the 2nd/3rd visited cell (a contact at index
-        // j belongs to visited cell (j >= b1) + (j >= b2))
-        const uint2 c0 = __ldg(cells + row + (uint32_t)(g.x + x0));
-        const uint2 c1 = x1 - x0 >= 1 ? __ldg(cells + row + (uint32_t)(g.x + x0 + 1)) : c0;
-        const uint2 c2 = x1 - x0 >= 2 ? __ldg(cells + row + (uint32_t)(g.x + x1)) : c1;
-        const uint32_t e0 = c0.x < c0.y ? c0.y : 0u;
-        const uint32_t s1 = c1.x < c1.y ? c1.x : 0xffffffffu;
-        const uint32_t e1 = c1.x < c1.y ? c1.y : 0u;
-        const uint32_t s2 = c2.x < c2.y ? c2.x : 0xffffffffu;
-        uint32_t a = c0.x < c0.y ? c0.x : (s1 != 0xffffffffu ? s1 : s2);
-        uint32_t b = x1 - x0 >= 2 ? (c2.x < c2.y ? c2.y : (x1 - x0 >= 1 ? max(e1, e0) : e0))
-                                  : (x1 - x0 >= 1 ? max(e1, e0) : e0);
-        if (a == 0xffffffffu) a = b = 0u;  // every visited cell is empty
-        const uint32_t b1 = x1 - x0 >= 1 ? (s1 != 0xffffffffu ? s1 : (e0 ? e0 : a)) : 0xffffffffu;
-        const uint32_t b2 = x1 - x0 >= 2 ? (s2 != 0xffffffffu ? s2 : max(max(e1, e0), a))
-                                         : 0xffffffffu;
+        // the visited cells of this row are first = x0 .. x1; visited cell k
+        // holds the particles
+        // [start[first + k], start[first + k + 1]); a contact at index j
+        // belongs to visited cell (j >= b1) + (j >= b2)
+        const uint32_t* __restrict__ sc = cellFirst + (row + (uint32_t)(g.x + x0));
+        const uint32_t o0 = __ldg(sc), o1 = __ldg(sc + 1), o2 = __ldg(sc + 2), o3 = __ldg(sc + 3);
+        const int span = x1 - x0;  // visited cells - 1
+        const uint32_t a = o0;
+        const uint32_t b = span == 0 ? o1 : (span == 1 ? o2 : o3);
+        const uint32_t b1 = span >= 1 ? o1 : 0xffffffffu;
+        const uint32_t b2 = span >= 2 ? o2 : 0xffffffffu;
         float2 f0 = make_float2(0.0f, 0.0f), f1 = f0, f2 = f0;
         // filter: a bit per candidate that may touch, then the contact law on
         // the set bits in index order.  Groups of 8 candidates are read whole
@@ -332,10 +326,12 @@ __device__ __forceinline__ bool collide_rows(const KParams& P, uint32_t i, int2 
             for (uint32_t k0 = 0; k0 < cnt; k0 += 8) {
                 float2 q[8];
                 float rq[8];
+                const float2* __restrict__ pq = pos + (base + k0);
+                const float* __restrict__ pr8 = radius + (base + k0);
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
-                    q[k] = __ldg(pos + base + k0 + k);
-                    rq[k] = __ldg(radius + base + k0 + k);
+                    q[k] = __ldg(pq + k);
+                    rq[k] = __ldg(pr8 + k);
                 }
 #pragma unroll
                 for (int k = 0; k < 8; k += 2) {
@@ -479,7 +475,8 @@ template <bool TYPED, bool ATTRACT, bool CULL, bool CONTROL = false>
 __device__ __forceinline__ void step_particle(const KParams& P, uint32_t i, DynSet in,
                                               StatSet inS,
                                               const uint32_t* __restrict__ sortedKey,
-                                              const uint2* __restrict__ cellRange, DynSet out,
+                                              const uint2* __restrict__ cellRange,
+                                              const uint32_t* __restrict__ cellFirst, DynSet out,
                                               uint32_t* __restrict__ nextHash,
                                               float* __restrict__ pressure,
                                               float2* __restrict__ acc,
@@ -502,7 +499,7 @@ __device__ __forceinline__ void step_particle(const KParams& P, uint32_t i, DynS
     float moment, pr;
     if (ATTRACT || !CULL || !P.cull ||
         !collide_rows<TYPED>(P, i, g, s.p, s.v, s.w, r, mat, in.pos, in.vel, in.omega,
-                             inS.radius, inS.type, cellRange, f, moment, pr)) {
+                             inS.radius, inS.type, cellFirst, f, moment, pr)) {
         if (CULL && P.cull)
             collide_one<TYPED, ATTRACT, true>(P, i, g, s.p, s.v, s.w, r, mat, in.pos, in.vel,
                                               in.omega, inS.radius, inS.type,
@@ -543,12 +540,13 @@ template <bool TYPED, bool ATTRACT, bool CULL, bool CONTROL, int THREADS = kColl
           int MINB = 1024 / kCollideThreads>
 __global__ void __launch_bounds__(THREADS, MINB)
 step_kernel(KParams P, DynSet in, StatSet inS, const uint32_t* __restrict__ sortedKey,
-            const uint2* __restrict__ cellRange, DynSet out, uint32_t* __restrict__ nextHash,
+            const uint2* __restrict__ cellRange, const uint32_t* __restrict__ cellFirst, DynSet out,
+            uint32_t* __restrict__ nextHash,
             float* __restrict__ pressure, float2* __restrict__ acc, float* __restrict__ alpha,
             uint32_t* __restrict__ errFlag, uint32_t n, MoverSinkArgs sink, ControlArgs ctl) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    step_particle<TYPED, ATTRACT, CULL, CONTROL>(P, i, in, inS, sortedKey, cellRange, out,
+    step_particle<TYPED, ATTRACT, CULL, CONTROL>(P, i, in, inS, sortedKey, cellRange, cellFirst, out,
                                                  nextHash, pressure, acc, alpha, errFlag, sink,
                                                  ctl);
 }
@@ -613,13 +611,13 @@ template <bool TYPED, bool ATTRACT, bool CULL, int THREADS = kCollideThreads,
 __global__ void __launch_bounds__(THREADS, MINB)
 step_kernel_batched(const KParams* __restrict__ table, const uint32_t* __restrict__ spec,
                     DynSet in, StatSet inS, const uint32_t* __restrict__ sortedKey,
-                    const uint2* __restrict__ cellRange, DynSet out,
-                    uint32_t* __restrict__ nextHash, float* __restrict__ pressure,
+                    const uint2* __restrict__ cellRange, const uint32_t* __restrict__ cellFirst,
+                    DynSet out, uint32_t* __restrict__ nextHash, float* __restrict__ pressure,
                     float2* __restrict__ acc, float* __restrict__ alpha,
                     uint32_t* __restrict__ errFlag, uint32_t n, MoverSinkArgs sink) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    step_particle<TYPED, ATTRACT, CULL>(table[spec[i]], i, in, inS, sortedKey, cellRange, out,
+    step_particle<TYPED, ATTRACT, CULL>(table[spec[i]], i, in, inS, sortedKey, cellRange, cellFirst, out,
                                         nextHash, pressure, acc, alpha, errFlag, sink);
 }
 
@@ -797,7 +795,7 @@ cudaError_t launch_integrate(const KParams& P, float2* pos, float2* vel, const f
 }
 
 cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t* sortedKey,
-                        const uint2* cellRange, DynSet out, uint32_t* nextHash, float* pressure,
+                        const uint2* cellRange, const uint32_t* cellFirst, DynSet out, uint32_t* nextHash, float* pressure,
                         float2* acc, float* alpha, uint32_t* errFlag, uint32_t n,
                         MoverSinkArgs sink, cudaStream_t st, const KParams* table,
                         const uint32_t* spec, ControlArgs ctl, int variant) {
@@ -811,15 +809,15 @@ cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t
         const unsigned b = blocks_for(n, TH);                                                  \
         if (table)                                                                             \
             step_kernel_batched<T, A, C, TH, MB><<<b, TH, 0, st>>>(                            \
-                table, spec, in, inS, sortedKey, cellRange, out, nextHash, pressure, acc, alpha, \
+                table, spec, in, inS, sortedKey, cellRange, cellFirst, out, nextHash, pressure, acc, alpha, \
                 errFlag, n, sink);                                                             \
         else if (ctl.c)                                                                        \
             step_kernel<T, A, C, true><<<blocks_for(n, kCollideThreads), kCollideThreads, 0,  \
-                                         st>>>(P, in, inS, sortedKey, cellRange, out, nextHash, \
+                                         st>>>(P, in, inS, sortedKey, cellRange, cellFirst, out, nextHash, \
                                                pressure, acc, alpha, errFlag, n, sink, ctl);  \
         else                                                                                   \
             step_kernel<T, A, C, false, TH, MB><<<b, TH, 0, st>>>(                             \
-                P, in, inS, sortedKey, cellRange, out, nextHash, pressure, acc, alpha, errFlag, \
+                P, in, inS, sortedKey, cellRange, cellFirst, out, nextHash, pressure, acc, alpha, errFlag, \
                 n, sink, ctl);                                                                 \
     } while (0)
 #define DEM_STEP(T, A, C)                                                                      \

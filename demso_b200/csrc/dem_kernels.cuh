@@ -87,8 +87,12 @@ struct ControlArgs {
     float* fy;
     float* fm;
 };
+// cellRange: (start, end) of every cell; cellFirst: numCells + 4 words, the
+// first particle of every cell (for an empty cell, that of the next
+// non-empty one) and n at [numCells].
 cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t* sortedKey,
-                        const uint2* cellRange, DynSet out, uint32_t* nextHash, float* pressure,
+                        const uint2* cellRange, const uint32_t* cellFirst, DynSet out,
+                        uint32_t* nextHash, float* pressure,
                         float2* acc, float* alpha, uint32_t* errFlag, uint32_t n,
                         MoverSinkArgs sink, cudaStream_t st, const KParams* table = nullptr,
                         const uint32_t* spec = nullptr, ControlArgs ctl = ControlArgs{},
