@@ -333,6 +333,7 @@ __device__ __forceinline__ bool collide_rows(const KParams& P, uint32_t i, int2 
                     q[k] = __ldg(pq + k);
                     rq[k] = __ldg(pr8 + k);
                 }
+                uint32_t m8 = 0u;
 #pragma unroll
                 for (int k = 0; k < 8; k += 2) {
                     const float2 da = f32x2_sub(q[k], p), db = f32x2_sub(q[k + 1], p);
@@ -341,9 +342,10 @@ __device__ __forceinline__ bool collide_rows(const KParams& P, uint32_t i, int2 
                     const float2 cd = f32x2_add(make_float2(r, r), make_float2(rq[k], rq[k + 1]));
                     const float2 c2 = f32x2_mul(cd, cd);
                     const float2 bound = f32x2_fma(c2, make_float2(2e-6f, 2e-6f), c2);
-                    if (d2a <= bound.x) mask |= 1u << (k0 + k);
-                    if (d2b <= bound.y) mask |= 2u << (k0 + k);
+                    if (d2a <= bound.x) m8 |= 1u << k;
+                    if (d2b <= bound.y) m8 |= 2u << k;
                 }
+                mask |= m8 << k0;
             }
             if (cnt < 32u) mask &= (1u << cnt) - 1u;
             if (i - base < 32u) mask &= ~(1u << (i - base));
