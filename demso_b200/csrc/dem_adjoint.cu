@@ -290,18 +290,20 @@ StepRec carve_step(void* base, uint32_t n, uint32_t numCells) {
 
 namespace {
 __global__ void __launch_bounds__(kAdjThreads)
-adj_record_kernel(StepRec r, DynSet d, StatSet s, const uint2* __restrict__ cells,
+adj_record_kernel(StepRec r, DynSet d, StatSet s, const uint32_t* __restrict__ src,
+                  const uint2* __restrict__ cells,
                   const float2* __restrict__ acc, const float* __restrict__ alpha, uint32_t n,
                   uint32_t numCells) {
     const uint32_t m = n > numCells ? n : numCells;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
         if (i < n) {
+            const uint32_t si = src[i];
             r.pos[i] = d.pos[i];
-            r.vel[i] = d.vel[i];
-            r.omega[i] = d.omega[i];
+            r.vel[i] = d.vel[si];
+            r.omega[i] = d.omega[si];
             r.radius[i] = s.radius[i];
-            r.mass[i] = s.mass[i];
-            r.id[i] = s.id[i];
+            r.mass[i] = s.mass[si];
+            r.id[i] = s.id[si];
             r.acc[i] = acc[i];
             r.alpha[i] = alpha[i];
         }
@@ -311,12 +313,12 @@ adj_record_kernel(StepRec r, DynSet d, StatSet s, const uint2* __restrict__ cell
 }  // namespace
 
 cudaError_t adj_record_step(void* recBase, uint32_t n, uint32_t numCells, DynSet d, StatSet s,
-                            const uint2* cells, const float2* acc, const float* alpha,
-                            cudaStream_t st) {
+                            const uint32_t* src, const uint2* cells, const float2* acc,
+                            const float* alpha, cudaStream_t st) {
     const uint32_t m = n > numCells ? n : numCells;
     const unsigned b = std::min<unsigned>(blocks_for(m, kAdjThreads), 148u * 16u);
-    adj_record_kernel<<<b, kAdjThreads, 0, st>>>(carve_step(recBase, n, numCells), d, s, cells,
-                                                 acc, alpha, n, numCells);
+    adj_record_kernel<<<b, kAdjThreads, 0, st>>>(carve_step(recBase, n, numCells), d, s, src,
+                                                 cells, acc, alpha, n, numCells);
     return cudaGetLastError();
 }
 

@@ -277,11 +277,16 @@ struct DemContext {
     uint32_t capacity = 0, n = 0, flags = 0, numCells = 0, keyBits = 0;
     int device = 0;
     bool typed = false;
-    // dynamic fields: dyn[0] holds the integrated state, dyn[1] the sorted copy
+    // The current state (order of the last sort): positions in dyn[0].pos,
+    // velocities, angles and spins in dyn[cur], the static fields in
+    // stat[cur].  A step's sort moves positions into dyn[1].pos and radii
+    // into stat[cur ^ 1] and records src; its step kernel gathers the other
+    // fields through src and writes the new state into dyn[0].pos,
+    // dyn[cur ^ 1] and stat[cur ^ 1].
     DynSet dyn[2];
-    // static fields ping-pong between the two sets on every sort
     StatSet stat[2];
-    int cur = 0;               // static set holding the current state
+    int cur = 0;               // parity of the sets holding the current state
+    uint32_t* src = nullptr;   // per sorted slot: the particle's slot in the previous order
     uint32_t* loc = nullptr;   // indexed by id
     uint32_t* keys = nullptr;  // cell of each particle of the current state
     uint32_t* perm = nullptr;  // radix sort values (full path)
@@ -394,19 +399,23 @@ MoverSinkArgs sink_of(DemContext* c) {
 }
 
 // Full sort of the current state (parity a) into the other static set.
+// What the sort phase of parity a moves: positions and radii into the
+// sorted order, with the previous slot of every sorted slot.
+SortMove sort_move(DemContext* c, int a) {
+    return SortMove{c->dyn[0].pos, c->stat[a].radius, c->dyn[1].pos, c->stat[a ^ 1].radius,
+                    c->src};
+}
+
 cudaError_t enqueue_full_sort(DemContext* c, int a, cudaStream_t st, int* launches) {
     const int b = a ^ 1;
     return enqueue_full(c->inc, c->n, c->keyBits, c->keys, c->perm, c->ss, c->errFlag, c->skey[b],
-                        c->cells[b], c->first[b], c->dyn[0], c->stat[a], c->dyn[1], c->stat[b],
-                        c->loc, st,
-                        launches);
+                        c->cells[b], c->first[b], sort_move(c, a), st, launches);
 }
 
 cudaError_t enqueue_inc_tail(DemContext* c, int a, cudaStream_t st, int* launches) {
     const int b = a ^ 1;
     return enqueue_incremental_tail(c->inc, c->n, c->keys, c->skey[a], c->cells[a], c->skey[b],
-                                    c->cells[b], c->first[b], c->dyn[0], c->stat[a], c->dyn[1],
-                                    c->stat[b], c->loc, st, launches);
+                                    c->cells[b], c->first[b], sort_move(c, a), st, launches);
 }
 
 // The incremental sort launched directly (the host chose it).
@@ -480,13 +489,27 @@ cudaError_t enqueue_sort_phase(DemContext* c, int kind, cudaStream_t st, int* la
 }
 
 // Collide + integrate + next hash over the sorted set made by the sort phase.
+// The inputs of the step kernel of parity a: sorted positions and radii, the
+// other fields in the previous order (gathered through src).
+DynSet step_in(DemContext* c, int a) {
+    return DynSet{c->dyn[1].pos, c->dyn[a].vel, c->dyn[a].theta, c->dyn[a].omega};
+}
+StatSet step_in_static(DemContext* c, int a) {
+    return StatSet{c->stat[a ^ 1].radius, c->stat[a].mass, c->stat[a].id, c->stat[a].type};
+}
+// The current state (order of the last sort), see DemContext.
+DynSet state_dyn(DemContext* c) {
+    return DynSet{c->dyn[0].pos, c->dyn[c->cur].vel, c->dyn[c->cur].theta, c->dyn[c->cur].omega};
+}
+
 cudaError_t enqueue_step_kernel(DemContext* c, cudaStream_t st, int* launches) {
-    const int b = c->cur ^ 1;
+    const int a = c->cur, b = a ^ 1;
     ControlArgs ctl{};
     if (c->ctlOn) ctl = ControlArgs{c->dCtl, c->ctlVec, c->ctlVec + c->capacity,
                                     c->ctlVec + 2ull * c->capacity};
-    cudaError_t e = launch_step(c->P, c->dyn[1], c->stat[b], c->skey[b], c->cells[b],
-                                c->first[b], c->dyn[0],
+    const DynSet out{c->dyn[0].pos, c->dyn[b].vel, c->dyn[b].theta, c->dyn[b].omega};
+    cudaError_t e = launch_step(c->P, step_in(c, a), step_in_static(c, a), c->src, c->skey[b],
+                                c->cells[b], c->first[b], out, c->stat[b], c->loc,
                                 c->keys, (c->flags & DEM_CTX_PRESSURE) ? c->pressure : nullptr,
                                 (c->flags & DEM_CTX_ACCEL) ? c->acc : nullptr,
                                 (c->flags & DEM_CTX_ACCEL) ? c->alpha : nullptr, c->errFlag, c->n,
@@ -707,7 +730,7 @@ int init_context(DemContext* c, uint32_t capacity, uint32_t numCells, DemContext
     size_t total = 0;
     total += 2 * (f8p + f8 + 2 * f4);            // dyn sets
     total += 2 * (f4p + 2 * f4 + (c->typed ? f4 : 0));  // static sets
-    total += 3 * f4 + 2 * f4;                    // loc, keys, perm, sorted keys x2
+    total += 4 * f4 + 2 * f4;                    // loc, keys, perm, src, sorted keys x2
     total += 2 * cells8 + 2 * first4;            // cell ranges and first particles x2
     total += f4 + f8 + f4;                       // pressure, acc, alpha
     total += 256;                                // error flag
@@ -738,6 +761,7 @@ int init_context(DemContext* c, uint32_t capacity, uint32_t numCells, DemContext
     c->loc = reinterpret_cast<uint32_t*>(take(f4));
     c->keys = reinterpret_cast<uint32_t*>(take(f4));
     c->perm = reinterpret_cast<uint32_t*>(take(f4));
+    c->src = reinterpret_cast<uint32_t*>(take(f4));
     for (int s = 0; s < 2; ++s) {
         c->skey[s] = reinterpret_cast<uint32_t*>(take(f4));
         c->cells[s] = reinterpret_cast<uint2*>(take(cells8));
@@ -868,9 +892,9 @@ extern "C" int dem_set_state(DemContext* c, uint32_t n, const float* pos, const 
     const cudaMemcpyKind k = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
     const int a = c->cur;
     DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[0].pos, pos, 8ull * n, k, st), "set pos");
-    DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[0].vel, vel, 8ull * n, k, st), "set vel");
-    DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[0].theta, theta, 4ull * n, k, st), "set theta");
-    DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[0].omega, omega, 4ull * n, k, st), "set omega");
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[a].vel, vel, 8ull * n, k, st), "set vel");
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[a].theta, theta, 4ull * n, k, st), "set theta");
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[a].omega, omega, 4ull * n, k, st), "set omega");
     DEM_TRY_CUDA(cudaMemcpyAsync(c->stat[a].radius, radius, 4ull * n, k, st), "set radius");
     DEM_TRY_CUDA(cudaMemcpyAsync(c->stat[a].mass, mass, 4ull * n, k, st), "set mass");
     DEM_TRY_CUDA(cudaMemcpyAsync(c->stat[a].id, id, 4ull * n, k, st), "set id");
@@ -912,9 +936,9 @@ extern "C" int dem_get_state(DemContext* c, float* pos, float* vel, float* theta
     const uint32_t n = c->n;
     const int a = c->cur;
     if (pos) DEM_TRY_CUDA(cudaMemcpyAsync(pos, c->dyn[0].pos, 8ull * n, k, st), "get pos");
-    if (vel) DEM_TRY_CUDA(cudaMemcpyAsync(vel, c->dyn[0].vel, 8ull * n, k, st), "get vel");
-    if (theta) DEM_TRY_CUDA(cudaMemcpyAsync(theta, c->dyn[0].theta, 4ull * n, k, st), "get theta");
-    if (omega) DEM_TRY_CUDA(cudaMemcpyAsync(omega, c->dyn[0].omega, 4ull * n, k, st), "get omega");
+    if (vel) DEM_TRY_CUDA(cudaMemcpyAsync(vel, c->dyn[a].vel, 8ull * n, k, st), "get vel");
+    if (theta) DEM_TRY_CUDA(cudaMemcpyAsync(theta, c->dyn[a].theta, 4ull * n, k, st), "get theta");
+    if (omega) DEM_TRY_CUDA(cudaMemcpyAsync(omega, c->dyn[a].omega, 4ull * n, k, st), "get omega");
     if (radius) DEM_TRY_CUDA(cudaMemcpyAsync(radius, c->stat[a].radius, 4ull * n, k, st), "get radius");
     if (mass) DEM_TRY_CUDA(cudaMemcpyAsync(mass, c->stat[a].mass, 4ull * n, k, st), "get mass");
     if (id) DEM_TRY_CUDA(cudaMemcpyAsync(id, c->stat[a].id, 4ull * n, k, st), "get id");
@@ -1114,7 +1138,7 @@ extern "C" int dem_get_followed(DemContext* c, const uint32_t* ids, uint32_t cou
         FollowIds f;
         f.count = count - base < kFollowBatch ? count - base : kFollowBatch;
         for (uint32_t i = 0; i < f.count; ++i) f.id[i] = ids[base + i];
-        DEM_TRY_CUDA(launch_followed(f, c->loc, c->dyn[0], c->stat[a],
+        DEM_TRY_CUDA(launch_followed(f, c->loc, state_dyn(c), c->stat[a],
                                      (c->flags & DEM_CTX_ACCEL) ? c->acc : nullptr,
                                      (c->flags & DEM_CTX_ACCEL) ? c->alpha : nullptr,
                                      (c->flags & DEM_CTX_PRESSURE) ? c->pressure : nullptr,
@@ -1177,7 +1201,7 @@ extern "C" int dem_render(DemContext* c, const DemRenderParams* rp, void* image,
     }
     const int a = c->cur;
     DEM_TRY_CUDA(launch_render(*rp, c->sys.cubeDimension[0], c->sys.cubeDimension[1],
-                               c->dyn[0].pos, c->dyn[0].theta, c->typed ? c->stat[a].type : nullptr,
+                               c->dyn[0].pos, c->dyn[a].theta, c->typed ? c->stat[a].type : nullptr,
                                c->stat[a].radius,
                                (c->flags & DEM_CTX_PRESSURE) ? c->pressure : nullptr, c->n,
                                c->renderOwner, static_cast<uchar4*>(image), (cudaStream_t)stream),
@@ -1340,7 +1364,8 @@ int step_recorded(DemContext* c, cudaStream_t st, char* rec) {
     // the step kernel leaves the sorted state it read intact: record it, the
     // cell ranges and the accelerations in one launch
     if (rec)
-        DEM_TRY_CUDA(adj_record_step(rec, c->n, c->numCells, c->dyn[1], c->stat[b], c->cells[b],
+        DEM_TRY_CUDA(adj_record_step(rec, c->n, c->numCells, step_in(c, p), step_in_static(c, p),
+                                     c->src, c->cells[b],
                                      c->acc, c->alpha, st),
                      "record");
     c->cur ^= 1;

@@ -194,43 +194,12 @@ __global__ void arrivals_scatter_kernel(const uint4* __restrict__ movers,
     }
 }
 
-// One particle's fields, read in one round of independent loads.
-struct ParticleRec {
-    float2 pos, vel;
-    float theta, omega, radius, mass;
-    uint32_t id, type;
-};
-
-__device__ __forceinline__ ParticleRec load_particle(uint32_t src, DynSet from, StatSet fromS) {
-    ParticleRec r;
-    r.pos = from.pos[src];
-    r.vel = from.vel[src];
-    r.theta = from.theta[src];
-    r.omega = from.omega[src];
-    r.radius = fromS.radius[src];
-    r.mass = fromS.mass[src];
-    r.id = fromS.id[src];
-    r.type = fromS.type ? fromS.type[src] : 0u;
-    return r;
-}
-
-__device__ __forceinline__ void store_particle(const ParticleRec& r, uint32_t dst, DynSet to,
-                                               StatSet toS, uint32_t* __restrict__ loc) {
-    to.pos[dst] = r.pos;
-    to.vel[dst] = r.vel;
-    to.theta[dst] = r.theta;
-    to.omega[dst] = r.omega;
-    toS.radius[dst] = r.radius;
-    toS.mass[dst] = r.mass;
-    toS.id[dst] = r.id;
-    loc[r.id] = dst;
-    if (toS.type) toS.type[dst] = r.type;
-}
-
-__device__ __forceinline__ void move_particle(uint32_t src, uint32_t dst, DynSet from,
-                                              StatSet fromS, DynSet to, StatSet toS,
-                                              uint32_t* __restrict__ loc) {
-    store_particle(load_particle(src, from, fromS), dst, to, toS, loc);
+// A particle's move to its sorted slot: position and radius (what neighbour
+// searches read in sorted order) and the slot it came from.
+__device__ __forceinline__ void move_particle(uint32_t from, uint32_t dst, const SortMove& m) {
+    m.posOut[dst] = m.pos[from];
+    m.radiusOut[dst] = m.radius[from];
+    m.src[dst] = from;
 }
 
 // A mover goes after the arrivals of its new cell with smaller index, and
@@ -240,9 +209,7 @@ __global__ void place_movers_kernel(const uint4* __restrict__ movers,
                                     const uint2* __restrict__ arrInfo,
                                     const uint32_t* __restrict__ arrSlots,
                                     const uint2* __restrict__ newCells,
-                                    uint32_t* __restrict__ newSortedKey, DynSet from,
-                                    StatSet fromS, DynSet to, StatSet toS,
-                                    uint32_t* __restrict__ loc) {
+                                    uint32_t* __restrict__ newSortedKey, SortMove mv) {
     if (ctrl[kCtrlPath]) return;
     const uint32_t count = min(ctrl[kCtrlMovers], cap);
     for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < count;
@@ -256,7 +223,7 @@ __global__ void place_movers_kernel(const uint4* __restrict__ movers,
         const uint32_t stay = (cr.y - cr.x) - info.y;
         const uint32_t dst = cr.x + rank + (r.z > r.y ? stay : 0u);
         newSortedKey[dst] = r.y;
-        move_particle(r.x, dst, from, fromS, to, toS, loc);
+        move_particle(r.x, dst, mv);
     }
 }
 
@@ -267,15 +234,16 @@ __global__ void __launch_bounds__(kThreads)
 place_stayers_kernel(uint32_t n, const uint32_t* __restrict__ keys,
                      const uint32_t* __restrict__ prevSortedKey,
                      const uint2* __restrict__ prevCells, const uint32_t* __restrict__ stayBase,
-                     uint32_t* __restrict__ newSortedKey, DynSet from, StatSet fromS, DynSet to,
-                     StatSet toS, uint32_t* __restrict__ loc, uint32_t* __restrict__ ctrl) {
+                     uint32_t* __restrict__ newSortedKey, SortMove mv,
+                     uint32_t* __restrict__ ctrl) {
     if (ctrl[kCtrlPath]) return;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) ctrl[kCtrlMovers] = 0u;  // movers were consumed by the previous kernels
     if (i >= n) return;
     const uint32_t o = prevSortedKey[i];
     const uint32_t k = keys[i];
-    const ParticleRec rec = load_particle(i, from, fromS);
+    const float2 p = mv.pos[i];
+    const float r = mv.radius[i];
     if (k != o) return;
     const uint32_t os = prevCells[o].x;
     const uint32_t sb = stayBase[o];
@@ -286,7 +254,9 @@ place_stayers_kernel(uint32_t n, const uint32_t* __restrict__ keys,
     }
     const uint32_t dst = (sb & ~kHasLeavers) + rank;
     newSortedKey[dst] = o;
-    store_particle(rec, dst, to, toS, loc);
+    mv.posOut[dst] = p;
+    mv.radiusOut[dst] = r;
+    mv.src[dst] = i;
 }
 
 // First particle of every cell c <= numCells (for an empty cell, that of the
@@ -310,8 +280,7 @@ __global__ void cell_first_kernel(const uint32_t* __restrict__ sortedKey, uint32
 __global__ void __launch_bounds__(kThreads)
 full_reorder_kernel(uint32_t n, const uint32_t* __restrict__ hash,
                     const uint32_t* __restrict__ index, uint2* __restrict__ cells,
-                    uint32_t* __restrict__ newSortedKey, DynSet from, StatSet fromS, DynSet to,
-                    StatSet toS, uint32_t* __restrict__ loc) {
+                    uint32_t* __restrict__ newSortedKey, SortMove mv) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = i < n;
     const uint32_t h = valid ? hash[i] : 0u;
@@ -324,7 +293,7 @@ full_reorder_kernel(uint32_t n, const uint32_t* __restrict__ hash,
     }
     if (i == n - 1) cells[h].y = i + 1;
     newSortedKey[i] = h;
-    move_particle(index[i], i, from, fromS, to, toS, loc);
+    move_particle(index[i], i, mv);
 }
 
 }  // namespace
@@ -373,8 +342,7 @@ cudaError_t enqueue_incremental_head(const IncSort& s, const uint2* prevCells,
 cudaError_t enqueue_incremental_tail(const IncSort& s, uint32_t n, const uint32_t* keys,
                                      const uint32_t* prevSortedKey, const uint2* prevCells,
                                      uint32_t* newSortedKey, uint2* newCells, uint32_t* newFirst,
-                                     DynSet from, StatSet fromS, DynSet to, StatSet toS,
-                                     uint32_t* loc, cudaStream_t st, int* launches) {
+                                     const SortMove& mv, cudaStream_t st, int* launches) {
     const uint32_t C = s.numCells;
     const uint32_t items = cell_items(C);
     const size_t nb = cell_blocks(C);
@@ -388,12 +356,10 @@ cudaError_t enqueue_incremental_tail(const IncSort& s, uint32_t n, const uint32_
     arrivals_scatter_kernel<<<mb, kThreads, 0, st>>>(s.movers, s.ctrl, s.moverCap, s.arrInfo,
                                                      s.arrSlots);
     place_movers_kernel<<<mb, kThreads, 0, st>>>(s.movers, s.ctrl, s.moverCap, s.arrInfo,
-                                                 s.arrSlots, newCells, newSortedKey, from, fromS,
-                                                 to, toS, loc);
+                                                 s.arrSlots, newCells, newSortedKey, mv);
     if (n) {
         place_stayers_kernel<<<blocks_for(n, kThreads), kThreads, 0, st>>>(
-            n, keys, prevSortedKey, prevCells, s.stayBase, newSortedKey, from, fromS, to, toS,
-            loc, s.ctrl);
+            n, keys, prevSortedKey, prevCells, s.stayBase, newSortedKey, mv, s.ctrl);
     }
     if (launches) *launches += 5;
     return cudaGetLastError();
@@ -402,8 +368,7 @@ cudaError_t enqueue_incremental_tail(const IncSort& s, uint32_t n, const uint32_
 cudaError_t enqueue_full(const IncSort& s, uint32_t n, uint32_t keyBits, uint32_t* keys,
                          uint32_t* perm, const OnesweepScratch& os, uint32_t* errFlag,
                          uint32_t* newSortedKey, uint2* newCells, uint32_t* newFirst,
-                         DynSet from, StatSet fromS, DynSet to, StatSet toS, uint32_t* loc,
-                         cudaStream_t st, int* launches) {
+                         const SortMove& mv, cudaStream_t st, int* launches) {
     uint32_t *ko, *vo;
     cudaError_t e = onesweep_sort_pairs(keys, perm, n, keyBits, true, os, errFlag, st, &ko, &vo,
                                         launches);
@@ -413,7 +378,7 @@ cudaError_t enqueue_full(const IncSort& s, uint32_t n, uint32_t keyBits, uint32_
     if (e != cudaSuccess) return e;
     if (n) {
         full_reorder_kernel<<<blocks_for(n, kThreads), kThreads, 0, st>>>(
-            n, ko, vo, newCells, newSortedKey, from, fromS, to, toS, loc);
+            n, ko, vo, newCells, newSortedKey, mv);
         if (launches) ++*launches;
     }
     cell_first_kernel<<<std::min<unsigned>(blocks_for((size_t)s.numCells + 1, kThreads), 148u * 8u),

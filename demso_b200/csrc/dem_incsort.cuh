@@ -15,8 +15,9 @@
 //                 start and its arrivals' base;
 //   movers      : each mover's rank among its cell's arrivals by index;
 //   placement   : every particle computes its sorted position and moves its
-//                 own state there (scatter, nearly coalesced), writing
-//                 loc[id] and its sorted key.
+//                 position and radius there (scatter, nearly coalesced),
+//                 with its sorted key and the slot it came from; the step
+//                 kernel gathers the other fields through that slot.
 // The result is identical to the stable radix sort + reorder of the
 // reference.  When the mover list overflows, an arrival group or a leaving
 // cell is larger than kMaxGroup, or there is no previous order (first
@@ -38,6 +39,17 @@ constexpr uint32_t kCtrlNeedFull = 0;        // ctrl[0]: non-zero -> full path n
 constexpr uint32_t kCtrlMovers = 1;          // ctrl[1]: movers recorded by the step kernel
 constexpr uint32_t kCtrlPath = 2;            // ctrl[2]: this step runs the full path
 constexpr uint32_t kHasLeavers = 0x80000000u;  // flag bit in stayBase
+
+// The state the sort phase moves: positions and radii from the previous
+// order to the sorted one, and for every sorted slot the previous slot of
+// its particle (src).
+struct SortMove {
+    const float2* pos;
+    const float* radius;
+    float2* posOut;
+    float* radiusOut;
+    uint32_t* src;
+};
 
 // Buffers of the incremental path (all device memory, owned by the context).
 struct IncSort {
@@ -67,15 +79,13 @@ cudaError_t enqueue_incremental_head(const IncSort& s, const uint2* prevCells,
 cudaError_t enqueue_incremental_tail(const IncSort& s, uint32_t n, const uint32_t* keys,
                                      const uint32_t* prevSortedKey, const uint2* prevCells,
                                      uint32_t* newSortedKey, uint2* newCells, uint32_t* newFirst,
-                                     DynSet from, StatSet fromS, DynSet to, StatSet toS,
-                                     uint32_t* loc, cudaStream_t st, int* launches);
+                                     const SortMove& mv, cudaStream_t st, int* launches);
 
 // Full path: onesweep sort of `keys`, cell ranges, gather, reset of the
 // incremental counters.  `perm` and `keys` are overwritten.
 cudaError_t enqueue_full(const IncSort& s, uint32_t n, uint32_t keyBits, uint32_t* keys,
                          uint32_t* perm, const OnesweepScratch& os, uint32_t* errFlag,
                          uint32_t* newSortedKey, uint2* newCells, uint32_t* newFirst,
-                         DynSet from, StatSet fromS, DynSet to, StatSet toS, uint32_t* loc,
-                         cudaStream_t st, int* launches);
+                         const SortMove& mv, cudaStream_t st, int* launches);
 
 }  // namespace dem

@@ -134,19 +134,23 @@ __device__ __forceinline__ void candidate(const KParams& P, uint32_t j, float2 p
                                           const float2* __restrict__ vel,
                                           const float* __restrict__ omega,
                                           const float* __restrict__ radius,
-                                          const uint32_t* __restrict__ type, float2& fc,
+                                          const uint32_t* __restrict__ type,
+                                          const uint32_t* __restrict__ src, float2& fc,
                                           float& moment, float& pr) {
     const float rj = __ldg(radius + j);
+    // velocity, spin and type of candidate j sit at its slot of the previous
+    // order (src), or at j when the arrays are all in one order (src null)
+    const uint32_t sj = src ? __ldg(src + j) : j;
     uint32_t mj = 0;
     float4 pc = P.pair[0];
     if (TYPED) {
-        mj = __ldg(type + j);
+        mj = __ldg(type + sj);
         pc = P.pair[mat * P.nmat + mj];
     }
     const float cd = r + rj;
     // d2 > cd^2 (1 + 2e-6) implies sqrtf(d2) >= cd after rounding: no contact
     if (d2 <= cd * cd * 1.000002f && sqrtf(d2) < cd) {
-        const float2 f = pair_force(p, pj, v, __ldg(vel + j), w, __ldg(omega + j), r, rj, pc,
+        const float2 f = pair_force(p, pj, v, __ldg(vel + sj), w, __ldg(omega + sj), r, rj, pc,
                                     P.dt, moment, pr);
         fc.x += f.x;
         fc.y += f.y;
@@ -188,7 +192,8 @@ __device__ __forceinline__ void collide_one(const KParams& P, uint32_t i, int2 g
                                             const float2* __restrict__ vel,
                                             const float* __restrict__ omega,
                                             const float* __restrict__ radius,
-                                            const uint32_t* __restrict__ type, Cells cells,
+                                            const uint32_t* __restrict__ type,
+                                            const uint32_t* __restrict__ src, Cells cells,
                                             float2& force, float& moment, float& pr) {
     force = make_float2(0.0f, 0.0f);
     moment = 0.0f;
@@ -227,10 +232,10 @@ __device__ __forceinline__ void collide_one(const KParams& P, uint32_t i, int2 g
                 const float db = bx * bx + by * by;
                 if (j != i && (ATTRACT || !CULL || da <= reach2))
                     candidate<TYPED, ATTRACT>(P, j, p, v, w, r, mat, pa, da, vel, omega, radius,
-                                              type, fc, moment, pr);
+                                              type, src, fc, moment, pr);
                 if (j + 1 != i && (ATTRACT || !CULL || db <= reach2))
                     candidate<TYPED, ATTRACT>(P, j + 1, p, v, w, r, mat, pb, db, vel, omega,
-                                              radius, type, fc, moment, pr);
+                                              radius, type, src, fc, moment, pr);
             }
             if ((count & 1u) && j != i) {
                 const float2 pa = __ldg(pos + j);
@@ -238,7 +243,7 @@ __device__ __forceinline__ void collide_one(const KParams& P, uint32_t i, int2 g
                 const float da = ax * ax + ay * ay;
                 if (ATTRACT || !CULL || da <= reach2)
                     candidate<TYPED, ATTRACT>(P, j, p, v, w, r, mat, pa, da, vel, omega, radius,
-                                              type, fc, moment, pr);
+                                              type, src, fc, moment, pr);
             }
             force.x += fc.x;
             force.y += fc.y;
@@ -277,6 +282,7 @@ __device__ __forceinline__ bool collide_rows(const KParams& P, uint32_t i, int2 
                                              const float* __restrict__ omega,
                                              const float* __restrict__ radius,
                                              const uint32_t* __restrict__ type,
+                                             const uint32_t* __restrict__ src,
                                              const uint32_t* __restrict__ cellFirst,
                                              float2& force, float& moment, float& pr) {
     int y0 = -1, y1 = 1, x0 = -1, x1 = 1;
@@ -354,8 +360,9 @@ __device__ __forceinline__ bool collide_rows(const KParams& P, uint32_t i, int2 
                 mask &= mask - 1u;
                 const float rj = __ldg(radius + j);
                 float4 pc = pc0;
-                if (TYPED) pc = P.pair[mat * P.nmat + __ldg(type + j)];
-                const float2 f = pair_force(p, __ldg(pos + j), v, __ldg(vel + j), w, __ldg(omega + j),
+                const uint32_t sj = __ldg(src + j);
+                if (TYPED) pc = P.pair[mat * P.nmat + __ldg(type + sj)];
+                const float2 f = pair_force(p, __ldg(pos + j), v, __ldg(vel + sj), w, __ldg(omega + sj),
                                             r, rj, pc, P.dt, moment, pr);
                 if (j >= b2) { f2.x += f.x; f2.y += f.y; }
                 else if (j >= b1) { f1.x += f.x; f1.y += f.y; }
@@ -387,8 +394,8 @@ collide_kernel(KParams P, const float2* __restrict__ pos, const float2* __restri
     float2 f;
     float moment, pr;
     collide_one<TYPED, ATTRACT, false>(P, i, grid_pos(P, p), p, v, w, r, mat, pos, vel, omega,
-                                       radius, type, SplitCells{cellStart, cellEnd}, f, moment,
-                                       pr);
+                                       radius, type, nullptr, SplitCells{cellStart, cellEnd}, f,
+                                       moment, pr);
     const float m = mass[i];
     acc[i] = make_float2(f.x / m, f.y / m);
     alpha[i] = moment / inertia_of(m, r);
@@ -425,9 +432,10 @@ integrate_kernel(KParams P, float2* __restrict__ pos, float2* __restrict__ vel,
 template <bool TYPED>
 __device__ __forceinline__ void finish_particle(
     const KParams& P, uint32_t i, Dyn& s, float2 f, float moment, float pr, float r, float m,
-    uint32_t mat, uint32_t key, const uint2* __restrict__ cellRange, DynSet out,
-    uint32_t* __restrict__ nextHash, float* __restrict__ pressure, float2* __restrict__ acc,
-    float* __restrict__ alpha, uint32_t* __restrict__ errFlag, MoverSinkArgs sink) {
+    uint32_t mat, uint32_t id, uint32_t key, const uint2* __restrict__ cellRange, DynSet out,
+    StatSet outS, uint32_t* __restrict__ loc, uint32_t* __restrict__ nextHash,
+    float* __restrict__ pressure, float2* __restrict__ acc, float* __restrict__ alpha,
+    uint32_t* __restrict__ errFlag, MoverSinkArgs sink) {
     // F/m and M/I as the reference divides them.  Without contacts F and M
     // are +0 (sums that start at +0 never become -0), and +0 divided by a
     // positive finite mass or inertia is exactly +0, so the divisions are
@@ -447,10 +455,15 @@ __device__ __forceinline__ void finish_particle(
     if (acc) acc[i] = a;
     if (alpha) alpha[i] = al;
     integrate_one(P, s, a, al, r, m, mat, pr);
+    // the new state in this step's sorted order
     out.pos[i] = s.p;
     out.vel[i] = s.v;
     out.theta[i] = s.th;
     out.omega[i] = s.w;
+    outS.mass[i] = m;
+    outS.id[i] = id;
+    if (TYPED) outS.type[i] = mat;
+    loc[id] = i;
     if (pressure) pressure[i] = pr;
     const int2 gn = grid_pos_fast(P, s.p);
     const uint32_t nk = grid_hash(P, gn.x, gn.y);
@@ -475,24 +488,29 @@ __device__ __forceinline__ void finish_particle(
 // the arithmetic is the same expressions in the same order.
 template <bool TYPED, bool ATTRACT, bool CULL, bool CONTROL = false>
 __device__ __forceinline__ void step_particle(const KParams& P, uint32_t i, DynSet in,
-                                              StatSet inS,
+                                              StatSet inS, const uint32_t* __restrict__ src,
                                               const uint32_t* __restrict__ sortedKey,
                                               const uint2* __restrict__ cellRange,
                                               const uint32_t* __restrict__ cellFirst, DynSet out,
+                                              StatSet outS, uint32_t* __restrict__ loc,
                                               uint32_t* __restrict__ nextHash,
                                               float* __restrict__ pressure,
                                               float2* __restrict__ acc,
                                               float* __restrict__ alpha,
                                               uint32_t* __restrict__ errFlag, MoverSinkArgs sink,
                                               ControlArgs ctl = ControlArgs{}) {
+    // position and radius are in this step's sorted order; the other fields
+    // at the particle's slot of the previous order, src[i]
     Dyn s;
     s.p = in.pos[i];
-    s.v = in.vel[i];
-    s.w = in.omega[i];
-    s.th = in.theta[i];
     const float r = inS.radius[i];
-    const float m = inS.mass[i];
-    const uint32_t mat = TYPED ? inS.type[i] : 0u;
+    const uint32_t si = src[i];
+    s.v = in.vel[si];
+    s.w = in.omega[si];
+    s.th = in.theta[si];
+    const float m = inS.mass[si];
+    const uint32_t id = inS.id[si];
+    const uint32_t mat = TYPED ? inS.type[si] : 0u;
     // the sort key of particle i is calcGridPos of this very position, wrapped
     const uint32_t key = sortedKey[i];
     const uint32_t local = key - P.cellOff;
@@ -501,14 +519,14 @@ __device__ __forceinline__ void step_particle(const KParams& P, uint32_t i, DynS
     float moment, pr;
     if (ATTRACT || !CULL || !P.cull ||
         !collide_rows<TYPED>(P, i, g, s.p, s.v, s.w, r, mat, in.pos, in.vel, in.omega,
-                             inS.radius, inS.type, cellFirst, f, moment, pr)) {
+                             inS.radius, inS.type, src, cellFirst, f, moment, pr)) {
         if (CULL && P.cull)
             collide_one<TYPED, ATTRACT, true>(P, i, g, s.p, s.v, s.w, r, mat, in.pos, in.vel,
-                                              in.omega, inS.radius, inS.type,
+                                              in.omega, inS.radius, inS.type, src,
                                               PackedCells{cellRange}, f, moment, pr);
         else
             collide_one<TYPED, ATTRACT, false>(P, i, g, s.p, s.v, s.w, r, mat, in.pos, in.vel,
-                                               in.omega, inS.radius, inS.type,
+                                               in.omega, inS.radius, inS.type, src,
                                                PackedCells{cellRange}, f, moment, pr);
     }
     if (CONTROL) {
@@ -532,8 +550,8 @@ __device__ __forceinline__ void step_particle(const KParams& P, uint32_t i, DynS
         ctl.fy[i] = -fc.y;
         ctl.fm[i] = -mc / r * c.radius;
     }
-    finish_particle<TYPED>(P, i, s, f, moment, pr, r, m, mat, key, cellRange, out, nextHash,
-                           pressure, acc, alpha, errFlag, sink);
+    finish_particle<TYPED>(P, i, s, f, moment, pr, r, m, mat, id, key, cellRange, out, outS, loc,
+                           nextHash, pressure, acc, alpha, errFlag, sink);
 }
 
 // THREADS x MINB: the block size and the blocks per SM the registers are
@@ -541,16 +559,17 @@ __device__ __forceinline__ void step_particle(const KParams& P, uint32_t i, DynS
 template <bool TYPED, bool ATTRACT, bool CULL, bool CONTROL, int THREADS = kCollideThreads,
           int MINB = 1024 / kCollideThreads>
 __global__ void __launch_bounds__(THREADS, MINB)
-step_kernel(KParams P, DynSet in, StatSet inS, const uint32_t* __restrict__ sortedKey,
-            const uint2* __restrict__ cellRange, const uint32_t* __restrict__ cellFirst, DynSet out,
-            uint32_t* __restrict__ nextHash,
+step_kernel(KParams P, DynSet in, StatSet inS, const uint32_t* __restrict__ src,
+            const uint32_t* __restrict__ sortedKey, const uint2* __restrict__ cellRange,
+            const uint32_t* __restrict__ cellFirst, DynSet out, StatSet outS,
+            uint32_t* __restrict__ loc, uint32_t* __restrict__ nextHash,
             float* __restrict__ pressure, float2* __restrict__ acc, float* __restrict__ alpha,
             uint32_t* __restrict__ errFlag, uint32_t n, MoverSinkArgs sink, ControlArgs ctl) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    step_particle<TYPED, ATTRACT, CULL, CONTROL>(P, i, in, inS, sortedKey, cellRange, cellFirst, out,
-                                                 nextHash, pressure, acc, alpha, errFlag, sink,
-                                                 ctl);
+    step_particle<TYPED, ATTRACT, CULL, CONTROL>(P, i, in, inS, src, sortedKey, cellRange,
+                                                 cellFirst, out, outS, loc, nextHash, pressure,
+                                                 acc, alpha, errFlag, sink, ctl);
 }
 
 // reduceVecD (particles_kernel.cuh:551-578) for the three reaction vectors,
@@ -612,15 +631,18 @@ template <bool TYPED, bool ATTRACT, bool CULL, int THREADS = kCollideThreads,
           int MINB = 1024 / kCollideThreads>
 __global__ void __launch_bounds__(THREADS, MINB)
 step_kernel_batched(const KParams* __restrict__ table, const uint32_t* __restrict__ spec,
-                    DynSet in, StatSet inS, const uint32_t* __restrict__ sortedKey,
-                    const uint2* __restrict__ cellRange, const uint32_t* __restrict__ cellFirst,
-                    DynSet out, uint32_t* __restrict__ nextHash, float* __restrict__ pressure,
-                    float2* __restrict__ acc, float* __restrict__ alpha,
-                    uint32_t* __restrict__ errFlag, uint32_t n, MoverSinkArgs sink) {
+                    DynSet in, StatSet inS, const uint32_t* __restrict__ src,
+                    const uint32_t* __restrict__ sortedKey, const uint2* __restrict__ cellRange,
+                    const uint32_t* __restrict__ cellFirst, DynSet out, StatSet outS,
+                    uint32_t* __restrict__ loc, uint32_t* __restrict__ nextHash,
+                    float* __restrict__ pressure, float2* __restrict__ acc,
+                    float* __restrict__ alpha, uint32_t* __restrict__ errFlag, uint32_t n,
+                    MoverSinkArgs sink) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    step_particle<TYPED, ATTRACT, CULL>(table[spec[i]], i, in, inS, sortedKey, cellRange, cellFirst, out,
-                                        nextHash, pressure, acc, alpha, errFlag, sink);
+    step_particle<TYPED, ATTRACT, CULL>(table[spec[i]], i, in, inS, src, sortedKey, cellRange,
+                                        cellFirst, out, outS, loc, nextHash, pressure, acc,
+                                        alpha, errFlag, sink);
 }
 
 // Reorder for the context step: as reorder_kernel, but the cell ranges are
@@ -796,11 +818,13 @@ cudaError_t launch_integrate(const KParams& P, float2* pos, float2* vel, const f
     return cudaGetLastError();
 }
 
-cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t* sortedKey,
-                        const uint2* cellRange, const uint32_t* cellFirst, DynSet out, uint32_t* nextHash, float* pressure,
-                        float2* acc, float* alpha, uint32_t* errFlag, uint32_t n,
-                        MoverSinkArgs sink, cudaStream_t st, const KParams* table,
-                        const uint32_t* spec, ControlArgs ctl, int variant) {
+cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t* src,
+                        const uint32_t* sortedKey, const uint2* cellRange,
+                        const uint32_t* cellFirst, DynSet out, StatSet outS, uint32_t* loc,
+                        uint32_t* nextHash, float* pressure, float2* acc, float* alpha,
+                        uint32_t* errFlag, uint32_t n, MoverSinkArgs sink, cudaStream_t st,
+                        const KParams* table, const uint32_t* spec, ControlArgs ctl,
+                        int variant) {
     if (n == 0) return cudaSuccess;
     if (variant < 0 || variant >= kStepVariants) return cudaErrorInvalidValue;
     const bool typed = inS.type != nullptr && P.nmat > 1;
@@ -811,15 +835,18 @@ cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t
         const unsigned b = blocks_for(n, TH);                                                  \
         if (table)                                                                             \
             step_kernel_batched<T, A, C, TH, MB><<<b, TH, 0, st>>>(                            \
-                table, spec, in, inS, sortedKey, cellRange, cellFirst, out, nextHash, pressure, acc, alpha, \
+                table, spec, in, inS, src, sortedKey, cellRange, cellFirst, out, outS, loc,     \
+                nextHash, pressure, acc, alpha, \
                 errFlag, n, sink);                                                             \
         else if (ctl.c)                                                                        \
             step_kernel<T, A, C, true><<<blocks_for(n, kCollideThreads), kCollideThreads, 0,  \
-                                         st>>>(P, in, inS, sortedKey, cellRange, cellFirst, out, nextHash, \
+                                         st>>>(P, in, inS, src, sortedKey, cellRange, cellFirst, \
+                                               out, outS, loc, nextHash, \
                                                pressure, acc, alpha, errFlag, n, sink, ctl);  \
         else                                                                                   \
             step_kernel<T, A, C, false, TH, MB><<<b, TH, 0, st>>>(                             \
-                P, in, inS, sortedKey, cellRange, cellFirst, out, nextHash, pressure, acc, alpha, errFlag, \
+                P, in, inS, src, sortedKey, cellRange, cellFirst, out, outS, loc, nextHash,    \
+                pressure, acc, alpha, errFlag, \
                 n, sink, ctl);                                                                 \
     } while (0)
 #define DEM_STEP(T, A, C)                                                                      \

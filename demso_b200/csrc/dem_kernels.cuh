@@ -87,16 +87,21 @@ struct ControlArgs {
     float* fy;
     float* fm;
 };
+// The context step kernel.  in.pos and inS.radius are in this step's sorted
+// order; the particle at sorted slot i has its other fields (in.vel, theta,
+// omega, inS.mass, id, type) at slot src[i] of the previous order.  The new
+// state is written in the sorted order: positions, velocities, angles and
+// spins to `out`, mass, id and type to `outS`, and loc[id] = slot.
 // cellRange: (start, end) of every cell; cellFirst: numCells + 4 words, the
 // first particle of every cell (for an empty cell, that of the next
 // non-empty one) and n at [numCells].
-cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t* sortedKey,
-                        const uint2* cellRange, const uint32_t* cellFirst, DynSet out,
-                        uint32_t* nextHash, float* pressure,
-                        float2* acc, float* alpha, uint32_t* errFlag, uint32_t n,
-                        MoverSinkArgs sink, cudaStream_t st, const KParams* table = nullptr,
-                        const uint32_t* spec = nullptr, ControlArgs ctl = ControlArgs{},
-                        int variant = 0);
+cudaError_t launch_step(const KParams& P, DynSet in, StatSet inS, const uint32_t* src,
+                        const uint32_t* sortedKey, const uint2* cellRange,
+                        const uint32_t* cellFirst, DynSet out, StatSet outS, uint32_t* loc,
+                        uint32_t* nextHash, float* pressure, float2* acc, float* alpha,
+                        uint32_t* errFlag, uint32_t n, MoverSinkArgs sink, cudaStream_t st,
+                        const KParams* table = nullptr, const uint32_t* spec = nullptr,
+                        ControlArgs ctl = ControlArgs{}, int variant = 0);
 // Launch shapes of the step kernel: threads per block x the blocks per SM its
 // registers are capped for (variant 0: 128 x 8, 1: 64 x 16, 2: 256 x 4,
 // 3: 128 x 6, which allows 80 registers).  All compute the same bits; the
@@ -128,11 +133,12 @@ cudaError_t launch_unpack_cells(const uint2* cellRange, uint32_t numCells, uint3
 // Adjoint (dem_adjoint.cu).
 size_t adj_step_bytes(uint32_t n, uint32_t numCells);
 // Writes the record of one forward step at recBase in one launch: the sorted
-// state the step kernel stepped (d, s), its cell ranges and the acceleration
-// and angular acceleration it produced.
+// state the step kernel stepped (d, s and src as launch_step's in, inS and
+// src), its cell ranges and the acceleration and angular acceleration it
+// produced.
 cudaError_t adj_record_step(void* recBase, uint32_t n, uint32_t numCells, DynSet d, StatSet s,
-                            const uint2* cells, const float2* acc, const float* alpha,
-                            cudaStream_t st);
+                            const uint32_t* src, const uint2* cells, const float2* acc,
+                            const float* alpha, cudaStream_t st);
 // table/spec: the batch's specimen table and slot -> specimen map, or null
 // for a single scene (then P).
 cudaError_t adj_backward_step(const KParams& P, const KParams* table, const uint32_t* spec,
