@@ -158,8 +158,10 @@ int dem_integrate_system(const DemSystem* sys, float* pos, float* vel, const flo
 
 /* ---------------------------------------------------------------------------
  * Context API: the whole step (SimLooping's inner loop, main.cu:396-507)
- * on library-owned device buffers, with the five stages fused into four
- * kernels and graph-captured.
+ * on library-owned device buffers: a sort phase (incremental stable sort,
+ * cell ranges, positions and radii moved to sorted order) and one step
+ * kernel (collide, integrate, next hash, gathering the other fields into
+ * sorted order), both replayed as CUDA graphs.
  * ------------------------------------------------------------------------- */
 typedef struct DemContext DemContext;
 
@@ -263,9 +265,11 @@ int dem_get_followed(DemContext* ctx, const uint32_t* ids, uint32_t count, float
  * dem_profile_begin(ctx, maxSteps) the next dem_step calls (up to maxSteps
  * steps in total) record CUDA events around the two launches;
  * dem_profile_end synchronises and returns the summed milliseconds
- *   ms[0] = sort phase (sort + reorder of the state into sorted order),
- *   ms[1] = 0 (the reorder is part of the sort phase),
- *   ms[2] = collide + integrate + next hash
+ *   ms[0] = sort phase (sort, cell ranges, positions and radii moved into
+ *           sorted order),
+ *   ms[1] = 0 (the reorder is split between the two phases),
+ *   ms[2] = collide + integrate + next hash, with the gather of the other
+ *           fields into sorted order
  * and the number of steps profiled. */
 #define DEM_NUM_STAGES 3
 int dem_profile_begin(DemContext* ctx, uint32_t maxSteps);
