@@ -41,16 +41,22 @@ sys.path.insert(0, ROOT)
 METRIC = "particle-steps/s at 4M disks"
 UNIT = "particle-steps/s"
 N_DEFAULT = 4194304
-# Algorithmic bytes of the step kernel, which does the collide and integrate
-# stages of the reference step, counted per stage as the reference moves them:
-# collide reads own pos/vel/omega/radius/mass 28 and writes force 8 + torque 4
-# (neighbours are cache hits) = 40 per particle + 8 per cell (cell ranges);
-# integrate reads pos, vel, omega, theta, radius, mass, acc, alpha 44 and writes
-# pos, vel, omega, theta 24 = 68 per particle.  The fused kernel keeps force and
-# torque in registers, so its own minimum is 68 per particle (reported beside).
-STEP_KERNEL_BYTES_PER_PARTICLE = 108
+# Algorithmic bytes of the step kernel, counted per stage of the reference step
+# as the reference moves them, for the stages (or parts of them) it does:
+#   collide: reads own pos/vel/omega/radius/mass 28, writes force 8 + torque 4
+#     (neighbours are cache hits) = 40 per particle + 8 per cell (cell ranges);
+#   integrate: reads pos, vel, omega, theta, radius, mass, acc, alpha 44, writes
+#     pos, vel, omega, theta 24 = 68 per particle;
+#   the gather half of the reorder (84 per particle in all): the step kernel
+#     reads vel, theta, omega, mass, id at each particle's previous slot 24 and
+#     writes them in sorted order 24, with loc 4 = 52; the sort phase moves the
+#     positions and radii and writes the keys and slots (the other 32).
+# The fused kernel keeps force, torque and the sorted fields in registers, so
+# its own minimum is 88 per particle (reads 44, writes 44; reported beside).
+STEP_KERNEL_STAGE_BYTES = {"collide": 40, "integrate": 68, "reorder_gather": 52}
+STEP_KERNEL_BYTES_PER_PARTICLE = sum(STEP_KERNEL_STAGE_BYTES.values())
 STEP_KERNEL_BYTES_PER_CELL = 8
-FUSED_MIN_BYTES_PER_PARTICLE = 68
+FUSED_MIN_BYTES_PER_PARTICLE = 88
 # Whole step, per particle: hash 16 + sort 52 + reorder 84 + collide 40 +
 # integrate 68 = 260, plus 20 per cell (reorder 12, collide 8).
 WHOLE_STEP_BYTES = lambda n, c: 260.0 * n + 20.0 * c  # whole-step model, per step
@@ -550,12 +556,13 @@ def main():
     cells = sc.sys.num_cells
     if dom == 2:
         bytes_launch = STEP_KERNEL_BYTES_PER_PARTICLE * n + STEP_KERNEL_BYTES_PER_CELL * cells
-        kname = "step_kernel (collide + integrate + next hash)"
+        kname = "step_kernel (collide + integrate + next hash + gather into sorted order)"
     else:
-        # counted as the reorder alone (gather 36 B, write 36 B, key+index 8 B,
-        # loc 4 B per particle, 12 B per cell); the sort work is not counted
-        bytes_launch = 84 * n + 12 * cells
-        kname = "sort phase (incremental sort + state reorder)"
+        # counted as its share of the reorder alone (positions and radii 12 B
+        # in and out, key and slot 8 B per particle, 12 B per cell); the sort
+        # work is not counted
+        bytes_launch = 32 * n + 12 * cells
+        kname = "sort phase (incremental sort + positions and radii into sorted order)"
     achieved = bytes_launch / (stage_ms[dom] * 1e-3) / 1e9
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.txt")
@@ -647,6 +654,8 @@ def main():
                              "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                              "peak_kind": kind, "traffic": traffic,
                              "bytes_per_launch": bytes_launch,
+                             "stage_bytes_per_particle": (STEP_KERNEL_STAGE_BYTES if dom == 2
+                                                          else {"reorder_move": 32}),
                              "fused_minimum_frac": (FUSED_MIN_BYTES_PER_PARTICLE * n
                                                     / (stage_ms[dom] * 1e-3) / 1e9 / hbm
                                                     if dom == 2 else None)},
