@@ -254,9 +254,12 @@ __device__ __forceinline__ void collide_one(const KParams& P, uint32_t i, int2 g
 // Row-interval form of collide_one for the context step (no attraction, no
 // x-wrap among the visited columns).  The cells (cx-1, cx, cx+1) of one row
 // are consecutive cells, so their particles form one contiguous index
-// interval in sorted order.  A lane walks its (culled) row intervals as one
-// flat loop, so the lanes of a warp run about as many iterations as their
-// own candidates instead of the per-cell maximum over the warp.
+// interval in sorted order, read from the first-particle array (cellFirst).
+// A lane walks the interval of each row it visits after culling, one row
+// after the other, so the lanes of a warp run about as many iterations as
+// their own candidates in that row instead of the per-cell maximum.
+// Positions and radii are in sorted order; a contact's velocity, spin and
+// type are read at the neighbour's slot of the previous order, src[j].
 //
 // Each interval is walked twice, in chunks of 32 candidates: a lean filter
 // sets one bit per candidate whose squared distance is within
