@@ -591,6 +591,12 @@ def main():
         out_host = {k: torch.empty_like(v).pin_memory() for k, v in host.items()}
         follow = np.array([n // 3, (2 * n) // 3], dtype=np.uint32)
         rows = np.zeros(12 * follow.size, np.float32)
+        # each step's rows go to one of two pinned buffers while the next step
+        # is queued (dem_get_followed_async); the host reads a step's rows
+        # once the event recorded after its copy has passed
+        pinned = [torch.zeros(12 * follow.size, dtype=torch.float32).pin_memory()
+                  for _ in range(2)]
+        done = [torch.cuda.Event() for _ in range(2)]
         L = D.load()
         sim2.set_state(host["pos"], host["vel"], host["theta"], host["omega"], host["radius"],
                        host["mass"], host["id"])
@@ -600,10 +606,16 @@ def main():
         t0 = time.perf_counter()
         sim2.set_state(host["pos"], host["vel"], host["theta"], host["omega"], host["radius"],
                        host["mass"], host["id"])
-        for _ in range(args.steps):
+        for k in range(args.steps):
             sim2.step(1)
-            D.check(L.dem_get_followed(sim2.handle, follow.ctypes.data, follow.size,
-                                       rows.ctypes.data, D._stream()))
+            D.check(L.dem_get_followed_async(sim2.handle, follow.ctypes.data, follow.size,
+                                             pinned[k & 1].data_ptr(), D._stream()))
+            done[k & 1].record(stream)
+            if k:
+                done[(k - 1) & 1].synchronize()
+                rows[:] = pinned[(k - 1) & 1].numpy()
+        done[(args.steps - 1) & 1].synchronize()
+        rows[:] = pinned[(args.steps - 1) & 1].numpy()
         p = lambda k: out_host[k].data_ptr()
         D.check(L.dem_get_state(sim2.handle, p("pos"), p("vel"), p("theta"), p("omega"),
                                 p("radius"), p("mass"), p("id"), None, None, None, None, None, 1,

@@ -324,6 +324,20 @@ class Simulation:
                                           _stream(stream)))
         return rows
 
+    def followed_async(self, ids, rows, stream=None) -> None:
+        """dem_get_followed_async: enqueues the rows of `ids` into `rows`, an
+        (n, 12) float32 tensor in pinned host memory (or on the GPU), and
+        returns without waiting.  Synchronise `stream`, or an event recorded
+        on it after this call, before reading `rows`."""
+        import numpy as np
+        import torch
+        ids = np.ascontiguousarray(ids, dtype=np.uint32)
+        if rows.dtype != torch.float32 or not rows.is_contiguous() or rows.numel() < 12 * ids.size:
+            raise ValueError("rows must be a contiguous float32 tensor of 12 * len(ids) values")
+        if ids.size:
+            check(load().dem_get_followed_async(self._h, ids.ctypes.data, ids.size,
+                                                rows.data_ptr(), _stream(stream)))
+
     # -- adjoint (dem_adj_forward / dem_adj_backward) ------------------------
     def adjoint_forward(self, nsteps: int, every: int, stream=None) -> None:
         """`nsteps` steps as ``step``, keeping a checkpoint every `every` steps

@@ -1121,8 +1121,9 @@ extern "C" int dem_kernels_per_step(DemContext* c) {
     return c->launchesPerStep;
 }
 
-extern "C" int dem_get_followed(DemContext* c, const uint32_t* ids, uint32_t count, float* rows,
-                                void* stream) {
+namespace {
+int get_followed(DemContext* c, const uint32_t* ids, uint32_t count, float* rows, void* stream,
+                 bool sync) {
     if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
     if (count == 0) return DEM_OK;
     if (!ids || !rows) return fail(DEM_ERR_INVALID_ARG, "dem_get_followed: NULL buffer");
@@ -1145,11 +1146,24 @@ extern "C" int dem_get_followed(DemContext* c, const uint32_t* ids, uint32_t cou
                                      c->followRows, st),
                      "followed gather");
         DEM_TRY_CUDA(cudaMemcpyAsync(rows + 12ull * base, c->followRows,
-                                     sizeof(float) * 12 * f.count, cudaMemcpyDeviceToHost, st),
+                                     sizeof(float) * 12 * f.count, cudaMemcpyDefault, st),
                      "followed copy");
-        DEM_TRY_CUDA(cudaStreamSynchronize(st), "followed sync");
+        // the staging buffer is reused by the next batch of ids
+        if (sync || base + kFollowBatch < count)
+            DEM_TRY_CUDA(cudaStreamSynchronize(st), "followed sync");
     }
     return DEM_OK;
+}
+}  // namespace
+
+extern "C" int dem_get_followed(DemContext* c, const uint32_t* ids, uint32_t count, float* rows,
+                                void* stream) {
+    return get_followed(c, ids, count, rows, stream, true);
+}
+
+extern "C" int dem_get_followed_async(DemContext* c, const uint32_t* ids, uint32_t count,
+                                      float* rows, void* stream) {
+    return get_followed(c, ids, count, rows, stream, false);
 }
 
 namespace {

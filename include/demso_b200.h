@@ -258,6 +258,16 @@ int dem_kernels_per_step(DemContext* ctx);
  * DEM_CTX_* flags (zeros otherwise).  Synchronises `stream`. */
 int dem_get_followed(DemContext* ctx, const uint32_t* ids, uint32_t count, float* rows,
                      void* stream);
+/* dem_get_followed without the wait: the gather and the copy are enqueued on
+ * `stream` and the call returns, so the next dem_step can be queued while the
+ * rows travel.  `rows` (host memory, pinned for the copy to overlap, or device
+ * memory) must stay valid until `stream` has passed the copy; the caller
+ * waits for it (an event or a stream synchronisation) before reading them.
+ * The context's staging buffer is reused in stream order, so successive calls
+ * belong on one stream.  More than 64 ids still wait between batches.  No
+ * counterpart in the reference, whose per-step output is synchronous. */
+int dem_get_followed_async(DemContext* ctx, const uint32_t* ids, uint32_t count, float* rows,
+                           void* stream);
 
 /* Stage timing inside dem_step.  Each step is two graph launches on the
  * caller's stream: the sort phase (incremental sort, or the full radix sort

@@ -118,3 +118,33 @@ def test_runner_writes_the_reference_csv(tmp_path):
     assert names == ["frame_0000000.ppm", "frame_0000030.ppm", "frame_0000060.ppm"]
     head = open(frames / names[-1], "rb").read(32)
     assert head.startswith(b"P6\n720 480\n255\n")
+
+
+def test_async_followed_rows_equal_the_synchronous_ones():
+    """dem_get_followed_async, pipelined one step ahead into two pinned
+    buffers (more than one batch of 64 ids), gives every step's rows bit for
+    bit as dem_get_followed does on a second context stepping the same
+    scene."""
+    import torch
+    sc = scenes.agitated_gas(n=3000, seed=21)
+    a, b = _sim(sc, 0), _sim(sc, 0)
+    ids = np.arange(0, 3000, 19, dtype=np.uint32)  # 158 ids: three batches
+    stream = torch.cuda.current_stream()
+    bufs = [torch.zeros((ids.size, 12), dtype=torch.float32).pin_memory() for _ in range(2)]
+    events = [torch.cuda.Event() for _ in range(2)]
+    got, want = [], []
+    for k in range(12):
+        a.step(1)
+        a.followed_async(ids, bufs[k & 1])
+        events[k & 1].record(stream)
+        if k:
+            events[(k - 1) & 1].synchronize()
+            got.append(bufs[(k - 1) & 1].numpy().copy())
+        b.step(1)
+        want.append(b.followed(ids))
+    events[11 & 1].synchronize()
+    got.append(bufs[11 & 1].numpy().copy())
+    a.close()
+    b.close()
+    for k in range(12):
+        assert same(got[k], want[k]), k
