@@ -55,6 +55,26 @@ struct StepRec {
     uint2* cells;
 };
 
+template <typename T>
+__device__ __forceinline__ T* bump(T* p, size_t off) {
+    return reinterpret_cast<T*>(reinterpret_cast<char*>(p) + off);
+}
+// The record `at` names (see RecSlot), from the one at the window's base.
+__device__ __forceinline__ StepRec rec_at(StepRec r, RecSlot at) {
+    if (!at.slot) return r;
+    const size_t off = at.stride * (size_t)(*at.slot + at.add);
+    r.pos = bump(r.pos, off);
+    r.vel = bump(r.vel, off);
+    r.omega = bump(r.omega, off);
+    r.radius = bump(r.radius, off);
+    r.mass = bump(r.mass, off);
+    r.id = bump(r.id, off);
+    r.acc = bump(r.acc, off);
+    r.alpha = bump(r.alpha, off);
+    r.cells = bump(r.cells, off);
+    return r;
+}
+
 // Adds a thread's coefficient cotangents to the per-slot accumulators
 // acc[k * n + slot]: the values of a warp are reduced over runs of equal
 // `seg` (slots of one specimen are contiguous) in a fixed pattern, and the
@@ -82,7 +102,7 @@ __device__ __forceinline__ void warp_add_coef(const double (&v)[kCoef], uint32_t
 // Reverse of integrate_one (particles_kernel.cuh:580-627) for one particle.
 __global__ void __launch_bounds__(kAdjThreads)
 adj_integrate_kernel(KParams P0, const KParams* __restrict__ table,
-                     const uint32_t* __restrict__ spec, StepRec rec, uint32_t n,
+                     const uint32_t* __restrict__ spec, StepRec rec0, RecSlot at, uint32_t n,
                      const float2* __restrict__ lamXin, const float2* __restrict__ lamVin,
                      const float* __restrict__ lamWin, float2* __restrict__ lx,
                      float2* __restrict__ lv, float* __restrict__ lw, float2* __restrict__ lamF,
@@ -91,6 +111,7 @@ adj_integrate_kernel(KParams P0, const KParams* __restrict__ table,
     double coef[kCoef] = {0, 0, 0, 0, 0, 0, 0};
     const uint32_t seg = i < n ? (table ? spec[i] : 0u) : 0xffffffffu;
     if (i < n) {
+        const StepRec rec = rec_at(rec0, at);
         const KParams& P = table ? table[seg] : P0;
         const uint32_t id = rec.id[i];
         const float r = rec.radius[i], m = rec.mass[i];
@@ -153,16 +174,22 @@ adj_integrate_kernel(KParams P0, const KParams* __restrict__ table,
 }
 
 // Contacts of particle i in recorded step `rec`: adds the state cotangents
-// of i and, once per pair (i < j), the coefficient cotangents.
+// of i to those of the integrate VJP (lx, lv, lw, sorted order) and writes
+// the sums back to id order (lamX, lamV, lamW: nothing else reads or writes
+// them while this kernel runs); once per pair (i < j), the coefficient
+// cotangents.
 __global__ void __launch_bounds__(kAdjThreads)
 adj_pairs_kernel(KParams P0, const KParams* __restrict__ table, const uint32_t* __restrict__ spec,
-                 StepRec rec, uint32_t n, const float2* __restrict__ lamF,
-                 const float* __restrict__ lamM, float2* __restrict__ lx,
-                 float2* __restrict__ lv, float* __restrict__ lw, double* __restrict__ acc) {
+                 StepRec rec0, RecSlot at, uint32_t n, const float2* __restrict__ lamF,
+                 const float* __restrict__ lamM, const float2* __restrict__ lx,
+                 const float2* __restrict__ lv, const float* __restrict__ lw,
+                 float2* __restrict__ lamX, float2* __restrict__ lamV, float* __restrict__ lamW,
+                 double* __restrict__ acc) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double coef[kCoef] = {0, 0, 0, 0, 0, 0, 0};
     const uint32_t seg = i < n ? (table ? spec[i] : 0u) : 0xffffffffu;
     if (i < n) {
+        const StepRec rec = rec_at(rec0, at);
         const KParams& P = table ? table[seg] : P0;
         const float2 p = rec.pos[i], v = rec.vel[i];
         const float w = rec.omega[i], r = rec.radius[i];
@@ -218,25 +245,13 @@ adj_pairs_kernel(KParams P0, const KParams* __restrict__ table, const uint32_t* 
                 }
             }
         }
-        float2 l = lx[i];
-        lx[i] = make_float2(l.x + gx, l.y + gy);
-        float2 u = lv[i];
-        lv[i] = make_float2(u.x + gvx, u.y + gvy);
-        lw[i] += gw;
+        const uint32_t k = rec.id[i];
+        const float2 l = lx[i], u = lv[i];
+        lamX[k] = make_float2(l.x + gx, l.y + gy);
+        lamV[k] = make_float2(u.x + gvx, u.y + gvy);
+        lamW[k] = lw[i] + gw;
     }
     warp_add_coef(coef, seg, i, n, acc);
-}
-
-__global__ void adj_scatter_kernel(const uint32_t* __restrict__ id, uint32_t n,
-                                   const float2* __restrict__ lx, const float2* __restrict__ lv,
-                                   const float* __restrict__ lw, float2* __restrict__ lamX,
-                                   float2* __restrict__ lamV, float* __restrict__ lamW) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t k = id[i];
-    lamX[k] = lx[i];
-    lamV[k] = lv[i];
-    lamW[k] = lw[i];
 }
 
 // Per specimen s: the sum of acc[k * n + slot] over its slots
@@ -290,10 +305,11 @@ StepRec carve_step(void* base, uint32_t n, uint32_t numCells) {
 
 namespace {
 __global__ void __launch_bounds__(kAdjThreads)
-adj_record_kernel(StepRec r, DynSet d, StatSet s, const uint32_t* __restrict__ src,
+adj_record_kernel(StepRec r0, RecSlot at, DynSet d, StatSet s, const uint32_t* __restrict__ src,
                   const uint2* __restrict__ cells,
                   const float2* __restrict__ acc, const float* __restrict__ alpha, uint32_t n,
                   uint32_t numCells) {
+    const StepRec r = rec_at(r0, at);
     const uint32_t m = n > numCells ? n : numCells;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
         if (i < n) {
@@ -312,27 +328,26 @@ adj_record_kernel(StepRec r, DynSet d, StatSet s, const uint32_t* __restrict__ s
 }
 }  // namespace
 
-cudaError_t adj_record_step(void* recBase, uint32_t n, uint32_t numCells, DynSet d, StatSet s,
-                            const uint32_t* src, const uint2* cells, const float2* acc,
+cudaError_t adj_record_step(void* recBase, RecSlot at, uint32_t n, uint32_t numCells, DynSet d,
+                            StatSet s, const uint32_t* src, const uint2* cells, const float2* acc,
                             const float* alpha, cudaStream_t st) {
     const uint32_t m = n > numCells ? n : numCells;
     const unsigned b = std::min<unsigned>(blocks_for(m, kAdjThreads), 148u * 16u);
-    adj_record_kernel<<<b, kAdjThreads, 0, st>>>(carve_step(recBase, n, numCells), d, s, src,
+    adj_record_kernel<<<b, kAdjThreads, 0, st>>>(carve_step(recBase, n, numCells), at, d, s, src,
                                                  cells, acc, alpha, n, numCells);
     return cudaGetLastError();
 }
 
 cudaError_t adj_backward_step(const KParams& P, const KParams* table, const uint32_t* spec,
-                              void* recBase, uint32_t n, uint32_t numCells, float2* lamX,
-                              float2* lamV, float* lamW, float2* tlx, float2* tlv, float* tlw,
-                              float2* lamF, float* lamM, double* acc, cudaStream_t st) {
+                              void* recBase, RecSlot at, uint32_t n, uint32_t numCells,
+                              float2* lamX, float2* lamV, float* lamW, float2* tlx, float2* tlv,
+                              float* tlw, float2* lamF, float* lamM, double* acc, cudaStream_t st) {
     const StepRec rec = carve_step(recBase, n, numCells);
     const unsigned b = blocks_for(n, kAdjThreads);
-    adj_integrate_kernel<<<b, kAdjThreads, 0, st>>>(P, table, spec, rec, n, lamX, lamV, lamW, tlx,
-                                                    tlv, tlw, lamF, lamM, acc);
-    adj_pairs_kernel<<<b, kAdjThreads, 0, st>>>(P, table, spec, rec, n, lamF, lamM, tlx, tlv, tlw,
-                                                acc);
-    adj_scatter_kernel<<<b, kAdjThreads, 0, st>>>(rec.id, n, tlx, tlv, tlw, lamX, lamV, lamW);
+    adj_integrate_kernel<<<b, kAdjThreads, 0, st>>>(P, table, spec, rec, at, n, lamX, lamV, lamW,
+                                                    tlx, tlv, tlw, lamF, lamM, acc);
+    adj_pairs_kernel<<<b, kAdjThreads, 0, st>>>(P, table, spec, rec, at, n, lamF, lamM, tlx, tlv,
+                                                tlw, lamX, lamV, lamW, acc);
     return cudaGetLastError();
 }
 

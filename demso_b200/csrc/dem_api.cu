@@ -326,6 +326,15 @@ struct DemContext {
     // capture-time fork of the sort phase: the full path's branch
     cudaStream_t forkStream = nullptr;
     cudaEvent_t forkEv = nullptr, joinEv = nullptr;
+    // The device-side step loop of multi-step dem_step calls: loopGraph[p]
+    // runs pairs of incremental steps from parity p in a WHILE node while the
+    // count in loopCtl[1] (copied from loopCtl[0], written before each launch)
+    // is non-zero; its body is captured on loopStream.
+    cudaGraphExec_t loopGraph[2] = {};
+    uint32_t* loopCtl = nullptr;
+    uint32_t loopPairs = 0;
+    uint32_t adjLoopHost[6] = {};  // a backward window's words loopCtl[kLoopRecReq..]
+    cudaStream_t loopStream = nullptr;
     // Each step is two graph launches: the sort phase sortGraph[kind][parity]
     // (kind 0 = full radix sort, 1 = incremental sort with the full sort as a
     // device-chosen fallback), then the step kernel stepGraph[parity].
@@ -372,8 +381,16 @@ void drop_tune_graphs(DemContext* c) {
         }
 }
 
+void drop_loop_graphs(DemContext* c) {
+    for (int p = 0; p < 2; ++p) {
+        if (c->loopGraph[p]) cudaGraphExecDestroy(c->loopGraph[p]);
+        c->loopGraph[p] = nullptr;
+    }
+}
+
 void drop_graphs(DemContext* c) {
     drop_tune_graphs(c);
+    drop_loop_graphs(c);
     // a tuning interrupted by a change of the step starts again
     if (c->tuned < 0) c->tuneStep = 0;
     for (int k = 0; k < 2; ++k)
@@ -424,10 +441,12 @@ cudaError_t enqueue_inc_sort(DemContext* c, int a, cudaStream_t st, int* launche
     return e == cudaSuccess ? enqueue_inc_tail(c, a, st, launches) : e;
 }
 
-// Adds an IF node on `h` at the current capture point of `st` and captures
-// `body` into it on c->bodyStream.
+// Adds a conditional node of `type` on `h` at the current capture point of
+// `st` and captures `body` into it on `bodyStream`.
 template <typename Body>
-cudaError_t add_if(DemContext* c, cudaStream_t st, cudaGraphConditionalHandle h, Body body) {
+cudaError_t add_conditional(cudaStream_t st, cudaGraphConditionalHandle h,
+                            cudaGraphConditionalNodeType type, cudaStream_t bodyStream,
+                            Body body) {
     cudaStreamCaptureStatus status;
     cudaGraph_t g = nullptr;
     const cudaGraphNode_t* deps = nullptr;
@@ -437,7 +456,7 @@ cudaError_t add_if(DemContext* c, cudaStream_t st, cudaGraphConditionalHandle h,
     cudaGraphNodeParams prm = {};
     prm.type = cudaGraphNodeTypeConditional;
     prm.conditional.handle = h;
-    prm.conditional.type = cudaGraphCondTypeIf;
+    prm.conditional.type = type;
     prm.conditional.size = 1;
     cudaGraphNode_t node;
     e = cudaGraphAddNode(&node, g, deps, nd, &prm);
@@ -445,12 +464,17 @@ cudaError_t add_if(DemContext* c, cudaStream_t st, cudaGraphConditionalHandle h,
     e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
     if (e != cudaSuccess) return e;
     cudaGraph_t bodyGraph = prm.conditional.phGraph_out[0];
-    e = cudaStreamBeginCaptureToGraph(c->bodyStream, bodyGraph, nullptr, nullptr, 0,
+    e = cudaStreamBeginCaptureToGraph(bodyStream, bodyGraph, nullptr, nullptr, 0,
                                       cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return e;
-    cudaError_t eb = body(c->bodyStream);
-    e = cudaStreamEndCapture(c->bodyStream, &bodyGraph);
+    cudaError_t eb = body(bodyStream);
+    e = cudaStreamEndCapture(bodyStream, &bodyGraph);
     return eb != cudaSuccess ? eb : e;
+}
+
+template <typename Body>
+cudaError_t add_if(DemContext* c, cudaStream_t st, cudaGraphConditionalHandle h, Body body) {
+    return add_conditional(st, h, cudaGraphCondTypeIf, c->bodyStream, body);
 }
 
 // Sort phase of one step: the state (dyn[0], stat[cur]) is sorted into
@@ -549,6 +573,78 @@ int build_graph(DemContext* c, int what, int parity) {
     return DEM_OK;
 }
 
+// Device-side loop control words (loopCtl, written by the host before each
+// launch of a loop graph): the requested count, the count left, the slot.
+enum : uint32_t {
+    kLoopStepReq = 0, kLoopStepLeft = 1,                    // dem_step's step pairs
+    kLoopRecReq = 2, kLoopRecLeft = 3, kLoopRecSlot = 4,    // adjoint recompute pairs
+    kLoopRevReq = 5, kLoopRevLeft = 6, kLoopRevSlot = 7,    // adjoint reversed steps
+};
+
+// A graph of one device-side loop: an init kernel that copies loopCtl[req]
+// to loopCtl[req + 1] and sets the condition, then a WHILE node whose body
+// is `body` (captured on loopStream) followed by the kernel that counts one
+// iteration down and adds idxStep to loopCtl[idx] (idx < 0: none).
+template <typename Body>
+int build_while_graph(DemContext* c, uint32_t req, int idx, int32_t idxStep, Body body,
+                      cudaGraphExec_t* out) {
+    const int saved = c->cur;
+    DEM_TRY_CUDA(cudaStreamBeginCapture(c->capStream, cudaStreamCaptureModeThreadLocal),
+                 "begin capture");
+    cudaStreamCaptureStatus status;
+    cudaGraph_t cg = nullptr;
+    cudaGraphConditionalHandle h = 0;
+    uint32_t* left = c->loopCtl + req + 1;
+    uint32_t* slot = idx < 0 ? nullptr : c->loopCtl + idx;
+    cudaError_t e = cudaStreamGetCaptureInfo(c->capStream, &status, nullptr, &cg, nullptr, nullptr);
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, cg, 0, 0);
+    if (e == cudaSuccess) e = launch_loop_init(c->loopCtl + req, left, h, c->capStream);
+    if (e == cudaSuccess)
+        e = add_conditional(c->capStream, h, cudaGraphCondTypeWhile, c->loopStream,
+                            [&](cudaStream_t bs) {
+                                cudaError_t eb = body(bs);
+                                if (eb == cudaSuccess) eb = launch_loop_next(left, slot, idxStep, h, bs);
+                                return eb;
+                            });
+    c->cur = saved;
+    cudaGraph_t g = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(c->capStream, &g);
+    if (e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return cuda_fail(e, "loop capture");
+    }
+    if (e2 != cudaSuccess) return cuda_fail(e2, "end capture");
+    e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "loop instantiate");
+    return DEM_OK;
+}
+
+// Two incremental steps from parity p (p, then p ^ 1: the sort phase and the
+// step kernel as in sortGraph[1] and stepGraph) into `bs`; after each, when
+// `rec` is set, its record at slot loopCtl[kLoopRecSlot] + k.
+cudaError_t enqueue_step_pair(DemContext* c, int p, cudaStream_t bs, void* rec, size_t stride) {
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+        c->cur = p ^ k;
+        e = enqueue_sort_phase(c, 1, bs, nullptr);
+        if (e == cudaSuccess) e = enqueue_step_kernel(c, bs, nullptr);
+        if (e == cudaSuccess && rec)
+            e = adj_record_step(rec, RecSlot{c->loopCtl + kLoopRecSlot, (uint32_t)k, stride}, c->n,
+                                c->numCells, step_in(c, p ^ k), step_in_static(c, p ^ k), c->src,
+                                c->cells[p ^ k ^ 1], c->acc, c->alpha, bs);
+    }
+    return e;
+}
+
+// dem_step's loop from parity p: pairs of steps while loopCtl[kLoopStepLeft].
+int build_loop_graph(DemContext* c, int p) {
+    return build_while_graph(
+        c, kLoopStepReq, -1, 0,
+        [&](cudaStream_t bs) { return enqueue_step_pair(c, p, bs, nullptr, 0); },
+        &c->loopGraph[p]);
+}
+
 void drop_tune_events(DemContext* c) {
     if (!c->tuneEv) return;
     for (uint32_t i = 0; i < 2 * kTuneSteps; ++i)
@@ -605,6 +701,7 @@ int tune_finish(DemContext* c, bool graphs) {
         }
     drop_tune_graphs(c);
     drop_tune_events(c);
+    drop_loop_graphs(c);  // they hold the step kernel of the old shape
     return DEM_OK;
 }
 
@@ -734,6 +831,7 @@ int init_context(DemContext* c, uint32_t capacity, uint32_t numCells, DemContext
     total += 2 * cells8 + 2 * first4;            // cell ranges and first particles x2
     total += f4 + f8 + f4;                       // pressure, acc, alpha
     total += 256;                                // error flag
+    total += 256;                                // step-loop counters
     const size_t sortBytes = onesweep_scratch_bytes(capacity, c->keyBits);
     const size_t incBytes = incsort_bytes(capacity, c->numCells, nullptr);
     cudaError_t e = cudaMalloc(&c->block, total);
@@ -771,6 +869,7 @@ int init_context(DemContext* c, uint32_t capacity, uint32_t numCells, DemContext
     c->acc = reinterpret_cast<float2*>(take(f8));
     c->alpha = reinterpret_cast<float*>(take(f4));
     c->errFlag = reinterpret_cast<uint32_t*>(take(256));
+    c->loopCtl = reinterpret_cast<uint32_t*>(take(256));
     c->ss = carve_onesweep_scratch(c->sortScratch, capacity, c->keyBits);
     c->inc = carve_incsort(c->incScratch, capacity, c->numCells);
     e = cudaMemset(c->block, 0, total);
@@ -780,11 +879,13 @@ int init_context(DemContext* c, uint32_t capacity, uint32_t numCells, DemContext
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->capStream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->bodyStream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->forkStream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->loopStream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->forkEv, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->joinEv, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         if (c->joinEv) cudaEventDestroy(c->joinEv);
         if (c->forkEv) cudaEventDestroy(c->forkEv);
+        if (c->loopStream) cudaStreamDestroy(c->loopStream);
         if (c->forkStream) cudaStreamDestroy(c->forkStream);
         if (c->bodyStream) cudaStreamDestroy(c->bodyStream);
         if (c->capStream) cudaStreamDestroy(c->capStream);
@@ -806,6 +907,7 @@ extern "C" int dem_destroy(DemContext* c) {
     if (c->capStream) cudaStreamDestroy(c->capStream);
     if (c->bodyStream) cudaStreamDestroy(c->bodyStream);
     if (c->forkStream) cudaStreamDestroy(c->forkStream);
+    if (c->loopStream) cudaStreamDestroy(c->loopStream);
     if (c->forkEv) cudaEventDestroy(c->forkEv);
     if (c->joinEv) cudaEventDestroy(c->joinEv);
     cudaFree(c->followRows);
@@ -1030,6 +1132,25 @@ extern "C" int dem_step(DemContext* c, uint32_t nsteps, void* stream) {
         }
     }
     for (uint32_t s = 0; s < nsteps; ++s) {
+        // Pairs of steps run inside the device-side loop, one graph launch for
+        // all of them, unless the host has work between steps (stage
+        // profiling, the tuner) or there is no previous order yet (the first
+        // sort is a full sort).
+        if (!c->profiling && c->tuned >= 0 && c->haveOrder && nsteps - s >= 2) {
+            const uint32_t pairs = (nsteps - s) / 2;
+            const int p = c->cur;
+            if (!c->loopGraph[p]) {
+                int rc = build_loop_graph(c, p);
+                if (rc) return rc;
+            }
+            c->loopPairs = pairs;
+            DEM_TRY_CUDA(cudaMemcpyAsync(c->loopCtl + kLoopStepReq, &c->loopPairs, 4,
+                                         cudaMemcpyHostToDevice, st),
+                         "step loop count");
+            DEM_TRY_CUDA(cudaGraphLaunch(c->loopGraph[p], st), "graph launch");
+            s += 2 * pairs - 1;  // an even number of steps leaves the parity as it was
+            continue;
+        }
         const int p = c->cur;
         const int kind = c->haveOrder ? 1 : 0;
         const bool prof = c->profiling && c->evUsed + 3 <= c->evCap;
@@ -1077,6 +1198,7 @@ extern "C" int dem_set_step_variant(DemContext* c, int32_t variant) {
             if (c->stepGraph[p]) cudaGraphExecDestroy(c->stepGraph[p]);
             c->stepGraph[p] = nullptr;
         }
+        drop_loop_graphs(c);
     }
     return DEM_OK;
 }
@@ -1378,7 +1500,8 @@ int step_recorded(DemContext* c, cudaStream_t st, char* rec) {
     // the step kernel leaves the sorted state it read intact: record it, the
     // cell ranges and the accelerations in one launch
     if (rec)
-        DEM_TRY_CUDA(adj_record_step(rec, c->n, c->numCells, step_in(c, p), step_in_static(c, p),
+        DEM_TRY_CUDA(adj_record_step(rec, RecSlot{}, c->n, c->numCells, step_in(c, p),
+                                     step_in_static(c, p),
                                      c->src, c->cells[b],
                                      c->acc, c->alpha, st),
                      "record");
@@ -1475,6 +1598,7 @@ extern "C" int dem_adj_backward(DemContext* c, float* lamPos, float* lamVel, flo
     if (e == cudaSuccess && first)
         e = cudaMemcpyAsync(first, c->partOff.data(), 4ull * (ns + 1), cudaMemcpyHostToDevice, st);
     const size_t snap = snapshot_bytes(n);
+    cudaGraphExec_t recLoop[2] = {}, revLoop = nullptr;
     for (int w = (int)c->adjWindows - 1; w >= 0 && rc == DEM_OK && e == cudaSuccess; --w) {
         Snapshot s = carve_snapshot(static_cast<char*>(c->adjCheck) + snap * w, n);
         rc = dem_set_state(c, n, s.pos, s.vel, s.theta, s.omega, s.radius, s.mass, s.id, nullptr,
@@ -1492,14 +1616,54 @@ extern "C" int dem_adj_backward(DemContext* c, float* lamPos, float* lamVel, flo
                 if (!c->sortGraph[kk][pp]) rc = build_graph(c, kk, pp);
             if (rc == DEM_OK && !c->stepGraph[pp]) rc = build_graph(c, 2, pp);
         }
-        for (uint32_t t = 0; t < k && rc == DEM_OK; ++t) rc = step_recorded(c, st, rec + stepBytes * t);
-        for (int t = (int)k - 1; t >= 0 && rc == DEM_OK && e == cudaSuccess; --t)
-            e = adj_backward_step(c->P, c->nspec ? c->dTable : nullptr, c->spec,
-                                  rec + stepBytes * t, n, c->numCells,
-                                  reinterpret_cast<float2*>(lamPos),
-                                  reinterpret_cast<float2*>(lamVel), lamOmega, tlx, tlv, tlw, lamF,
-                                  lamM, acc, st);
+        if (rc != DEM_OK || e != cudaSuccess) break;
+        // The window's first step sorts from scratch (host-launched, record
+        // slot 0); the rest run in pairs inside the recompute loop, each
+        // recorded at the loop's slot, and an odd last step is host-launched.
+        // The reversed steps then run in the reverse loop, slot k - 1 down
+        // to 0.  Both loops are graphs of this call (they hold its buffers).
+        rc = step_recorded(c, st, rec);
+        if (rc) break;
+        const uint32_t pairs = (k - 1) / 2;
+        const uint32_t words[6] = {pairs, 0u, 1u, k, 0u, k - 1u};
+        std::memcpy(c->adjLoopHost, words, sizeof(words));
+        e = cudaMemcpyAsync(c->loopCtl + kLoopRecReq, c->adjLoopHost, sizeof(words),
+                            cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) break;
+        if (pairs) {
+            const int p = c->cur;
+            if (!recLoop[p]) {
+                rc = build_while_graph(
+                    c, kLoopRecReq, kLoopRecSlot, 2,
+                    [&](cudaStream_t bs) { return enqueue_step_pair(c, p, bs, rec, stepBytes); },
+                    &recLoop[p]);
+                if (rc) break;
+            }
+            e = cudaGraphLaunch(recLoop[p], st);
+            if (e != cudaSuccess) break;
+        }
+        if ((k - 1) & 1) {
+            rc = step_recorded(c, st, rec + stepBytes * (k - 1));
+            if (rc) break;
+        }
+        if (!revLoop) {
+            rc = build_while_graph(
+                c, kLoopRevReq, kLoopRevSlot, -1,
+                [&](cudaStream_t bs) {
+                    return adj_backward_step(c->P, c->nspec ? c->dTable : nullptr, c->spec, rec,
+                                             RecSlot{c->loopCtl + kLoopRevSlot, 0u, stepBytes}, n,
+                                             c->numCells, reinterpret_cast<float2*>(lamPos),
+                                             reinterpret_cast<float2*>(lamVel), lamOmega, tlx,
+                                             tlv, tlw, lamF, lamM, acc, bs);
+                },
+                &revLoop);
+            if (rc) break;
+        }
+        e = cudaGraphLaunch(revLoop, st);
     }
+    // (a graph still in flight is freed when it completes)
+    for (cudaGraphExec_t g : {recLoop[0], recLoop[1], revLoop})
+        if (g) cudaGraphExecDestroy(g);
     if (rc == DEM_OK && e == cudaSuccess) e = adj_sum_coef(acc, n, first, ns, sum, st);
     if (rc == DEM_OK && e == cudaSuccess)
         e = cudaMemcpyAsync(grad, sum, 8ull * DEM_ADJ_NUM_COEF * ns, cudaMemcpyDeviceToHost, st);

@@ -884,6 +884,34 @@ StepShape step_variant_shape(int variant) {
     }
 }
 
+namespace {
+__global__ void loop_init_kernel(const uint32_t* __restrict__ req, uint32_t* __restrict__ left,
+                                 cudaGraphConditionalHandle h) {
+    const uint32_t n = *req;
+    *left = n;
+    cudaGraphSetConditional(h, n ? 1u : 0u);
+}
+__global__ void loop_next_kernel(uint32_t* __restrict__ left, uint32_t* __restrict__ idx,
+                                 int32_t idxStep, cudaGraphConditionalHandle h) {
+    const uint32_t n = *left - 1u;
+    *left = n;
+    if (idx) *idx += (uint32_t)idxStep;
+    cudaGraphSetConditional(h, n ? 1u : 0u);
+}
+}  // namespace
+
+cudaError_t launch_loop_init(const uint32_t* req, uint32_t* left, cudaGraphConditionalHandle h,
+                             cudaStream_t st) {
+    loop_init_kernel<<<1, 1, 0, st>>>(req, left, h);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_loop_next(uint32_t* left, uint32_t* idx, int32_t idxStep,
+                             cudaGraphConditionalHandle h, cudaStream_t st) {
+    loop_next_kernel<<<1, 1, 0, st>>>(left, idx, idxStep, h);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_control_post(ControlArgs ctl, ControlDev* c, uint32_t n, float* partials,
                                 float* out, cudaStream_t st, int* launches) {
     const uint32_t threads = n < (uint32_t)kControlThreads ? (n ? n : 1u) : (uint32_t)kControlThreads;

@@ -130,21 +130,40 @@ cudaError_t launch_reorder_packed(uint2* cellRange, DynSet sorted, StatSet sorte
 cudaError_t launch_unpack_cells(const uint2* cellRange, uint32_t numCells, uint32_t* cellStart,
                                 uint32_t* cellEnd, cudaStream_t st);
 
+// Device-side loops (a WHILE node of a graph): loop_init copies the
+// requested count of iterations (*req) to *left and sets the node's
+// condition; loop_next, the last kernel of each iteration, counts one down,
+// adds idxStep to *idx (when idx is not null: the loop's record slot) and
+// sets the condition again.
+cudaError_t launch_loop_init(const uint32_t* req, uint32_t* left, cudaGraphConditionalHandle h,
+                             cudaStream_t st);
+cudaError_t launch_loop_next(uint32_t* left, uint32_t* idx, int32_t idxStep,
+                             cudaGraphConditionalHandle h, cudaStream_t st);
+
 // Adjoint (dem_adjoint.cu).
 size_t adj_step_bytes(uint32_t n, uint32_t numCells);
 // Writes the record of one forward step at recBase in one launch: the sorted
 // state the step kernel stepped (d, s and src as launch_step's in, inS and
 // src), its cell ranges and the acceleration and angular acceleration it
 // produced.
-cudaError_t adj_record_step(void* recBase, uint32_t n, uint32_t numCells, DynSet d, StatSet s,
-                            const uint32_t* src, const uint2* cells, const float2* acc,
+// The record a kernel reads or writes: recBase itself, or, with `slot`
+// set, the record of step (*slot + add) of a window whose records are
+// `stride` bytes apart from recBase -- the form a device-side loop uses,
+// its slot advanced by loop_next.
+struct RecSlot {
+    const uint32_t* slot = nullptr;
+    uint32_t add = 0;
+    size_t stride = 0;
+};
+cudaError_t adj_record_step(void* recBase, RecSlot at, uint32_t n, uint32_t numCells, DynSet d,
+                            StatSet s, const uint32_t* src, const uint2* cells, const float2* acc,
                             const float* alpha, cudaStream_t st);
 // table/spec: the batch's specimen table and slot -> specimen map, or null
 // for a single scene (then P).
 cudaError_t adj_backward_step(const KParams& P, const KParams* table, const uint32_t* spec,
-                              void* recBase, uint32_t n, uint32_t numCells, float2* lamX,
-                              float2* lamV, float* lamW, float2* tlx, float2* tlv, float* tlw,
-                              float2* lamF, float* lamM, double* acc, cudaStream_t st);
+                              void* recBase, RecSlot at, uint32_t n, uint32_t numCells,
+                              float2* lamX, float2* lamV, float* lamW, float2* tlx, float2* tlv,
+                              float* tlw, float2* lamF, float* lamM, double* acc, cudaStream_t st);
 // Per-specimen coefficient gradients (first: numSpecimens + 1 slot offsets,
 // or null for one specimen of n slots).
 cudaError_t adj_sum_coef(const double* acc, uint32_t n, const uint32_t* first, uint32_t numSpecimens,

@@ -217,6 +217,14 @@ int dem_get_state(DemContext* ctx, float* pos, float* vel, float* theta, float* 
                   float* pressure, float* acc, float* alpha, int host, void* stream);
 
 /* Advances `nsteps` full steps (hash, sort, reorder, collide, integrate).
+ * Once the context holds a previous order (after its first step) and is
+ * neither tuning nor profiling, a call of two or more steps runs them in
+ * pairs inside ONE graph launch: a device-side loop (a CUDA graph WHILE
+ * node, its pair count written to the device before the launch and counted
+ * down there) whose body is two whole steps, one per buffer parity; an odd
+ * last step is one more ordinary step.  The loop runs the same kernels on
+ * the same buffers as single calls, so the bits are those of nsteps calls
+ * of one step.
  * With DEM_CTX_AUTOTUNE the context's first 24 steps run the step kernel's
  * launch shapes in turn, each timed by CUDA events on `stream`; the step
  * that completes the 24th waits for `stream` once and keeps the shape with
