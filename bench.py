@@ -10,15 +10,18 @@ With N > 1 (torchrun, one rank per GPU) every rank steps its own replica
 (seed = rank): the plain step of one box has a halo exchange that is not
 built, so this is weak scaling by replicas.
 
-`value` is whole-job particle-steps/s over K timed steps (device time, CUDA
-events, max over ranks).  `e2e` is the same workload through the C ABI with
-host buffers: the state uploaded from pinned host memory, K steps each
-followed by the reference's per-step followed-particle readback
-(writeOutputFile), and the state downloaded, all inside the timed region.
-`roofline` is for the dominant kernel, timed by events captured in the
-step's CUDA graph during the timed region.  `cpu_baseline` times the
-reference's own step functions built for the host (oracle/_ref) on a
-bounded sample of the same workload.
+`value` is whole-job particle-steps/s over K timed steps issued as one
+dem_step call (device time, CUDA events, max over ranks); the library runs
+them as one graph launch of its device-side step loop.  `e2e` is the same
+workload through the C ABI with host buffers: the state uploaded from pinned
+host memory, K steps each followed by the reference's per-step
+followed-particle readback (writeOutputFile), and the state downloaded, all
+inside the timed region.  `roofline` is for the dominant kernel, timed by
+CUDA events recorded around each stage's graph launch in a second pass of K
+steps launched one step at a time (events cannot sit inside the device-side
+loop); that pass's whole-step time is `ms_per_step_stage_timed`.
+`cpu_baseline` times the reference's own step functions built for the host
+(oracle/_ref) on a bounded sample of the same workload.
 
 `--impl reference` times only that CPU reference on the same metric.
 """
@@ -434,22 +437,27 @@ def measure_sweep(sizes, steps: int = 200, warmup: int = 50):
             sim.step(1)
         shape = sim.step_variant()
         torch.cuda.synchronize()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        e[0].record()
+        sim.step(steps)  # one call: the device-side step loop
+        e[1].record()
+        torch.cuda.synchronize()
         D.check(D.load().dem_profile_begin(sim.handle, steps))
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        sim.step(steps)
-        e1.record()
+        e[2].record()
+        sim.step(steps)  # stage timing, one step at a time
+        e[3].record()
         torch.cuda.synchronize()
         ms = (C.c_float * D._lib.NUM_STAGES)()
         k = C.c_uint32(0)
         D.check(D.load().dem_profile_end(sim.handle, ms, C.byref(k)))
         sim.check()
         sim.close()
-        step_ms = e0.elapsed_time(e1) / steps
+        step_ms = e[0].elapsed_time(e[1]) / steps
         cells = sc.sys.num_cells
         kern_ms = ms[2] / max(1, k.value)
         kb = STEP_KERNEL_BYTES_PER_PARTICLE * sc.n + STEP_KERNEL_BYTES_PER_CELL * cells
         rows.append({"n": sc.n, "grid": [sc.sys.gx, sc.sys.gy], "ms_per_step": step_ms,
+                     "ms_per_step_stage_timed": e[2].elapsed_time(e[3]) / steps,
                      "step_kernel_shape": [shape["threads"], shape["blocks_per_sm"]],
                      "value": sc.n / (step_ms * 1e-3),
                      "sort_ms": ms[0] / max(1, k.value), "step_kernel_ms": kern_ms,
@@ -527,31 +535,42 @@ def main():
     kernels_per_step = sim.kernels_per_step()
     shape = sim.step_variant()
 
-    # ---- timed region (device-resident state)
+    # ---- timed region (device-resident state): the K steps as one dem_step
+    # call, which the library runs as one graph launch of its device-side
+    # step loop
     clocks = Clocks(local)
     barrier()
     torch.cuda.synchronize()
     clocks.start()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    D.check(D.load().dem_profile_begin(sim.handle, args.steps))
-    ev0.record(stream)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev[0].record(stream)
     sim.step(args.steps)
-    ev1.record(stream)
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    # ---- stage timing: K more steps, launched one step at a time with CUDA
+    # events around each stage (events cannot sit inside the device-side
+    # loop); the roofline's kernel duration comes from this pass
+    D.check(D.load().dem_profile_begin(sim.handle, args.steps))
+    ev[2].record(stream)
+    sim.step(args.steps)
+    ev[3].record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
     import ctypes as C
     ms = (C.c_float * D._lib.NUM_STAGES)()
     nprof = C.c_uint32(0)
     D.check(D.load().dem_profile_end(sim.handle, ms, C.byref(nprof)))
-    elapsed = ev0.elapsed_time(ev1)
+    elapsed, elapsed_staged = ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3])
     barrier()
     if dist is not None:
-        t = torch.tensor([elapsed], device="cuda")
+        t = torch.tensor([elapsed, elapsed_staged], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+        elapsed, elapsed_staged = float(t[0].item()), float(t[1].item())
     sim.check()
     value = n * world * args.steps / (elapsed * 1e-3)
+    # kernels of the timed call: every step's, plus the loop's init kernel and
+    # one count-down kernel per pair of steps (none on direct launches)
+    loop_kernels = 0 if args.direct or args.steps < 2 else 1 + args.steps // 2
 
     stage_ms = [ms[i] / max(1, nprof.value) for i in range(3)]
     stage_names = ["sort_reorder", "reorder_separate", "collide_integrate"]
@@ -664,8 +683,13 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f32", "data": "synthetic", "config": dict(config_dict(n, sc), launch="direct, no graphs" if args.direct
-                               else "two CUDA graphs per step"),
+                "dtype": "f32", "data": "synthetic",
+                "config": dict(config_dict(n, sc),
+                               launch="direct, no graphs" if args.direct
+                               else "one graph launch of the device-side step loop for the "
+                                    "K steps (stage timing: a second pass of K steps, two "
+                                    "graph launches per step)"),
+                "ms_per_step_stage_timed": elapsed_staged / args.steps,
                 "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved,
                              "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                              "peak_kind": kind, "traffic": traffic,
@@ -682,7 +706,7 @@ def main():
                                "frac": whole_bytes / (step_ms * 1e-3) / 1e9 / hbm},
                 "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "batched": batched,
                 "adjoint": adjoint, "settling_pile": pile,
-                "gpu_launches": kernels_per_step * args.steps,
+                "gpu_launches": kernels_per_step * args.steps + loop_kernels,
                 "kernels_per_step": kernels_per_step,
                 "step_kernel_shape": {"threads": shape["threads"],
                                       "blocks_per_sm": shape["blocks_per_sm"],

@@ -332,8 +332,6 @@ struct DemContext {
     // is non-zero; its body is captured on loopStream.
     cudaGraphExec_t loopGraph[2] = {};
     uint32_t* loopCtl = nullptr;
-    uint32_t loopPairs = 0;
-    uint32_t adjLoopHost[6] = {};  // a backward window's words loopCtl[kLoopRecReq..]
     cudaStream_t loopStream = nullptr;
     // Each step is two graph launches: the sort phase sortGraph[kind][parity]
     // (kind 0 = full radix sort, 1 = incremental sort with the full sort as a
@@ -354,6 +352,8 @@ struct DemContext {
     void* adjCheck = nullptr;
     size_t adjCheckBytes = 0;
     uint32_t adjSteps = 0, adjEvery = 0, adjWindows = 0;
+    uint32_t adjN = 0;     // particles and largest radius of the checkpointed run
+    float adjRmax = 0.0f;  // (the backward restores checkpoints without re-deriving them)
     // the step kernel's launch shape (step_variant_shape) and its autotuner
     // (DEM_CTX_AUTOTUNE): the first kTuneSteps steps run the variants in turn,
     // each timed by a pair of events, then the one with the smallest median
@@ -1143,9 +1143,7 @@ extern "C" int dem_step(DemContext* c, uint32_t nsteps, void* stream) {
                 int rc = build_loop_graph(c, p);
                 if (rc) return rc;
             }
-            c->loopPairs = pairs;
-            DEM_TRY_CUDA(cudaMemcpyAsync(c->loopCtl + kLoopStepReq, &c->loopPairs, 4,
-                                         cudaMemcpyHostToDevice, st),
+            DEM_TRY_CUDA(launch_set_words(c->loopCtl + kLoopStepReq, Words{{pairs}, 1u}, st),
                          "step loop count");
             DEM_TRY_CUDA(cudaGraphLaunch(c->loopGraph[p], st), "graph launch");
             s += 2 * pairs - 1;  // an even number of steps leaves the parity as it was
@@ -1510,6 +1508,25 @@ int step_recorded(DemContext* c, cudaStream_t st, char* rec) {
     return DEM_OK;
 }
 
+// dem_set_state from a checkpoint of this context, without its stream
+// synchronisation and graph rebuild: a checkpoint holds the same particles,
+// so the largest radius, the kernel parameters and the graphs stay valid;
+// the next step sorts from scratch.
+int restore_checkpoint(DemContext* c, const Snapshot& s, cudaStream_t st) {
+    const int a = c->cur;
+    const size_t n = c->n;
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[0].pos, s.pos, 8 * n, cudaMemcpyDeviceToDevice, st), "restore pos");
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[a].vel, s.vel, 8 * n, cudaMemcpyDeviceToDevice, st), "restore vel");
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[a].theta, s.theta, 4 * n, cudaMemcpyDeviceToDevice, st), "restore theta");
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[a].omega, s.omega, 4 * n, cudaMemcpyDeviceToDevice, st), "restore omega");
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->stat[a].radius, s.radius, 4 * n, cudaMemcpyDeviceToDevice, st), "restore radius");
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->stat[a].mass, s.mass, 4 * n, cudaMemcpyDeviceToDevice, st), "restore mass");
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->stat[a].id, s.id, 4 * n, cudaMemcpyDeviceToDevice, st), "restore id");
+    c->keysValid = false;
+    c->haveOrder = false;
+    return DEM_OK;
+}
+
 bool has_attraction_host(const KParams& P) {
     for (uint32_t m = 0; m < P.nmat; ++m)
         if (P.at[m] != 0.0f) return true;
@@ -1560,6 +1577,8 @@ extern "C" int dem_adj_forward(DemContext* c, uint32_t nsteps, uint32_t every, v
     c->adjSteps = nsteps;
     c->adjEvery = every;
     c->adjWindows = windows;
+    c->adjN = c->n;
+    c->adjRmax = c->rmax;
     return DEM_OK;
 }
 
@@ -1568,6 +1587,9 @@ extern "C" int dem_adj_backward(DemContext* c, float* lamPos, float* lamVel, flo
     int rc = adj_check_context(c);
     if (rc) return rc;
     if (!c->adjWindows) return fail(DEM_ERR_INVALID_ARG, "run dem_adj_forward first");
+    if (c->n != c->adjN || !(c->rmax == c->adjRmax))
+        return fail(DEM_ERR_INVALID_ARG,
+                    "the particles changed since dem_adj_forward (dem_set_state): run it again");
     if (!lamPos || !lamVel || !lamOmega || !grad) return fail(DEM_ERR_INVALID_ARG, "NULL buffer");
     cudaStream_t st = (cudaStream_t)stream;
     const uint32_t n = c->n;
@@ -1600,9 +1622,8 @@ extern "C" int dem_adj_backward(DemContext* c, float* lamPos, float* lamVel, flo
     const size_t snap = snapshot_bytes(n);
     cudaGraphExec_t recLoop[2] = {}, revLoop = nullptr;
     for (int w = (int)c->adjWindows - 1; w >= 0 && rc == DEM_OK && e == cudaSuccess; --w) {
-        Snapshot s = carve_snapshot(static_cast<char*>(c->adjCheck) + snap * w, n);
-        rc = dem_set_state(c, n, s.pos, s.vel, s.theta, s.omega, s.radius, s.mass, s.id, nullptr,
-                           0, stream);
+        rc = restore_checkpoint(c, carve_snapshot(static_cast<char*>(c->adjCheck) + snap * w, n),
+                                st);
         if (rc) break;
         const uint32_t k = std::min(c->adjEvery, c->adjSteps - (uint32_t)w * c->adjEvery);
         if (!c->keysValid) {
@@ -1625,10 +1646,8 @@ extern "C" int dem_adj_backward(DemContext* c, float* lamPos, float* lamVel, flo
         rc = step_recorded(c, st, rec);
         if (rc) break;
         const uint32_t pairs = (k - 1) / 2;
-        const uint32_t words[6] = {pairs, 0u, 1u, k, 0u, k - 1u};
-        std::memcpy(c->adjLoopHost, words, sizeof(words));
-        e = cudaMemcpyAsync(c->loopCtl + kLoopRecReq, c->adjLoopHost, sizeof(words),
-                            cudaMemcpyHostToDevice, st);
+        e = launch_set_words(c->loopCtl + kLoopRecReq, Words{{pairs, 0u, 1u, k, 0u, k - 1u}, 6u},
+                             st);
         if (e != cudaSuccess) break;
         if (pairs) {
             const int p = c->cur;

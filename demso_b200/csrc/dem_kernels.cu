@@ -900,6 +900,18 @@ __global__ void loop_next_kernel(uint32_t* __restrict__ left, uint32_t* __restri
 }
 }  // namespace
 
+namespace {
+__global__ void set_words_kernel(uint32_t* __restrict__ dst, Words w) {
+    for (uint32_t i = 0; i < w.count; ++i) dst[i] = w.v[i];
+}
+}  // namespace
+
+cudaError_t launch_set_words(uint32_t* dst, Words w, cudaStream_t st) {
+    if (w.count > 8) return cudaErrorInvalidValue;
+    set_words_kernel<<<1, 1, 0, st>>>(dst, w);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_loop_init(const uint32_t* req, uint32_t* left, cudaGraphConditionalHandle h,
                              cudaStream_t st) {
     loop_init_kernel<<<1, 1, 0, st>>>(req, left, h);

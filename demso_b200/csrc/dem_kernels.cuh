@@ -139,6 +139,14 @@ cudaError_t launch_loop_init(const uint32_t* req, uint32_t* left, cudaGraphCondi
                              cudaStream_t st);
 cudaError_t launch_loop_next(uint32_t* left, uint32_t* idx, int32_t idxStep,
                              cudaGraphConditionalHandle h, cudaStream_t st);
+// Writes up to 8 words, passed by value, to device memory in stream order
+// (a loop's counts before its launch: no host buffer has to outlive the
+// call, and the host never waits).
+struct Words {
+    uint32_t v[8];
+    uint32_t count;
+};
+cudaError_t launch_set_words(uint32_t* dst, Words w, cudaStream_t st);
 
 // Adjoint (dem_adjoint.cu).
 size_t adj_step_bytes(uint32_t n, uint32_t numCells);

@@ -375,7 +375,12 @@ int dem_render(DemContext* ctx, const DemRenderParams* params, void* image, void
  * (particles_kernel.cuh:419-421).  Coefficient sums are in double, in a
  * fixed order (deterministic).  After
  * dem_adj_backward the context holds the state at the end of the first
- * window; set the state again before stepping on.
+ * window; set the state again before stepping on.  The backward restores
+ * the checkpoints as they are: a dem_set_state between the two calls that
+ * changes the particle count or the largest radius makes dem_adj_backward
+ * fail with DEM_ERR_INVALID_ARG.  Each window's re-run and reversed steps
+ * run as two device-side loops (graph WHILE nodes), so the host does not
+ * wait between windows.
  * ------------------------------------------------------------------------- */
 #define DEM_ADJ_NUM_COEF 7
 int dem_adj_forward(DemContext* ctx, uint32_t nsteps, uint32_t every, void* stream);

@@ -132,6 +132,33 @@ def test_adjoint_rejects_what_it_does_not_differentiate():
     sim.close()
 
 
+def test_backward_refuses_particles_replaced_after_the_forward():
+    """The backward restores the forward's checkpoints without re-deriving
+    the culling bound, so a state with a larger radius set in between is
+    refused; the same particles set again are not."""
+    import torch
+    import demso_b200 as D
+    sc = scenes.agitated_gas(n=512, seed=3)
+    sim = D.Simulation(sc.sys, capacity=sc.n, flags=D.CTX_ACCEL)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a).copy())
+    state = lambda r: (t(sc.pos), t(sc.vel), t(sc.theta), t(sc.omega), t(r), t(sc.mass),
+                       t(sc.id.view(np.int32)))
+    L = D.load()
+    stream = torch.cuda.current_stream().cuda_stream
+    lam = [torch.zeros(k, dtype=torch.float32, device="cuda") for k in (2 * sc.n, 2 * sc.n, sc.n)]
+    sim.set_state(*state(sc.radius))
+    sim.adjoint_forward(20, 7)
+    sim.set_state(*state(sc.radius * np.float32(1.5)))
+    with pytest.raises(D.DemError):
+        sim.adjoint_backward(*lam)
+    sim.set_state(*state(sc.radius))
+    sim.adjoint_forward(20, 7)
+    sim.set_state(*state(sc.radius))
+    g = sim.adjoint_backward(*lam)
+    assert np.all(np.isfinite(g))
+    sim.close()
+
+
 def test_batched_adjoint_equals_each_specimen_alone():
     """Three specimens of different sizes and contact parameters in one
     batch: the state cotangents equal each specimen's own adjoint bit for
