@@ -14,9 +14,10 @@ built, so this is weak scaling by replicas.
 dem_step call (device time, CUDA events, max over ranks); the library runs
 them as one graph launch of its device-side step loop.  `e2e` is the same
 workload through the C ABI with host buffers: the state uploaded from pinned
-host memory, K steps each followed by the reference's per-step
-followed-particle readback (writeOutputFile), and the state downloaded, all
-inside the timed region.  `roofline` is for the dominant kernel, timed by
+host memory, K steps with the reference's per-step followed-particle output
+(writeOutputFile) of every step gathered on the device and copied to pinned
+host memory (dem_step_followed), and the state downloaded, all inside the
+timed region.  `roofline` is for the dominant kernel, timed by
 CUDA events recorded around each stage's graph launch in a second pass of K
 steps launched one step at a time (events cannot sit inside the device-side
 loop); that pass's whole-step time is `ms_per_step_stage_timed`.
@@ -613,38 +614,33 @@ def main():
         sim2.set_step_variant(shape["variant"])
         out_host = {k: torch.empty_like(v).pin_memory() for k, v in host.items()}
         follow = np.array([n // 3, (2 * n) // 3], dtype=np.uint32)
-        rows = np.zeros(12 * follow.size, np.float32)
-        # each step's rows go to one of two pinned buffers while the next step
-        # is queued (dem_get_followed_async); the host reads a step's rows
-        # once the event recorded after its copy has passed
-        pinned = [torch.zeros(12 * follow.size, dtype=torch.float32).pin_memory()
-                  for _ in range(2)]
-        done = [torch.cuda.Event() for _ in range(2)]
+        # every step's followed rows (the reference's per-step output) are
+        # gathered on the device inside the step loop and reach this pinned
+        # buffer by one copy (dem_step_followed)
+        rows = torch.zeros(args.steps * follow.size * 12, dtype=torch.float32).pin_memory()
         L = D.load()
+        # warm-up outside the timed region: the step loop's graphs of both
+        # parities are captured here
         sim2.set_state(host["pos"], host["vel"], host["theta"], host["omega"], host["radius"],
                        host["mass"], host["id"])
-        sim2.step(3)  # build graphs outside the timed region
+        sim2.step_followed(3, follow, rows)
+        sim2.step(1)
+        sim2.step_followed(2, follow, rows)
         torch.cuda.synchronize()
         barrier()
         t0 = time.perf_counter()
         sim2.set_state(host["pos"], host["vel"], host["theta"], host["omega"], host["radius"],
                        host["mass"], host["id"])
-        for k in range(args.steps):
-            sim2.step(1)
-            D.check(L.dem_get_followed_async(sim2.handle, follow.ctypes.data, follow.size,
-                                             pinned[k & 1].data_ptr(), D._stream()))
-            done[k & 1].record(stream)
-            if k:
-                done[(k - 1) & 1].synchronize()
-                rows[:] = pinned[(k - 1) & 1].numpy()
-        done[(args.steps - 1) & 1].synchronize()
-        rows[:] = pinned[(args.steps - 1) & 1].numpy()
+        sim2.step_followed(args.steps, follow, rows)
         p = lambda k: out_host[k].data_ptr()
         D.check(L.dem_get_state(sim2.handle, p("pos"), p("vel"), p("theta"), p("omega"),
                                 p("radius"), p("mass"), p("id"), None, None, None, None, None, 1,
                                 D._stream()))
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t0
+        last = rows.numpy().reshape(args.steps, follow.size, 12)[-1]
+        if not np.array_equal(last[:, 0].view(np.uint32), follow):
+            raise RuntimeError("the last step's followed rows were not written")
         if dist is not None:
             t = torch.tensor([e2e_s], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -652,7 +648,9 @@ def main():
         state_bytes = sum(v.numel() * v.element_size() for v in host.values())
         e2e = {"value": n * world * args.steps / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": state_bytes / args.steps,
-               "d2h_bytes_per_step": state_bytes / args.steps + rows.nbytes}
+               "d2h_bytes_per_step": state_bytes / args.steps + 48 * follow.size,
+               "path": "dem_set_state from pinned host memory, dem_step_followed (the "
+                       "followed rows of every step), dem_get_state to pinned host memory"}
         sim2.close()
 
     batched = None

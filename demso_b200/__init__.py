@@ -338,6 +338,32 @@ class Simulation:
             check(load().dem_get_followed_async(self._h, ids.ctypes.data, ids.size,
                                                 rows.data_ptr(), _stream(stream)))
 
+    def step_followed(self, nsteps: int, ids, rows=None, stream=None):
+        """dem_step_followed: `nsteps` steps with the followed rows of `ids`
+        after each, into `rows`, a contiguous float32 tensor of
+        nsteps * len(ids) * 12 values in pinned host memory or on the GPU
+        (returned without waiting: synchronise `stream` before reading it), or,
+        when None, a new (nsteps, len(ids), 12) numpy array (filled on
+        return)."""
+        import numpy as np
+        ids = np.ascontiguousarray(ids, dtype=np.uint32)
+        need = int(nsteps) * ids.size * 12
+        if rows is None:
+            out = np.zeros((int(nsteps), ids.size, 12), np.float32)
+            ptr = out.ctypes.data
+        else:
+            import torch
+            if rows.dtype != torch.float32 or not rows.is_contiguous() or rows.numel() < need:
+                raise ValueError("rows must be a contiguous float32 tensor of "
+                                 "nsteps * 12 * len(ids) values")
+            out, ptr = rows, rows.data_ptr()
+        check(load().dem_step_followed(self._h, int(nsteps), ids.ctypes.data if ids.size else None,
+                                       ids.size, ptr if ids.size else None, _stream(stream)))
+        if rows is None:
+            import torch
+            (stream or torch.cuda.current_stream()).synchronize()
+        return out
+
     # -- adjoint (dem_adj_forward / dem_adj_backward) ------------------------
     def adjoint_forward(self, nsteps: int, every: int, stream=None) -> None:
         """`nsteps` steps as ``step``, keeping a checkpoint every `every` steps

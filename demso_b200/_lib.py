@@ -108,6 +108,7 @@ SIGNATURES = [
     ("dem_get_step_variant", C.c_int, [_P, C.POINTER(DemStepVariant)]),
     ("dem_get_followed", C.c_int, [_P, _P, _U, _P, _P]),
     ("dem_get_followed_async", C.c_int, [_P, _P, _U, _P, _P]),
+    ("dem_step_followed", C.c_int, [_P, _U, _P, _U, _P, _P]),
     ("dem_profile_begin", C.c_int, [_P, _U]),
     ("dem_profile_end", C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(_U)]),
     ("dem_adj_forward", C.c_int, [_P, _U, _U, _P]),

@@ -342,6 +342,14 @@ struct DemContext {
     void* block = nullptr;  // one allocation for every per-particle/per-cell array
     // followed-particle staging (device), see dem_get_followed
     float* followRows = nullptr;
+    // dem_step_followed: the ids (device copy), the ring of per-step rows,
+    // and its device-side loop followGraph[parity] (holds both pointers)
+    uint32_t* followIds = nullptr;
+    uint32_t followIdsCap = 0;
+    float* followRing = nullptr;
+    size_t followRingBytes = 0;
+    std::vector<uint32_t> followIdsHost;
+    cudaGraphExec_t followGraph[2] = {};
     // stage profiling: events recorded on the caller's stream around the two
     // launches of each step (3 per step)
     bool profiling = false;
@@ -385,6 +393,8 @@ void drop_loop_graphs(DemContext* c) {
     for (int p = 0; p < 2; ++p) {
         if (c->loopGraph[p]) cudaGraphExecDestroy(c->loopGraph[p]);
         c->loopGraph[p] = nullptr;
+        if (c->followGraph[p]) cudaGraphExecDestroy(c->followGraph[p]);
+        c->followGraph[p] = nullptr;
     }
 }
 
@@ -579,6 +589,8 @@ enum : uint32_t {
     kLoopStepReq = 0, kLoopStepLeft = 1,                    // dem_step's step pairs
     kLoopRecReq = 2, kLoopRecLeft = 3, kLoopRecSlot = 4,    // adjoint recompute pairs
     kLoopRevReq = 5, kLoopRevLeft = 6, kLoopRevSlot = 7,    // adjoint reversed steps
+    kLoopFolReq = 8, kLoopFolLeft = 9, kLoopFolSlot = 10,   // dem_step_followed pairs
+    kLoopFolCount = 11,                                     // its number of ids
 };
 
 // A graph of one device-side loop: an init kernel that copies loopCtl[req]
@@ -621,18 +633,16 @@ int build_while_graph(DemContext* c, uint32_t req, int idx, int32_t idxStep, Bod
 }
 
 // Two incremental steps from parity p (p, then p ^ 1: the sort phase and the
-// step kernel as in sortGraph[1] and stepGraph) into `bs`; after each, when
-// `rec` is set, its record at slot loopCtl[kLoopRecSlot] + k.
-cudaError_t enqueue_step_pair(DemContext* c, int p, cudaStream_t bs, void* rec, size_t stride) {
+// step kernel as in sortGraph[1] and stepGraph) into `bs`, each followed by
+// after(k, bs) (k = 0, 1: the step's place in the pair).
+template <typename After>
+cudaError_t enqueue_step_pair(DemContext* c, int p, cudaStream_t bs, After after) {
     cudaError_t e = cudaSuccess;
     for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
         c->cur = p ^ k;
         e = enqueue_sort_phase(c, 1, bs, nullptr);
         if (e == cudaSuccess) e = enqueue_step_kernel(c, bs, nullptr);
-        if (e == cudaSuccess && rec)
-            e = adj_record_step(rec, RecSlot{c->loopCtl + kLoopRecSlot, (uint32_t)k, stride}, c->n,
-                                c->numCells, step_in(c, p ^ k), step_in_static(c, p ^ k), c->src,
-                                c->cells[p ^ k ^ 1], c->acc, c->alpha, bs);
+        if (e == cudaSuccess) e = after(k, bs);
     }
     return e;
 }
@@ -641,8 +651,37 @@ cudaError_t enqueue_step_pair(DemContext* c, int p, cudaStream_t bs, void* rec, 
 int build_loop_graph(DemContext* c, int p) {
     return build_while_graph(
         c, kLoopStepReq, -1, 0,
-        [&](cudaStream_t bs) { return enqueue_step_pair(c, p, bs, nullptr, 0); },
+        [&](cudaStream_t bs) {
+            return enqueue_step_pair(c, p, bs, [](int, cudaStream_t) { return cudaSuccess; });
+        },
         &c->loopGraph[p]);
+}
+
+// The followed rows of the state after a step of parity a (the current
+// state is then dyn[0].pos, dyn[a ^ 1], stat[a ^ 1]) into ring block
+// (slot ? *slot : 0) + add.
+cudaError_t enqueue_followed_ring(DemContext* c, int a, const uint32_t* slot, uint32_t add,
+                                  cudaStream_t st) {
+    const int b = a ^ 1;
+    return launch_followed_ring(c->followIds, c->loopCtl + kLoopFolCount, slot, add, c->loc,
+                                DynSet{c->dyn[0].pos, c->dyn[b].vel, c->dyn[b].theta, c->dyn[b].omega},
+                                c->stat[b], (c->flags & DEM_CTX_ACCEL) ? c->acc : nullptr,
+                                (c->flags & DEM_CTX_ACCEL) ? c->alpha : nullptr,
+                                (c->flags & DEM_CTX_PRESSURE) ? c->pressure : nullptr,
+                                c->followRing, st);
+}
+
+// dem_step_followed's loop from parity p: pairs of steps, each followed by
+// its rows at ring block loopCtl[kLoopFolSlot] + k.
+int build_follow_graph(DemContext* c, int p) {
+    return build_while_graph(
+        c, kLoopFolReq, kLoopFolSlot, 2,
+        [&](cudaStream_t bs) {
+            return enqueue_step_pair(c, p, bs, [&](int k, cudaStream_t s2) {
+                return enqueue_followed_ring(c, p ^ k, c->loopCtl + kLoopFolSlot, (uint32_t)k, s2);
+            });
+        },
+        &c->followGraph[p]);
 }
 
 void drop_tune_events(DemContext* c) {
@@ -911,6 +950,8 @@ extern "C" int dem_destroy(DemContext* c) {
     if (c->forkEv) cudaEventDestroy(c->forkEv);
     if (c->joinEv) cudaEventDestroy(c->joinEv);
     cudaFree(c->followRows);
+    cudaFree(c->followIds);
+    cudaFree(c->followRing);
     cudaFree(c->adjCheck);
     cudaFree(c->renderOwner);
     cudaFree(c->ctlBlock);
@@ -1287,6 +1328,78 @@ extern "C" int dem_get_followed_async(DemContext* c, const uint32_t* ids, uint32
 }
 
 namespace {
+constexpr size_t kFollowRingBytes = 64ull << 20;  // rows of one chunk of steps
+}  // namespace
+
+extern "C" int dem_step_followed(DemContext* c, uint32_t nsteps, const uint32_t* ids,
+                                 uint32_t count, float* rows, void* stream) {
+    if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    if (count == 0 || nsteps == 0) return dem_step(c, nsteps, stream);
+    if (!ids || !rows) return fail(DEM_ERR_INVALID_ARG, "dem_step_followed: NULL buffer");
+    for (uint32_t i = 0; i < count; ++i)
+        if (ids[i] >= c->n) return fail(DEM_ERR_INVALID_ARG, "followed id %u >= n %u", ids[i], c->n);
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t rowBytes = 48ull * count;  // one step's rows
+    const uint32_t chunk =
+        (uint32_t)std::min<size_t>(nsteps, std::max<size_t>(1, kFollowRingBytes / rowBytes));
+    if (c->followIdsCap < count) {
+        drop_loop_graphs(c);
+        cudaFree(c->followIds);
+        c->followIds = nullptr;
+        c->followIdsCap = 0;
+        DEM_TRY_CUDA(cudaMalloc(&c->followIds, 4ull * count), "cudaMalloc followed ids");
+        c->followIdsCap = count;
+    }
+    if (c->followRingBytes < chunk * rowBytes) {
+        drop_loop_graphs(c);
+        cudaFree(c->followRing);
+        c->followRing = nullptr;
+        c->followRingBytes = 0;
+        DEM_TRY_CUDA(cudaMalloc(&c->followRing, chunk * rowBytes), "cudaMalloc followed rows");
+        c->followRingBytes = chunk * rowBytes;
+    }
+    // the ids go through a library-owned host copy, so they are read before
+    // this call returns whatever memory the caller passed
+    c->followIdsHost.assign(ids, ids + count);
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->followIds, c->followIdsHost.data(), 4ull * count,
+                                 cudaMemcpyHostToDevice, st),
+                 "followed ids");
+    DEM_TRY_CUDA(launch_set_words(c->loopCtl + kLoopFolCount, Words{{count}, 1u}, st),
+                 "followed count");
+    for (uint32_t s = 0; s < nsteps;) {
+        const uint32_t m = std::min(chunk, nsteps - s);
+        for (uint32_t j = 0; j < m;) {
+            // pairs of steps with their rows in the device-side loop, as in
+            // dem_step; a step with host work around it (the first after
+            // dem_set_state, tuning, profiling, direct launches) alone
+            if (!(c->flags & DEM_CTX_DIRECT) && !c->profiling && c->tuned >= 0 && c->haveOrder &&
+                m - j >= 2) {
+                const uint32_t pairs = (m - j) / 2;
+                const int p = c->cur;
+                if (!c->followGraph[p]) {
+                    int rc = build_follow_graph(c, p);
+                    if (rc) return rc;
+                }
+                DEM_TRY_CUDA(launch_set_words(c->loopCtl + kLoopFolReq, Words{{pairs, 0u, j}, 3u}, st),
+                             "followed loop count");
+                DEM_TRY_CUDA(cudaGraphLaunch(c->followGraph[p], st), "graph launch");
+                j += 2 * pairs;
+            } else {
+                int rc = dem_step(c, 1, stream);
+                if (rc) return rc;
+                DEM_TRY_CUDA(enqueue_followed_ring(c, c->cur ^ 1, nullptr, j, st), "followed gather");
+                ++j;
+            }
+        }
+        DEM_TRY_CUDA(cudaMemcpyAsync(rows + (size_t)s * count * 12, c->followRing, m * rowBytes,
+                                     cudaMemcpyDefault, st),
+                     "followed rows copy");
+        s += m;
+    }
+    return DEM_OK;
+}
+
+namespace {
 int check_render(const DemRenderParams* rp) {
     if (!rp) return fail(DEM_ERR_INVALID_ARG, "render parameters are NULL");
     if (rp->imageDIMx == 0 || rp->imageDIMy == 0 ||
@@ -1654,7 +1767,14 @@ extern "C" int dem_adj_backward(DemContext* c, float* lamPos, float* lamVel, flo
             if (!recLoop[p]) {
                 rc = build_while_graph(
                     c, kLoopRecReq, kLoopRecSlot, 2,
-                    [&](cudaStream_t bs) { return enqueue_step_pair(c, p, bs, rec, stepBytes); },
+                    [&](cudaStream_t bs) {
+                        return enqueue_step_pair(c, p, bs, [&](int k, cudaStream_t s2) {
+                            return adj_record_step(
+                                rec, RecSlot{c->loopCtl + kLoopRecSlot, (uint32_t)k, stepBytes},
+                                c->n, c->numCells, step_in(c, p ^ k), step_in_static(c, p ^ k),
+                                c->src, c->cells[p ^ k ^ 1], c->acc, c->alpha, s2);
+                        });
+                    },
                     &recLoop[p]);
                 if (rc) break;
             }

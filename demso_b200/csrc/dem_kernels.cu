@@ -689,15 +689,13 @@ __global__ void unpack_cells_kernel(const uint2* __restrict__ range, uint32_t nu
     if (cellEnd) cellEnd[c] = v.y;
 }
 
-// One row of the reference's followed-particle output per id
-// (functions.cu:630-654): id, type, pos, vel, acc, theta, omega, alpha, pressure.
-__global__ void followed_kernel(FollowIds f, const uint32_t* __restrict__ loc, DynSet d, StatSet s,
-                                const float2* __restrict__ acc, const float* __restrict__ alpha,
-                                const float* __restrict__ pressure, float* __restrict__ rows) {
-    const uint32_t k = threadIdx.x;
-    if (k >= f.count) return;
-    const uint32_t i = loc[f.id[k]];
-    float* r = rows + 12 * k;
+// One row of the reference's followed-particle output (functions.cu:630-654)
+// for the particle in slot i: id, type, pos, vel, acc, theta, omega, alpha,
+// pressure.
+__device__ __forceinline__ void followed_row(uint32_t i, float* __restrict__ r, const DynSet& d,
+                                             const StatSet& s, const float2* __restrict__ acc,
+                                             const float* __restrict__ alpha,
+                                             const float* __restrict__ pressure) {
     r[0] = __uint_as_float(s.id[i]);
     r[1] = __uint_as_float(s.type ? s.type[i] : 0u);
     const float2 p = d.pos[i], v = d.vel[i];
@@ -712,6 +710,29 @@ __global__ void followed_kernel(FollowIds f, const uint32_t* __restrict__ loc, D
     r[9] = d.omega[i];
     r[10] = alpha ? alpha[i] : 0.0f;
     r[11] = pressure ? pressure[i] : 0.0f;
+}
+
+__global__ void followed_kernel(FollowIds f, const uint32_t* __restrict__ loc, DynSet d, StatSet s,
+                                const float2* __restrict__ acc, const float* __restrict__ alpha,
+                                const float* __restrict__ pressure, float* __restrict__ rows) {
+    const uint32_t k = threadIdx.x;
+    if (k >= f.count) return;
+    followed_row(loc[f.id[k]], rows + 12 * k, d, s, acc, alpha, pressure);
+}
+
+// The rows of ids[0, *count) into row block (slot ? *slot : 0) + add of
+// `ring` (*count rows of 12 words per block).
+__global__ void followed_ring_kernel(const uint32_t* __restrict__ ids,
+                                     const uint32_t* __restrict__ countWord,
+                                     const uint32_t* __restrict__ slot, uint32_t add,
+                                     const uint32_t* __restrict__ loc, DynSet d, StatSet s,
+                                     const float2* __restrict__ acc,
+                                     const float* __restrict__ alpha,
+                                     const float* __restrict__ pressure, float* __restrict__ ring) {
+    const uint32_t count = *countWord;
+    float* base = ring + (size_t)((slot ? *slot : 0u) + add) * count * 12;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x)
+        followed_row(loc[ids[k]], base + 12ull * k, d, s, acc, alpha, pressure);
 }
 
 // Largest radius (positive floats order like their bit patterns).
@@ -737,6 +758,15 @@ cudaError_t launch_followed(const FollowIds& f, const uint32_t* loc, DynSet d, S
                             const float2* acc, const float* alpha, const float* pressure,
                             float* rows, cudaStream_t st) {
     followed_kernel<<<1, kFollowBatch, 0, st>>>(f, loc, d, s, acc, alpha, pressure, rows);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_followed_ring(const uint32_t* ids, const uint32_t* countWord,
+                                 const uint32_t* slot, uint32_t add, const uint32_t* loc, DynSet d,
+                                 StatSet s, const float2* acc, const float* alpha,
+                                 const float* pressure, float* ring, cudaStream_t st) {
+    followed_ring_kernel<<<16, 128, 0, st>>>(ids, countWord, slot, add, loc, d, s, acc, alpha,
+                                             pressure, ring);
     return cudaGetLastError();
 }
 

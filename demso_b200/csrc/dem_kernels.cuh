@@ -30,6 +30,13 @@ struct FollowIds {
 cudaError_t launch_followed(const FollowIds& f, const uint32_t* loc, DynSet d, StatSet s,
                             const float2* acc, const float* alpha, const float* pressure,
                             float* rows, cudaStream_t st);
+// Followed rows of a multi-step call: the ids ids[0, *countWord) (device
+// memory) gathered into row block (slot ? *slot : 0) + add of `ring`, each
+// block *countWord rows of 12 words (the device-side loop advances *slot).
+cudaError_t launch_followed_ring(const uint32_t* ids, const uint32_t* countWord,
+                                 const uint32_t* slot, uint32_t add, const uint32_t* loc, DynSet d,
+                                 StatSet s, const float2* acc, const float* alpha,
+                                 const float* pressure, float* ring, cudaStream_t st);
 
 // Upper bound of the radii: writes the largest radius's bit pattern to *out.
 cudaError_t launch_max_radius(const float* radius, uint32_t n, uint32_t* out, cudaStream_t st);

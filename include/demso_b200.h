@@ -277,6 +277,21 @@ int dem_get_followed(DemContext* ctx, const uint32_t* ids, uint32_t count, float
 int dem_get_followed_async(DemContext* ctx, const uint32_t* ids, uint32_t count, float* rows,
                            void* stream);
 
+/* `nsteps` steps as dem_step, with after each step the rows dem_get_followed
+ * would give for `ids` (host array of `count` ids < n, read before the call
+ * returns): rows (host or device memory) receives nsteps * count * 12 words,
+ * step-major, the rows of step k at rows + 12 * count * k.  This is the
+ * reference's stepping loop with writeOutputFile after every step
+ * (main.cu:396-507, functions.cu:608-661) in one call: pairs of steps run in
+ * the device-side loop, each step's rows gathered on the device into a ring
+ * of up to 64 MB, which reaches `rows` by one copy per chunk of steps.  The
+ * copies are queued on `stream`: with pinned or device memory the rows are
+ * complete once `stream` has synchronised (pageable memory is written before
+ * each copy returns).  Bit for bit the rows and state of nsteps calls of
+ * dem_step(ctx, 1) each followed by dem_get_followed. */
+int dem_step_followed(DemContext* ctx, uint32_t nsteps, const uint32_t* ids, uint32_t count,
+                      float* rows, void* stream);
+
 /* Stage timing inside dem_step.  Each step is two graph launches on the
  * caller's stream: the sort phase (incremental sort, or the full radix sort
  * with cell ranges and gather) and the step kernel.  After
