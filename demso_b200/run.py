@@ -63,16 +63,17 @@ def run(path: str, steps: int = None, seed: int = 0, csv: str = None, frames: st
         frame(0)
     done = 0
     while done < steps:
+        k = min(chunk, steps - done)
+        if frames and frame_every:
+            k = min(k, frame_every - done % frame_every)
         if out is not None:
-            sim.step(1)
-            done += 1
-            out.write(followed_line(elapsed_time(sc.time_step, done), sim.followed(followed)))
+            # k steps with every step's rows gathered on the device (dem_step_followed)
+            rows = sim.step_followed(k, followed)
+            for j in range(k):
+                out.write(followed_line(elapsed_time(sc.time_step, done + j + 1), rows[j]))
         else:
-            k = min(chunk, steps - done)
-            if frames and frame_every:
-                k = min(k, frame_every - done % frame_every)
             sim.step(k)
-            done += k
+        done += k
         if frames and frame_every and done % frame_every == 0:
             frame(done)
     torch.cuda.synchronize()
