@@ -93,6 +93,13 @@ def test_autotuned_context_into_pinned_rows():
     _check(lambda: _make(sc, flags=D.CTX_AUTOTUNE), ids, [1, 20, 9, 10], pinned=True)
 
 
+def test_direct_launches():
+    import demso_b200 as D
+    sc = scenes.agitated_gas(n=2000, seed=9, vel_std=1.0)
+    ids = np.arange(0, 2000, 7, dtype=np.uint32)
+    _check(lambda: _make(sc, flags=D.CTX_DIRECT), ids, [12, 5])
+
+
 def test_batch_rows():
     batch = scenes.specimen_batch(num=10, seed=8, nmin=64, nmax=2048)
     n = sum(s.n for s in batch)
