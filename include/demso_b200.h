@@ -161,7 +161,10 @@ int dem_integrate_system(const DemSystem* sys, float* pos, float* vel, const flo
  * on library-owned device buffers: a sort phase (incremental stable sort,
  * cell ranges, positions and radii moved to sorted order) and one step
  * kernel (collide, integrate, next hash, gathering the other fields into
- * sorted order), both replayed as CUDA graphs.
+ * sorted order), both replayed as CUDA graphs.  A context's calls share its
+ * device buffers and its loop counters: issue them on one stream, or
+ * synchronise before a call on another stream.  Different contexts are
+ * independent and may run on different streams and host threads.
  * ------------------------------------------------------------------------- */
 typedef struct DemContext DemContext;
 
