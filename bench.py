@@ -373,14 +373,12 @@ def measure_adjoint(n: int = 16384, steps: int = 2000, every: int = 100):
 
 
 # ------------------------------------------------------------------ config 0
-def measure_settling_pile(steps: int = 20000, cpu_sample: int = 2000):
+def measure_settling_pile(steps: int = 20000):
     """The plain 2D settling pile (4,096 disks, 20,000 steps): wall time of
-    the whole run on the GPU, beside the reference's step functions built
-    for the host (timed on `cpu_sample` of the steps, all host threads)."""
+    the whole run on the GPU (settling_pile_cpu adds the host build's)."""
     import torch
     import demso_b200 as D
     from demso_b200 import scenes
-    from oracle import oracle as O
     sc = scenes.settling_pile()
     sim = D.Simulation(sc.sys, capacity=sc.n, flags=D.CTX_PRESSURE)
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int32) if a.dtype == np.uint32
@@ -404,6 +402,17 @@ def measure_settling_pile(steps: int = 20000, cpu_sample: int = 2000):
                        "jittered lattice in a 0.2 x 0.2 m box, dt 2e-6 s, %d steps" % steps,
            "gpu_seconds": gpu_s, "gpu_steps_per_s": steps / gpu_s,
            "gpu_particle_steps_per_s": sc.n * steps / gpu_s}
+    return out
+
+
+def settling_pile_cpu(out: dict, steps: int = 20000, cpu_sample: int = 2000) -> dict:
+    """The reference's step functions built for the host on the settling pile
+    (timed on `cpu_sample` of the steps, all host threads), beside the GPU
+    run of measure_settling_pile."""
+    from demso_b200 import scenes
+    from oracle import oracle as O
+    sc = scenes.settling_pile()
+    gpu_s = out["gpu_seconds"]
     if O.ref_available():
         h = O.RefHarness(threads=os.cpu_count() or 1)
         h.setup(sc.sys, sc.radius, sc.mass, None)
@@ -598,15 +607,6 @@ def main():
     whole_bytes = WHOLE_STEP_BYTES(n, cells)
     step_ms = elapsed / args.steps
 
-    # ---- CPU baseline (rank 0, N = 1 only)
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        try:
-            cpu, _ = cpu_reference_rate(12.0)
-        except Exception as e:  # the baseline is reported, never the target
-            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "unavailable",
-                   "sample": "failed: %s" % e}
-
     # ---- end to end through the C ABI with host buffers
     e2e = None
     if not args.no_e2e:
@@ -676,6 +676,22 @@ def main():
             adjoint = measure_adjoint()
         except Exception as e:  # reported beside the headline, never instead of it
             adjoint = {"error": str(e)}
+
+    # ---- host-core measurements, after every GPU leg: the reference's host
+    # build leaves its OpenMP threads busy on every core for a while after it
+    # returns, which would slow the host-side work of a GPU leg run after it
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu, _ = cpu_reference_rate(12.0)
+        except Exception as e:  # the baseline is reported, never the target
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "unavailable",
+                   "sample": "failed: %s" % e}
+    if pile is not None and "error" not in pile:
+        try:
+            pile = settling_pile_cpu(pile)
+        except Exception as e:  # reported beside the GPU time, never instead of it
+            pile["cpu_error"] = str(e)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
