@@ -221,10 +221,11 @@ int dem_get_state(DemContext* ctx, float* pos, float* vel, float* theta, float* 
 
 /* Advances `nsteps` full steps (hash, sort, reorder, collide, integrate).
  * Once the context holds a previous order (after its first step) and is
- * neither tuning nor profiling, a call of two or more steps runs them in
- * pairs inside ONE graph launch: a device-side loop (a CUDA graph WHILE
- * node, its pair count written to the device before the launch and counted
- * down there) whose body is two whole steps, one per buffer parity; an odd
+ * neither tuning nor profiling nor created with DEM_CTX_DIRECT, a call of
+ * two or more steps runs them in pairs inside ONE graph launch: a
+ * device-side loop (a CUDA graph WHILE node, its pair count written to the
+ * device by a one-thread kernel before the launch and counted down there)
+ * whose body is two whole steps, one per buffer parity; an odd
  * last step is one more ordinary step.  The loop runs the same kernels on
  * the same buffers as single calls, so the bits are those of nsteps calls
  * of one step.
