@@ -95,6 +95,13 @@ def test_bad_arguments_are_status_codes_not_crashes():
     assert lib.dem_create(None, 10, 0, C.byref(h)) == 1
     assert lib.dem_create(s, 0, 0, C.byref(h)) == 1
     assert lib.dem_step(None, 1, None) == 1
+    ids = (C.c_uint32 * 2)(0, 1)
+    rows = (C.c_float * 24)()
+    assert lib.dem_step_followed(None, 1, ids, 2, rows, None) == 1
+    assert lib.dem_get_followed(None, ids, 2, rows, None) == 1
+    assert lib.dem_get_followed_async(None, ids, 2, rows, None) == 1
+    assert lib.dem_adj_forward(None, 10, 5, None) == 1
+    assert lib.dem_adj_backward(None, None, None, None, None, None) == 1
     assert lib.dem_destroy(None) == 0
     # n = 0 is a no-op
     assert lib.dem_calc_hash(s, None, None, None, 0, None) == 0
