@@ -64,6 +64,9 @@ FUSED_MIN_BYTES_PER_PARTICLE = 88
 # Whole step, per particle: hash 16 + sort 52 + reorder 84 + collide 40 +
 # integrate 68 = 260, plus 20 per cell (reorder 12, collide 8).
 WHOLE_STEP_BYTES = lambda n, c: 260.0 * n + 20.0 * c  # whole-step model, per step
+# the timed K-step call is repeated until this much device time is under load
+MIN_TIMED_S = 1.0
+MIN_REPEATS, MAX_REPEATS = 3, 5000
 
 
 def peaks():
@@ -267,7 +270,9 @@ def measure_batched(steps: int, warmup: int, num: int = 4096, loop_sample: int =
     batched = total * steps / (e0.elapsed_time(e1) * 1e-3)
     kernels = b.kernels_per_step()
     b.close()
-    # looped plain step: one single-scene context per specimen, stepped in turn
+    # looped plain step, in its strongest form: one single-scene context per
+    # specimen, each stepping its `lsteps` steps as one dem_step call (one
+    # graph launch of the device-side step loop), specimens one after another
     sample = specimens[::max(1, num // loop_sample)]
     sims = []
     for sc in sample:
@@ -275,25 +280,42 @@ def measure_batched(steps: int, warmup: int, num: int = 4096, loop_sample: int =
         sim.set_state(t(sc.pos), t(sc.vel), t(sc.theta), t(sc.omega), t(sc.radius), t(sc.mass),
                       t(sc.id))
         sim.step(3)
+        sim.step(2)  # the step loop's graphs of both parities, captured untimed
+        sim.step(1)
+        sim.step(2)
         sims.append(sim)
     torch.cuda.synchronize()
-    lsteps = max(3, min(steps, 20))
+    lsteps = max(4, min(steps, 500))
     e0.record()
-    for _ in range(lsteps):
+    for sim in sims:
+        sim.step(lsteps)
+    e1.record()
+    torch.cuda.synchronize()
+    sample_n = sum(sc.n for sc in sample)
+    looped = sample_n * lsteps / (e0.elapsed_time(e1) * 1e-3)
+    # the weaker form measured before: single-step calls interleaved across
+    # the contexts (two graph launches per specimen-step)
+    isteps = 20
+    e0.record()
+    for _ in range(isteps):
         for sim in sims:
             sim.step(1)
     e1.record()
     torch.cuda.synchronize()
-    looped = sum(sc.n for sc in sample) * lsteps / (e0.elapsed_time(e1) * 1e-3)
+    interleaved = sample_n * isteps / (e0.elapsed_time(e1) * 1e-3)
     for sim in sims:
         sim.close()
     return {"metric": "aggregate particle-steps/s, batched vs looped plain",
             "value": batched, "looped_plain": looped, "ratio": batched / looped,
+            "looped_plain_interleaved_single_steps": interleaved,
+            "ratio_vs_interleaved": batched / interleaved,
             "unit": UNIT, "specimens": num, "particles": total, "steps": steps,
             "kernels_per_step": kernels,
             "graph_launches": 1 if steps % 2 == 0 else 2,
             "step_kernel_shape": [shape["threads"], shape["blocks_per_sm"]],
-            "looped_sample": "%d of the %d specimens (every %d-th), %d steps each"
+            "looped_sample": "%d of the %d specimens (every %d-th), each its own context "
+                             "stepping %d steps as one dem_step call (device-side step "
+                             "loop), one specimen after another"
                              % (len(sample), num, max(1, num // loop_sample), lsteps),
             "workload": "batched: specimens with counts log-uniform in [256, 8192], square "
                         "walled boxes at area fraction 0.5, radii U[0.9, 1.1] mm, kn "
@@ -540,6 +562,11 @@ def main():
     # still needs run here, untimed
     while sim.step_variant()["tuned"] < 0:
         sim.step(1)
+    # the device-side step loop's graphs of both parities (a multi-step call
+    # starting on an even and on an odd step) are captured here, untimed
+    sim.step(2)
+    sim.step(1)
+    sim.step(2)
     torch.cuda.synchronize()
     sim.check()
     kernels_per_step = sim.kernels_per_step()
@@ -547,16 +574,28 @@ def main():
 
     # ---- timed region (device-resident state): the K steps as one dem_step
     # call, which the library runs as one graph launch of its device-side
-    # step loop
+    # step loop.  The K-step call is repeated, each repeat bracketed by a
+    # barrier and a synchronize, until at least MIN_TIMED_S of device time is
+    # under load; `value` is from the median repeat (max over ranks).
     clocks = Clocks(local)
-    barrier()
-    torch.cuda.synchronize()
-    clocks.start()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-    ev[0].record(stream)
-    sim.step(args.steps)
-    ev[1].record(stream)
-    torch.cuda.synchronize()
+    clocks.start()
+    reps = []
+    target = None
+    while target is None or len(reps) < target:
+        barrier()
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        sim.step(args.steps)
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        reps.append(ev[0].elapsed_time(ev[1]))
+        if target is None:
+            first = torch.tensor([reps[0]], device="cuda")
+            if dist is not None:
+                dist.all_reduce(first, op=dist.ReduceOp.MAX)
+            target = int(min(MAX_REPEATS, max(MIN_REPEATS,
+                                              np.ceil(1e3 * MIN_TIMED_S / float(first.item())))))
     # ---- stage timing: K more steps, launched one step at a time with CUDA
     # events around each stage (events cannot sit inside the device-side
     # loop); the roofline's kernel duration comes from this pass
@@ -570,12 +609,14 @@ def main():
     ms = (C.c_float * D._lib.NUM_STAGES)()
     nprof = C.c_uint32(0)
     D.check(D.load().dem_profile_end(sim.handle, ms, C.byref(nprof)))
-    elapsed, elapsed_staged = ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3])
+    elapsed_staged = ev[2].elapsed_time(ev[3])
     barrier()
+    t = torch.tensor(reps + [elapsed_staged], device="cuda", dtype=torch.float64)
     if dist is not None:
-        t = torch.tensor([elapsed, elapsed_staged], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed, elapsed_staged = float(t[0].item()), float(t[1].item())
+    t = t.cpu().numpy()
+    reps, elapsed_staged = t[:-1], float(t[-1])
+    elapsed = float(np.median(reps))
     sim.check()
     value = n * world * args.steps / (elapsed * 1e-3)
     # kernels of the timed call: every step's, plus the loop's init kernel and
@@ -704,6 +745,10 @@ def main():
                                     "K steps (stage timing: a second pass of K steps, two "
                                     "graph launches per step)"),
                 "ms_per_step_stage_timed": elapsed_staged / args.steps,
+                "timed_repeats": {"count": int(len(reps)), "statistic": "median",
+                                  "timed_s": float(np.sum(reps)) * 1e-3,
+                                  "ms_per_step_min": float(np.min(reps)) / args.steps,
+                                  "ms_per_step_max": float(np.max(reps)) / args.steps},
                 "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved,
                              "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                              "peak_kind": kind, "traffic": traffic,

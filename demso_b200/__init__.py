@@ -420,12 +420,14 @@ class Batch(Simulation):
         self.num_specimens = len(specs)
         self.materials_max = max(len(sys.materials) for sys, _ in specs)
 
-    def set_systems(self, systems) -> None:
-        """New parameters for every specimen (same grids and counts)."""
+    def set_systems(self, systems, stream=None) -> None:
+        """New parameters for every specimen (same grids and counts), copied
+        on `stream` (default: torch's current stream) after the steps already
+        queued there."""
         arr = (_lib.DemSystem * len(systems))()
         for k, sys in enumerate(systems):
             arr[k] = sys.to_c(int(self.specs[k][1]))
-        check(load().dem_batch_set_systems(self._h, arr, len(systems)))
+        check(load().dem_batch_set_systems(self._h, arr, len(systems), _stream(stream)))
         self.specs = [(sys, n) for sys, (_, n) in zip(systems, self.specs)]
 
     def slots(self, s: int):

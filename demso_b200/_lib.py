@@ -95,7 +95,7 @@ SIGNATURES = [
     ("dem_create", C.c_int, [_SYS, _U, _U, C.POINTER(_P)]),
     ("dem_batch_create", C.c_int, [_SYS, _U, _U, C.POINTER(_P)]),
     ("dem_batch_specimen", C.c_int, [_P, _U, C.POINTER(_U), C.POINTER(_U)]),
-    ("dem_batch_set_systems", C.c_int, [_P, _P, _U]),
+    ("dem_batch_set_systems", C.c_int, [_P, _P, _U, _P]),
     ("dem_destroy", C.c_int, [_P]),
     ("dem_set_system", C.c_int, [_P, _SYS]),
     ("dem_set_state", C.c_int, [_P, _U] + [_P] * 8 + [C.c_int, _P]),

@@ -984,7 +984,7 @@ extern "C" int dem_set_system(DemContext* c, const DemSystem* sys) {
 }
 
 extern "C" int dem_batch_set_systems(DemContext* c, const DemSystem* specs,
-                                     uint32_t numSpecimens) {
+                                     uint32_t numSpecimens, void* stream) {
     if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
     if (!c->nspec) return fail(DEM_ERR_INVALID_ARG, "not a batch; use dem_set_system");
     if (!specs || numSpecimens != c->nspec)
@@ -1008,8 +1008,10 @@ extern "C" int dem_batch_set_systems(DemContext* c, const DemSystem* specs,
         if (attract && c->P.at[0] == 0.0f)
             return fail(DEM_ERR_INVALID_ARG, "specimen %u: attraction was off at create", s);
     }
-    DEM_TRY_CUDA(cudaMemcpy(c->dTable, table.data(), sizeof(KParams) * c->nspec,
-                            cudaMemcpyHostToDevice),
+    // ordered on the caller's stream after the steps already queued there,
+    // which read the table; the source is staged before the call returns
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->dTable, table.data(), sizeof(KParams) * c->nspec,
+                                 cudaMemcpyHostToDevice, (cudaStream_t)stream),
                  "batch table");
     c->hTable.swap(table);
     // keys depend on the boxes; recompute them and sort from scratch
@@ -1458,7 +1460,7 @@ extern "C" int dem_render(DemContext* c, const DemRenderParams* rp, void* image,
 
 extern "C" int dem_set_control(DemContext* c, const DemControl* ctl, void* stream) {
     if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
-    (void)stream;
+    cudaStream_t st = (cudaStream_t)stream;
     if (!ctl) {
         if (c->ctlOn) {
             c->ctlOn = false;
@@ -1477,7 +1479,7 @@ extern "C" int dem_set_control(DemContext* c, const DemControl* ctl, void* strea
         const size_t blocks = (cap + 511) / 512 + 1;
         const size_t bytes = al256(sizeof(ControlDev)) + al256(12 * cap) + al256(12 * blocks) + 256;
         DEM_TRY_CUDA(cudaMalloc(&c->ctlBlock, bytes), "cudaMalloc control particle");
-        DEM_TRY_CUDA(cudaMemset(c->ctlBlock, 0, bytes), "clear control particle");
+        DEM_TRY_CUDA(cudaMemsetAsync(c->ctlBlock, 0, bytes, st), "clear control particle");
         char* q = static_cast<char*>(c->ctlBlock);
         c->dCtl = reinterpret_cast<ControlDev*>(q); q += al256(sizeof(ControlDev));
         c->ctlVec = reinterpret_cast<float*>(q); q += al256(12 * cap);
@@ -1497,7 +1499,11 @@ extern "C" int dem_set_control(DemContext* c, const DemControl* ctl, void* strea
     d.wrapYTo = ctl->wrapYTo;
     d.wrapXAbove = ctl->wrapXAbove;
     d.wrapXTo = ctl->wrapXTo;
-    DEM_TRY_CUDA(cudaMemcpy(c->dCtl, &d, sizeof(d), cudaMemcpyHostToDevice), "set control");
+    // ordered on the caller's stream after the steps already queued there,
+    // which read and move the control particle; the source is staged before
+    // the call returns
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->dCtl, &d, sizeof(d), cudaMemcpyHostToDevice, st),
+                 "set control");
     if (!c->ctlOn) {
         c->ctlOn = true;
         drop_graphs(c);

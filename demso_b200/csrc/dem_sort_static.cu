@@ -43,7 +43,9 @@ static __device__ __align__(256) unsigned char g_sortScratch[kStaticSortScratchB
 
 // Device address of g_sortScratch, looked up once per device.  In host code
 // the symbol names a host-side stand-in, not device memory, so the kernels
-// must be given this address instead.
+// must be given this address instead.  It is kept for the life of the
+// process, so a device reset after the first call (which would free the
+// module's memory and load it again elsewhere) is not supported.
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 void* g_scratchPtr[kMaxDevices] = {};

@@ -118,7 +118,10 @@ int dem_sort_particles(uint32_t* gridParticleHash, uint32_t* gridParticleIndex,
  * (about 2.6 MB, held on every GPU that loads the library until exit), so at
  * most 262,144 pairs per call; larger calls fail with DEM_ERR_CAPACITY.
  * Allocates nothing.  The first call on a device looks up that array's
- * device address; make that first call before any stream capture.  All calls
+ * device address and keeps it for the life of the process; make that first
+ * call before any stream capture.  A device reset after it (cudaDeviceReset,
+ * or a reset of the primary context by other code in the process) is not
+ * supported: the kept address would be stale.  All calls
  * share the array: calls that overlap on the GPU race and must be ordered on
  * one stream or synchronised. */
 int dem_sort_particles_static(uint32_t* gridParticleHash, uint32_t* gridParticleIndex,
@@ -208,9 +211,12 @@ int dem_batch_create(const DemSystem* specs, uint32_t numSpecimens, uint32_t fla
 int dem_batch_specimen(DemContext* ctx, uint32_t specimen, uint32_t* firstSlot, uint32_t* count);
 /* Replaces every specimen's parameters (box, gravity, time step, wall and
  * contact coefficients) of a batch; grid sizes, particle counts and the
- * material layout stay those of dem_batch_create.  The next dem_step sorts
- * from scratch.  No reference counterpart. */
-int dem_batch_set_systems(DemContext* ctx, const DemSystem* specs, uint32_t numSpecimens);
+ * material layout stay those of dem_batch_create.  The new table is copied
+ * on `stream`, after the steps already queued there, so steps issued before
+ * the call use the old parameters and steps issued after it the new ones.
+ * The next dem_step sorts from scratch.  No reference counterpart. */
+int dem_batch_set_systems(DemContext* ctx, const DemSystem* specs, uint32_t numSpecimens,
+                          void* stream);
 
 /* Copies out the current state in its current (cell-sorted) order, plus loc
  * (indexed by id) and, when requested at create time, pressure/acc/alpha of
@@ -292,7 +298,13 @@ int dem_get_followed_async(DemContext* ctx, const uint32_t* ids, uint32_t count,
  * copies are queued on `stream`: with pinned or device memory the rows are
  * complete once `stream` has synchronised (pageable memory is written before
  * each copy returns).  Bit for bit the rows and state of nsteps calls of
- * dem_step(ctx, 1) each followed by dem_get_followed. */
+ * dem_step(ctx, 1) each followed by dem_get_followed.  The device copy of
+ * the ids and the ring grow to the largest call so far: a call that needs
+ * more of either than every earlier call frees and allocates them again
+ * (cudaFree/cudaMalloc, which can wait for the device) and captures the
+ * step loop's graphs again; a call no larger than an earlier one allocates
+ * nothing.  Callers whose id count varies can make one call with the largest
+ * count first. */
 int dem_step_followed(DemContext* ctx, uint32_t nsteps, const uint32_t* ids, uint32_t count,
                       float* rows, void* stream);
 
@@ -334,7 +346,8 @@ typedef struct DemControl {
     double wrapYBelow, wrapYTo;
     double wrapXAbove, wrapXTo;
 } DemControl;
-/* Sets (or, with NULL, removes) the control particle. */
+/* Sets (or, with NULL, removes) the control particle.  The new state is
+ * copied on `stream`, after the steps already queued there. */
 int dem_set_control(DemContext* ctx, const DemControl* control, void* stream);
 /* Its current state and the reaction (fx, fy, moment) of the last step;
  * synchronises `stream`.  Either output may be NULL. */

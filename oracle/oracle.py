@@ -117,13 +117,27 @@ def orc_control(ctl: dict) -> OrcControl:
     return c
 
 
-def build(ref_root: Optional[str] = None, quiet: bool = True) -> None:
+# Where this build container mounts the reference checkout; the REF_ROOT
+# environment variable overrides it.
+_DEFAULT_REF_ROOT = "/root/reference"
+
+
+def ref_root() -> Optional[str]:
+    """The reference checkout: $REF_ROOT, else the container's mount point;
+    None when neither holds the reference's sources."""
+    root = os.environ.get("REF_ROOT") or _DEFAULT_REF_ROOT
+    return root if os.path.isfile(os.path.join(root, "src", "particles_kernel.cuh")) else None
+
+
+def build(ref_root_dir: Optional[str] = None, quiet: bool = True) -> None:
     """Compile the oracles (and the reference host build when its tree exists)."""
     targets = ["all"]
-    root = ref_root or "/root/reference"
-    if os.path.isfile(os.path.join(root, "src", "particles_kernel.cuh")):
+    root = ref_root_dir or ref_root()
+    args = []
+    if root:
         targets.append("ref")
-    subprocess.run(["make", "-C", HERE, "REF_ROOT=" + root] + targets, check=True,
+        args.append("REF_ROOT=" + root)
+    subprocess.run(["make", "-C", HERE] + args + targets, check=True,
                    stdout=subprocess.DEVNULL if quiet else None)
 
 

@@ -12,11 +12,12 @@ import pytest
 
 from demso_b200 import dsml, scenes
 from demso_b200._lib import DemError
-from oracle.oracle import RefDsml, dsml_ref_available
+from oracle.oracle import RefDsml, dsml_ref_available, ref_root
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 FIXTURE = os.path.join(HERE, "golden", "dsml", "blocks.dsml")
-EXAMPLES = sorted(glob.glob("/root/reference/exemplos/*.dsml"))
+# the reference's example scenes, where its checkout is present ($REF_ROOT)
+EXAMPLES = sorted(glob.glob(os.path.join(ref_root(), "exemplos", "*.dsml"))) if ref_root() else []
 need_ref = pytest.mark.skipif(not dsml_ref_available(), reason="reference host build absent")
 
 

@@ -87,3 +87,45 @@ def test_generated_batch_matches_single_scene_contexts():
         ref = gpu_run(sc.sys, sc.state(), 120)
         for k in KEYS:
             assert same(out[k][a:b], ref[k]), (sc.name, k)
+
+
+def test_set_systems_is_ordered_on_the_callers_stream():
+    """Batch steps queued on a side stream, new specimen parameters set on
+    that stream while they may still run, then more steps: the result equals
+    the same sequence on the default stream, and differs from never changing
+    the parameters."""
+    import copy
+    import torch
+    import demso_b200 as D
+    specimens = scenes.specimen_batch(num=64, seed=5, nmin=2048, nmax=8192)
+    st = scenes.concat_specimens(specimens)
+    changed = []
+    for sc in specimens:
+        s = copy.deepcopy(sc.sys)
+        s.materials[0].normalStiffness *= 3.0
+        s.gravity = (2.0, -9.81)
+        changed.append(s)
+
+    def run(stream, change=True):
+        b = D.Batch([(sc.sys, sc.n) for sc in specimens], flags=D.CTX_PRESSURE)
+        b.set_state(_torch(st["pos"]), _torch(st["vel"]), _torch(st["theta"]),
+                    _torch(st["omega"]), _torch(st["radius"]), _torch(st["mass"]),
+                    _torch(st["id"]))
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            b.step(1)
+            b.step(300)
+            if change:
+                b.set_systems(changed)
+            b.step(30)
+        stream.synchronize()
+        out = {k: (None if v is None else v.numpy()) for k, v in b.get_state("cpu").items()}
+        b.close()
+        return out
+
+    a = run(torch.cuda.current_stream())
+    c = run(torch.cuda.Stream())
+    for k in KEYS:
+        assert same(a[k], c[k]), k
+    u = run(torch.cuda.current_stream(), change=False)
+    assert not same(a["pos"], u["pos"])

@@ -94,3 +94,36 @@ def test_control_particle_rejections():
     with pytest.raises(D.DemError):
         sim.control()                                       # none set
     sim.close()
+
+
+def test_set_control_is_ordered_on_the_callers_stream():
+    """Steps queued on a side stream (torch streams are non-blocking), then a
+    new control particle set on that stream while they may still run, then
+    more steps: the result equals the same sequence on the default stream."""
+    import torch
+    sc = scenes.agitated_gas(n=200000, seed=73, vel_std=0.3)
+    L = sc.sys.Lx
+    first = dict(pos=(0.3 * L, 0.5 * sc.sys.Ly), radius=5e-3, material=0, omega=1.0)
+    second = dict(pos=(0.7 * L, 0.4 * sc.sys.Ly), radius=8e-3, material=0, omega=-3.0)
+
+    def run(stream):
+        sim = _sim(sc)
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            sim.set_control(**first)
+            sim.step(1)
+            sim.step(200)
+            sim.set_control(**second)
+            sim.step(20)
+            p, r = sim.control()
+        stream.synchronize()
+        st = {k: (None if v is None else v.numpy()) for k, v in sim.get_state("cpu").items()}
+        sim.close()
+        return st, p, r
+
+    a = run(torch.cuda.current_stream())
+    b = run(torch.cuda.Stream())
+    for k in ("pos", "vel", "theta", "omega", "id"):
+        assert same(a[0][k], b[0][k]), k
+    assert np.array_equal(np.asarray(a[1], np.float32), np.asarray(b[1], np.float32))
+    assert np.array_equal(np.asarray(a[2], np.float32), np.asarray(b[2], np.float32))
