@@ -64,6 +64,8 @@ FUSED_MIN_BYTES_PER_PARTICLE = 88
 # Whole step, per particle: hash 16 + sort 52 + reorder 84 + collide 40 +
 # integrate 68 = 260, plus 20 per cell (reorder 12, collide 8).
 WHOLE_STEP_BYTES = lambda n, c: 260.0 * n + 20.0 * c  # whole-step model, per step
+# the plain-at-scale sizes of the roofline curve (the same workload scaled)
+DEFAULT_SWEEP = "65536,262144,1048576,4194304,16777216"
 # the timed K-step call is repeated until this much device time is under load
 MIN_TIMED_S = 1.0
 MIN_REPEATS, MAX_REPEATS = 3, 5000
@@ -513,9 +515,9 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-pile", action="store_true")
-    ap.add_argument("--sweep", default=None,
-                    help="comma-separated sizes of the plain-at-scale sweep (e.g. "
-                         "65536,262144,1048576,4194304,16777216)")
+    ap.add_argument("--sweep", default=DEFAULT_SWEEP,
+                    help="comma-separated sizes of the plain-at-scale sweep, 200 steps each "
+                         "(default: %s; empty for none)" % DEFAULT_SWEEP)
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the step kernel's default launch shape (128 threads x 8 "
                          "blocks per SM) instead of timing the shapes on the first steps")

@@ -103,6 +103,9 @@ SIGNATURES = [
     ("dem_step", C.c_int, [_P, _U, _P]),
     ("dem_get_cells", C.c_int, [_P, _P, _P, _P]),
     ("dem_check", C.c_int, [_P, _P]),
+    ("dem_debug_fail_allocation", C.c_int, [C.c_int]),
+    ("dem_debug_live_allocations", C.c_longlong, []),
+    ("dem_debug_sort_hold", C.c_int, [_P, _U, _U]),
     ("dem_kernels_per_step", C.c_int, [_P]),
     ("dem_set_step_variant", C.c_int, [_P, C.c_int32]),
     ("dem_get_step_variant", C.c_int, [_P, C.POINTER(DemStepVariant)]),

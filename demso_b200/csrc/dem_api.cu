@@ -2,6 +2,7 @@
 // per-stage entry points, and the context that runs the fused, graph-captured
 // step on library-owned buffers.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -34,6 +35,35 @@ int fail(int code, const char* fmt, ...) {
 int cuda_fail(cudaError_t e, const char* what) {
     return fail(e == cudaErrorMemoryAllocation ? DEM_ERR_NO_MEMORY : DEM_ERR_CUDA, "%s: %s", what,
                 cudaGetErrorString(e));
+}
+
+// Every device allocation of the contexts goes through dev_alloc/dev_free,
+// which count the allocations held and can be told to fail one
+// (dem_debug_fail_allocation), so that tests can check that a failed create
+// releases everything it took.
+std::atomic<long long> g_liveAllocs{0};
+std::atomic<int> g_failCountdown{0};
+
+template <typename T>
+cudaError_t dev_alloc(T** p, size_t bytes) {
+    *p = nullptr;
+    int k = g_failCountdown.load();
+    while (k > 0 && !g_failCountdown.compare_exchange_weak(k, k - 1)) {
+    }
+    if (k == 1) return cudaErrorMemoryAllocation;  // the injected failure
+    void* q = nullptr;
+    const cudaError_t e = cudaMalloc(&q, bytes);
+    if (e == cudaSuccess) {
+        *p = static_cast<T*>(q);
+        ++g_liveAllocs;
+    }
+    return e;
+}
+
+void dev_free(void* p) {
+    if (!p) return;
+    cudaFree(p);
+    --g_liveAllocs;
 }
 
 #define DEM_TRY_CUDA(expr, what)                          \
@@ -825,8 +855,8 @@ extern "C" int dem_batch_create(const DemSystem* specs, uint32_t numSpecimens, u
     std::vector<uint32_t> slotSpec(total);
     for (uint32_t s = 0; s < numSpecimens; ++s)
         for (uint32_t k = c->partOff[s]; k < c->partOff[s + 1]; ++k) slotSpec[k] = s;
-    cudaError_t e = cudaMalloc(&c->dTable, sizeof(KParams) * numSpecimens);
-    if (e == cudaSuccess) e = cudaMalloc(&c->spec, sizeof(uint32_t) * total);
+    cudaError_t e = dev_alloc(&c->dTable, sizeof(KParams) * numSpecimens);
+    if (e == cudaSuccess) e = dev_alloc(&c->spec, sizeof(uint32_t) * total);
     if (e == cudaSuccess)
         e = cudaMemcpy(c->dTable, c->hTable.data(), sizeof(KParams) * numSpecimens,
                        cudaMemcpyHostToDevice);
@@ -873,13 +903,13 @@ int init_context(DemContext* c, uint32_t capacity, uint32_t numCells, DemContext
     total += 256;                                // step-loop counters
     const size_t sortBytes = onesweep_scratch_bytes(capacity, c->keyBits);
     const size_t incBytes = incsort_bytes(capacity, c->numCells, nullptr);
-    cudaError_t e = cudaMalloc(&c->block, total);
-    if (e == cudaSuccess) e = cudaMalloc(&c->sortScratch, sortBytes);
-    if (e == cudaSuccess) e = cudaMalloc(&c->incScratch, incBytes);
+    cudaError_t e = dev_alloc(&c->block, total);
+    if (e == cudaSuccess) e = dev_alloc(&c->sortScratch, sortBytes);
+    if (e == cudaSuccess) e = dev_alloc(&c->incScratch, incBytes);
     if (e != cudaSuccess) {
-        cudaFree(c->incScratch);
-        cudaFree(c->sortScratch);
-        cudaFree(c->block);
+        dev_free(c->incScratch);
+        dev_free(c->sortScratch);
+        dev_free(c->block);
         delete c;
         return cuda_fail(e, "cudaMalloc context");
     }
@@ -911,6 +941,7 @@ int init_context(DemContext* c, uint32_t capacity, uint32_t numCells, DemContext
     c->loopCtl = reinterpret_cast<uint32_t*>(take(256));
     c->ss = carve_onesweep_scratch(c->sortScratch, capacity, c->keyBits);
     c->inc = carve_incsort(c->incScratch, capacity, c->numCells);
+    c->inc.errFlag = c->errFlag;
     e = cudaMemset(c->block, 0, total);
     if (e == cudaSuccess) e = cudaMemset(c->incScratch, 0, incBytes);
     for (int s = 0; s < 2 && e == cudaSuccess; ++s)
@@ -928,9 +959,9 @@ int init_context(DemContext* c, uint32_t capacity, uint32_t numCells, DemContext
         if (c->forkStream) cudaStreamDestroy(c->forkStream);
         if (c->bodyStream) cudaStreamDestroy(c->bodyStream);
         if (c->capStream) cudaStreamDestroy(c->capStream);
-        cudaFree(c->incScratch);
-        cudaFree(c->sortScratch);
-        cudaFree(c->block);
+        dev_free(c->incScratch);
+        dev_free(c->sortScratch);
+        dev_free(c->block);
         delete c;
         return cuda_fail(e, "context init");
     }
@@ -949,17 +980,17 @@ extern "C" int dem_destroy(DemContext* c) {
     if (c->loopStream) cudaStreamDestroy(c->loopStream);
     if (c->forkEv) cudaEventDestroy(c->forkEv);
     if (c->joinEv) cudaEventDestroy(c->joinEv);
-    cudaFree(c->followRows);
-    cudaFree(c->followIds);
-    cudaFree(c->followRing);
-    cudaFree(c->adjCheck);
-    cudaFree(c->renderOwner);
-    cudaFree(c->ctlBlock);
-    cudaFree(c->dTable);
-    cudaFree(c->spec);
-    cudaFree(c->incScratch);
-    cudaFree(c->sortScratch);
-    cudaFree(c->block);
+    dev_free(c->followRows);
+    dev_free(c->followIds);
+    dev_free(c->followRing);
+    dev_free(c->adjCheck);
+    dev_free(c->renderOwner);
+    dev_free(c->ctlBlock);
+    dev_free(c->dTable);
+    dev_free(c->spec);
+    dev_free(c->incScratch);
+    dev_free(c->sortScratch);
+    dev_free(c->block);
     delete c;
     return DEM_OK;
 }
@@ -1034,6 +1065,8 @@ extern "C" int dem_set_state(DemContext* c, uint32_t n, const float* pos, const 
     if (c->typed && n && !type)
         return fail(DEM_ERR_INVALID_ARG, "type array required with more than one material");
     cudaStream_t st = (cudaStream_t)stream;
+    // the new state replaces the one any recorded error was about
+    DEM_TRY_CUDA(cudaMemsetAsync(c->errFlag, 0, 4, st), "clear error word");
     const cudaMemcpyKind k = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
     const int a = c->cur;
     DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[0].pos, pos, 8ull * n, k, st), "set pos");
@@ -1276,6 +1309,22 @@ extern "C" int dem_check(DemContext* c, void* stream) {
     return DEM_OK;
 }
 
+extern "C" int dem_debug_fail_allocation(int nth) {
+    if (nth < 0) return fail(DEM_ERR_INVALID_ARG, "nth must be >= 0");
+    g_failCountdown.store(nth);
+    return DEM_OK;
+}
+
+extern "C" long long dem_debug_live_allocations(void) { return g_liveAllocs.load(); }
+
+extern "C" int dem_debug_sort_hold(DemContext* c, uint32_t holdTile, uint32_t spinLimit) {
+    if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    c->ss.holdTile = holdTile;
+    c->ss.spinLimit = spinLimit ? spinLimit : kSortSpinLimit;
+    drop_graphs(c);  // the sort's kernels take both as launch parameters
+    return DEM_OK;
+}
+
 extern "C" int dem_kernels_per_step(DemContext* c) {
     if (!c) return -1;
     if (!c->sortGraph[1][0] && c->n > 0) {
@@ -1293,7 +1342,7 @@ int get_followed(DemContext* c, const uint32_t* ids, uint32_t count, float* rows
     for (uint32_t i = 0; i < count; ++i)
         if (ids[i] >= c->n) return fail(DEM_ERR_INVALID_ARG, "followed id %u >= n %u", ids[i], c->n);
     if (!c->followRows) {
-        DEM_TRY_CUDA(cudaMalloc(&c->followRows, sizeof(float) * 12 * kFollowBatch),
+        DEM_TRY_CUDA(dev_alloc(&c->followRows, sizeof(float) * 12 * kFollowBatch),
                      "cudaMalloc followed rows");
     }
     cudaStream_t st = (cudaStream_t)stream;
@@ -1346,18 +1395,18 @@ extern "C" int dem_step_followed(DemContext* c, uint32_t nsteps, const uint32_t*
         (uint32_t)std::min<size_t>(nsteps, std::max<size_t>(1, kFollowRingBytes / rowBytes));
     if (c->followIdsCap < count) {
         drop_loop_graphs(c);
-        cudaFree(c->followIds);
+        dev_free(c->followIds);
         c->followIds = nullptr;
         c->followIdsCap = 0;
-        DEM_TRY_CUDA(cudaMalloc(&c->followIds, 4ull * count), "cudaMalloc followed ids");
+        DEM_TRY_CUDA(dev_alloc(&c->followIds, 4ull * count), "cudaMalloc followed ids");
         c->followIdsCap = count;
     }
     if (c->followRingBytes < chunk * rowBytes) {
         drop_loop_graphs(c);
-        cudaFree(c->followRing);
+        dev_free(c->followRing);
         c->followRing = nullptr;
         c->followRingBytes = 0;
-        DEM_TRY_CUDA(cudaMalloc(&c->followRing, chunk * rowBytes), "cudaMalloc followed rows");
+        DEM_TRY_CUDA(dev_alloc(&c->followRing, chunk * rowBytes), "cudaMalloc followed rows");
         c->followRingBytes = chunk * rowBytes;
     }
     // the ids go through a library-owned host copy, so they are read before
@@ -1441,11 +1490,10 @@ extern "C" int dem_render(DemContext* c, const DemRenderParams* rp, void* image,
     if (!image) return fail(DEM_ERR_INVALID_ARG, "dem_render: NULL image");
     const size_t words = (size_t)rp->imageDIMx * rp->imageDIMy;
     if (c->renderOwnerWords < words) {
-        cudaFree(c->renderOwner);
-    cudaFree(c->ctlBlock);
+        dev_free(c->renderOwner);
         c->renderOwner = nullptr;
         c->renderOwnerWords = 0;
-        DEM_TRY_CUDA(cudaMalloc(&c->renderOwner, 4 * words), "cudaMalloc render scratch");
+        DEM_TRY_CUDA(dev_alloc(&c->renderOwner, 4 * words), "cudaMalloc render scratch");
         c->renderOwnerWords = words;
     }
     const int a = c->cur;
@@ -1478,7 +1526,7 @@ extern "C" int dem_set_control(DemContext* c, const DemControl* ctl, void* strea
         const size_t cap = c->capacity ? c->capacity : 1;
         const size_t blocks = (cap + 511) / 512 + 1;
         const size_t bytes = al256(sizeof(ControlDev)) + al256(12 * cap) + al256(12 * blocks) + 256;
-        DEM_TRY_CUDA(cudaMalloc(&c->ctlBlock, bytes), "cudaMalloc control particle");
+        DEM_TRY_CUDA(dev_alloc(&c->ctlBlock, bytes), "cudaMalloc control particle");
         DEM_TRY_CUDA(cudaMemsetAsync(c->ctlBlock, 0, bytes, st), "clear control particle");
         char* q = static_cast<char*>(c->ctlBlock);
         c->dCtl = reinterpret_cast<ControlDev*>(q); q += al256(sizeof(ControlDev));
@@ -1677,10 +1725,10 @@ extern "C" int dem_adj_forward(DemContext* c, uint32_t nsteps, uint32_t every, v
     const uint32_t windows = (nsteps + every - 1) / every;
     const size_t snap = snapshot_bytes(c->n);
     if (c->adjCheckBytes < snap * windows) {
-        cudaFree(c->adjCheck);
+        dev_free(c->adjCheck);
         c->adjCheck = nullptr;
         c->adjCheckBytes = 0;
-        DEM_TRY_CUDA(cudaMalloc(&c->adjCheck, snap * windows), "cudaMalloc checkpoints");
+        DEM_TRY_CUDA(dev_alloc(&c->adjCheck, snap * windows), "cudaMalloc checkpoints");
         c->adjCheckBytes = snap * windows;
     }
     for (uint32_t w = 0; w < windows; ++w) {
@@ -1719,10 +1767,10 @@ extern "C" int dem_adj_backward(DemContext* c, float* lamPos, float* lamVel, flo
                             al256(4ull * (ns + 1));
     char* rec = nullptr;
     char* tmp = nullptr;
-    DEM_TRY_CUDA(cudaMalloc(&rec, stepBytes * c->adjEvery), "cudaMalloc adjoint record");
-    cudaError_t e = cudaMalloc(&tmp, tmpBytes);
+    DEM_TRY_CUDA(dev_alloc(&rec, stepBytes * c->adjEvery), "cudaMalloc adjoint record");
+    cudaError_t e = dev_alloc(&tmp, tmpBytes);
     if (e != cudaSuccess) {
-        cudaFree(rec);
+        dev_free(rec);
         return cuda_fail(e, "cudaMalloc adjoint scratch");
     }
     char* q = tmp;
@@ -1813,8 +1861,8 @@ extern "C" int dem_adj_backward(DemContext* c, float* lamPos, float* lamVel, flo
     if (rc == DEM_OK && e == cudaSuccess)
         e = cudaMemcpyAsync(grad, sum, 8ull * DEM_ADJ_NUM_COEF * ns, cudaMemcpyDeviceToHost, st);
     if (rc == DEM_OK && e == cudaSuccess) e = cudaStreamSynchronize(st);
-    cudaFree(rec);
-    cudaFree(tmp);
+    dev_free(rec);
+    dev_free(tmp);
     if (rc) return rc;
     if (e != cudaSuccess) return cuda_fail(e, "adjoint backward");
     return DEM_OK;

@@ -91,8 +91,12 @@ __global__ void __launch_bounds__(kThreads)
 cells_reduce_kernel(const uint2* __restrict__ prevCells, const uint32_t* __restrict__ leavers,
                     const uint32_t* __restrict__ arrCnt, uint32_t numCells, uint32_t items,
                     unsigned long long* __restrict__ partials, uint32_t* __restrict__ ctrl,
-                    cudaGraphConditionalHandle full, int setFull) {
-    const bool needFull = ctrl[kCtrlNeedFull] != 0u;
+                    const uint32_t* __restrict__ errFlag, cudaGraphConditionalHandle full,
+                    int setFull) {
+    // after a sort wait gave up the previous order is not a permutation the
+    // incremental path can build on: sort from scratch instead
+    const bool needFull = ctrl[kCtrlNeedFull] != 0u ||
+                          (errFlag != nullptr && (*errFlag & kSortTimeoutBit) != 0u);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         ctrl[kCtrlPath] = needFull ? 1u : 0u;
         if (setFull) cudaGraphSetConditional(full, needFull ? 1u : 0u);
@@ -277,15 +281,19 @@ __global__ void cell_first_kernel(const uint32_t* __restrict__ sortedKey, uint32
 
 // Full path, after the radix sort: cell ranges from the sorted keys, the
 // gather by the sorted indices, and the sorted keys kept for the next step.
+// Keys and indices are clamped to the cell and particle counts: they always
+// are in range unless a wait of the sort gave up (kSortTimeoutBit), when the
+// sort's output may hold stale words; the clamps keep every access in bounds
+// then (the state is invalid and dem_check says so).
 __global__ void __launch_bounds__(kThreads)
-full_reorder_kernel(uint32_t n, const uint32_t* __restrict__ hash,
+full_reorder_kernel(uint32_t n, uint32_t numCells, const uint32_t* __restrict__ hash,
                     const uint32_t* __restrict__ index, uint2* __restrict__ cells,
                     uint32_t* __restrict__ newSortedKey, SortMove mv) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = i < n;
-    const uint32_t h = valid ? hash[i] : 0u;
+    const uint32_t h = valid ? min(hash[i], numCells - 1u) : 0u;
     uint32_t hp = __shfl_up_sync(0xffffffffu, h, 1);
-    if ((threadIdx.x & 31) == 0 && valid && i > 0) hp = hash[i - 1];
+    if ((threadIdx.x & 31) == 0 && valid && i > 0) hp = min(hash[i - 1], numCells - 1u);
     if (!valid) return;
     if (i == 0 || h != hp) {
         cells[h].x = i;
@@ -293,7 +301,7 @@ full_reorder_kernel(uint32_t n, const uint32_t* __restrict__ hash,
     }
     if (i == n - 1) cells[h].y = i + 1;
     newSortedKey[i] = h;
-    move_particle(index[i], i, mv);
+    move_particle(min(index[i], n - 1u), i, mv);
 }
 
 }  // namespace
@@ -334,7 +342,7 @@ cudaError_t enqueue_incremental_head(const IncSort& s, const uint2* prevCells,
     if (nb > kMaxScanBlocks) return cudaErrorInvalidValue;
     cells_reduce_kernel<<<(unsigned)nb, kThreads, 0, st>>>(prevCells, s.leavers, s.arrCnt, C,
                                                            cell_items(C), s.partials, s.ctrl,
-                                                           full, setFull ? 1 : 0);
+                                                           s.errFlag, full, setFull ? 1 : 0);
     if (launches) ++*launches;
     return cudaGetLastError();
 }
@@ -378,7 +386,7 @@ cudaError_t enqueue_full(const IncSort& s, uint32_t n, uint32_t keyBits, uint32_
     if (e != cudaSuccess) return e;
     if (n) {
         full_reorder_kernel<<<blocks_for(n, kThreads), kThreads, 0, st>>>(
-            n, ko, vo, newCells, newSortedKey, mv);
+            n, s.numCells, ko, vo, newCells, newSortedKey, mv);
         if (launches) ++*launches;
     }
     cell_first_kernel<<<std::min<unsigned>(blocks_for((size_t)s.numCells + 1, kThreads), 148u * 8u),

@@ -63,6 +63,10 @@ struct IncSort {
     uint32_t* arrSlots = nullptr;  // moverCap
     unsigned long long* partials = nullptr;  // scan partials
     uint32_t* ctrl = nullptr;      // kCtrlNeedFull, kCtrlMovers, kCtrlPath
+    // the context's error word: while a sort wait has given up
+    // (kSortTimeoutBit), every step takes the full path, which needs no
+    // previous order (set by the context after carve_incsort)
+    const uint32_t* errFlag = nullptr;
 };
 
 size_t incsort_bytes(uint32_t n, uint32_t numCells, uint32_t* moverCapOut);

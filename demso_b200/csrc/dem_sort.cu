@@ -200,7 +200,6 @@ downsweep_kernel(const uint32_t* __restrict__ keysIn, const uint32_t* __restrict
 constexpr uint32_t kFlagAgg = 1u << 30;   // tile aggregate published
 constexpr uint32_t kFlagIncl = 2u << 30;  // inclusive prefix published
 constexpr uint32_t kValueMask = (1u << 30) - 1u;
-constexpr uint32_t kSpinLimit = 1u << 22;
 constexpr int kHistBlocksPerSM = 2;
 
 // Global digit histograms of every pass.  Each thread walks a run of
@@ -273,7 +272,8 @@ __global__ void __launch_bounds__(kSortThreads, 3)
 onesweep_kernel(const uint32_t* __restrict__ keysIn, const uint32_t* __restrict__ valsIn,
                 uint32_t* __restrict__ keysOut, uint32_t* __restrict__ valsOut, uint32_t n,
                 int shift, uint32_t rows, const uint32_t* __restrict__ gOffset,
-                uint32_t* __restrict__ lookback, uint32_t* __restrict__ errFlag) {
+                uint32_t* __restrict__ lookback, uint32_t* __restrict__ errFlag,
+                uint32_t holdTile, uint32_t spinLimit) {
     constexpr int R = 1 << BITS;
     __shared__ uint16_t cnt[kSortWarps][R];
     __shared__ uint32_t dbase[R];
@@ -321,7 +321,7 @@ onesweep_kernel(const uint32_t* __restrict__ keysIn, const uint32_t* __restrict_
             cnt[w][d] = (uint16_t)run;
             run += c;
         }
-        lb[(size_t)tile * rows + d] = (tile == 0 ? kFlagIncl : kFlagAgg) | run;
+        if (tile != holdTile) lb[(size_t)tile * rows + d] = (tile == 0 ? kFlagIncl : kFlagAgg) | run;
         dbase[d] = run;
     }
     // decoupled look-back: the tile's exclusive prefix of each digit
@@ -334,7 +334,7 @@ onesweep_kernel(const uint32_t* __restrict__ keysIn, const uint32_t* __restrict_
             while (true) {
                 const uint32_t v = lb[(size_t)t * rows + d];
                 if ((v & ~kValueMask) == 0u) {
-                    if (++spins > kSpinLimit) {
+                    if (++spins > spinLimit) {
                         atomicOr(errFlag, kSortTimeoutBit);
                         break;
                     }
@@ -345,7 +345,7 @@ onesweep_kernel(const uint32_t* __restrict__ keysIn, const uint32_t* __restrict_
                 if ((v & kFlagIncl) || t == 0) break;
                 --t;
             }
-            lb[(size_t)tile * rows + d] = kFlagIncl | (excl + run);
+            if (tile != holdTile) lb[(size_t)tile * rows + d] = kFlagIncl | (excl + run);
         }
         dbase[d] = gOffset[d] + excl;
     }
@@ -511,10 +511,12 @@ cudaError_t onesweep_impl(uint32_t* keys, uint32_t* vals, uint32_t n, const Sort
         const uint32_t* go = s.globalHist + (size_t)p * R;
         if (identityVals && p == 0)
             onesweep_kernel<BITS, true><<<numTiles, kSortThreads, 0, st>>>(
-                ki, vi, ko, vo, n, plan.shift[p], rows, go, s.lookback, errFlag);
+                ki, vi, ko, vo, n, plan.shift[p], rows, go, s.lookback, errFlag, s.holdTile,
+                s.spinLimit);
         else
             onesweep_kernel<BITS, false><<<numTiles, kSortThreads, 0, st>>>(
-                ki, vi, ko, vo, n, plan.shift[p], rows, go, s.lookback, errFlag);
+                ki, vi, ko, vo, n, plan.shift[p], rows, go, s.lookback, errFlag, s.holdTile,
+                s.spinLimit);
         if (launches) ++*launches;
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;

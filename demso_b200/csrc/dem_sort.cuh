@@ -59,12 +59,20 @@ cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_
 // every wait is bounded and, if it gives up, sets kSortTimeoutBit in
 // *errFlag and carries on (the result is then invalid, never a hang).
 constexpr uint32_t kSortTimeoutBit = 2u;
+// Iterations a look-back wait spins (with short sleeps) before it gives up.
+constexpr uint32_t kSortSpinLimit = 1u << 22;
+constexpr uint32_t kNoHeldTile = 0xffffffffu;
 
 struct OnesweepScratch {
     uint32_t* altKeys;    // n
     uint32_t* altVals;    // n
     uint32_t* globalHist; // passes * 2^maxBits (exclusive offsets after the scan)
     uint32_t* lookback;   // 1 counter word padded to 64, then numTiles * 2^maxBits
+    // Test hook (dem_debug_sort_hold): tile `holdTile` of every pass never
+    // publishes its counts, so the tile after it waits until `spinLimit`
+    // runs out; kNoHeldTile and kSortSpinLimit in normal use.
+    uint32_t holdTile = kNoHeldTile;
+    uint32_t spinLimit = kSortSpinLimit;
 };
 size_t onesweep_scratch_bytes(uint32_t n, uint32_t keyBits);
 OnesweepScratch carve_onesweep_scratch(void* base, uint32_t n, uint32_t keyBits);

@@ -261,8 +261,27 @@ int dem_get_step_variant(DemContext* ctx, DemStepVariant* out);
  * of numCells words each in the reference's layout (either may be NULL). */
 int dem_get_cells(DemContext* ctx, uint32_t* cellStart, uint32_t* cellEnd, void* stream);
 
-/* Reads the device error flag (synchronises `stream`): DEM_OK or DEM_ERR_OOB. */
+/* Reads the context's device error word (synchronises `stream`): DEM_OK;
+ * DEM_ERR_OOB when a position became NaN or infinite; DEM_ERR_TIMEOUT when a
+ * bounded wait of the sort gave up (the state is then invalid, though every
+ * access stayed in bounds, and every later step sorts from scratch until
+ * dem_set_state).  dem_set_state clears the word. */
 int dem_check(DemContext* ctx, void* stream);
+
+/* Test hooks, no reference counterpart.  They inject failures on the host or
+ * through bounded waits; none faults or hangs the GPU.
+ *  - dem_debug_fail_allocation(k): the k-th device allocation the contexts
+ *    make from now on fails as if the device had run out of memory (the
+ *    call then returns DEM_ERR_NO_MEMORY); 0 turns it off.
+ *  - dem_debug_live_allocations(): device allocations the contexts hold.
+ *  - dem_debug_sort_hold(ctx, tile, spinLimit): in the context's full sort,
+ *    tile `tile` of every pass never publishes its counts, so the tile after
+ *    it waits until its bounded wait runs out after `spinLimit` iterations
+ *    (0: the normal limit) and sets DEM_ERR_TIMEOUT; tile 0xFFFFFFFF holds
+ *    none (normal use). */
+int dem_debug_fail_allocation(int nth);
+long long dem_debug_live_allocations(void);
+int dem_debug_sort_hold(DemContext* ctx, uint32_t holdTile, uint32_t spinLimit);
 
 /* Number of kernels one dem_step(ctx, 1, ...) launches (library kernels
  * only; the cellStart memset is not counted). */

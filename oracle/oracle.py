@@ -427,6 +427,11 @@ class RefHarness:
         L.ref_run.argtypes = [u32] + [_f32p] * 4 + [_u32p] * 3 + [_f32p] * 4 + [_u32p] * 3 + \
             [_f32p, _f32p, _f32p, _u32p, _u32p, _u32p, _u32p]
         L.ref_max_particles.restype = C.c_int
+        L.ref_render.argtypes = [np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS"),
+                                 C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, _f32p,
+                                 _f32p, _f32p, C.c_void_p,
+                                 np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")]
+        L.ref_render.restype = C.c_int
         if control:
             f = C.c_float
             L.ref_set_control.argtypes = [f, f, f, f, f, f, f, f, _f32p]
@@ -524,6 +529,28 @@ class RefHarness:
                                np.ascontiguousarray(alpha, dtype=np.float32),
                                np.ascontiguousarray(ids, dtype=np.uint32), pr)
         return pos, vel, th, om, pr
+
+    def render(self, dimx, dimy, bg, view_rotations, by_pressure, max_pressure, rgb, pos, theta,
+               pressure=None):
+        """The reference's plotSpheresD over the particles of the last setup,
+        in index order, disks first and orientation lines after every disk;
+        rgb: (n, 3) colour of each particle.  Returns (image (dimy, dimx, 4)
+        uint8, mask (dimy, dimx) of the pixels whose line/disk class the
+        reference's output cannot decide: disk pixels of shade 0 under a
+        possible line)."""
+        img = np.zeros((dimy, dimx, 4), np.uint8)
+        amb = np.zeros((dimy, dimx), np.uint8)
+        pr = None if pressure is None else np.ascontiguousarray(pressure, dtype=np.float32)
+        k = self.lib.ref_render(img.reshape(-1), int(dimx), int(dimy), int(bg),
+                                int(bool(view_rotations)), int(bool(by_pressure)),
+                                float(max_pressure),
+                                np.ascontiguousarray(pos, dtype=np.float32).reshape(-1),
+                                np.ascontiguousarray(theta, dtype=np.float32),
+                                np.ascontiguousarray(rgb, dtype=np.float32).reshape(-1),
+                                pr.ctypes.data if pr is not None else None, amb.reshape(-1))
+        if k < 0:
+            raise ValueError("a particle's square reaches below pixel 0")
+        return img, amb.astype(bool)
 
     def make_buffers(self, st: dict):
         """Allocate the two state sets and scratch for ``run`` (kept out of timing)."""

@@ -25,6 +25,7 @@
  */
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -296,6 +297,99 @@ void ref_run(uint32_t nsteps,
         memcpy(type1, type2, sizeof(uint32_t) * n);
         memcpy(loc1, loc2, sizeof(uint32_t) * n);
     }
+}
+
+/* The reference's disk splat, plotSpheresD (particles_kernel.cuh:656-734),
+ * run one "CUDA thread" after the other in index order over the particles of
+ * the last ref_setup (particle i is reference type i), with the rule the
+ * library applies where the reference's threads race: a later particle's
+ * disk covers an earlier one's, and the orientation lines come after every
+ * disk.  `rgb` holds each particle's colour (3 floats), written into its
+ * type's colorR/G/B; `pressure` may be NULL (zeros).  The image (dimx *
+ * dimy RGBA bytes, row 0 at the bottom) is filled with bg first.
+ *
+ * The disks are one pass of calls with renderParD.viewRotations off.  The
+ * pixels of particle i's line are found by calling the kernel for it again
+ * twice over a scratch image filled with a sentinel, once with lines and
+ * once without: a pixel the call with lines leaves all-zero and the call
+ * without does not is a line pixel.  A pixel that the disk itself writes
+ * all-zero (shade below 1/255) and that the line call also leaves all-zero
+ * cannot be classed that way: such pixels are blackened and counted, and
+ * the count is returned (and the pixels flagged in ambiguousMask, dimx * dimy
+ * bytes, when it is not NULL).  Returns -1 when a particle's square reaches below
+ * pixel 0 (the reference then converts negative floats to unsigned, which
+ * the host does differently from the GPU). */
+int ref_render(uint8_t* image, int dimx, int dimy, int bg, int viewRotations,
+               int colorByPressure, float maxPressure, float* pos, float* theta,
+               const float* rgb, float* pressure, uint8_t* ambiguousMask) {
+    const uint n = sisPropD.numParticles;
+    const size_t size = (size_t)dimx * dimy;
+    renderParD.imageDIMx = dimx;
+    renderParD.imageDIMy = dimy;
+    renderParD.bgColor = bg;
+    renderParD.colorByPressure = colorByPressure != 0;
+    renderParD.maxPressure = maxPressure;
+    std::vector<uint> type(n);
+    std::vector<float> zeros;
+    if (!pressure) {
+        zeros.assign(n, 0.0f);
+        pressure = zeros.data();
+    }
+    for (uint i = 0; i < n; ++i) {
+        type[i] = i;
+        partPropD[i].colorR = rgb[3 * i];
+        partPropD[i].colorG = rgb[3 * i + 1];
+        partPropD[i].colorB = rgb[3 * i + 2];
+        const float pR = renderParD.imageDIMy / sisPropD.cubeDimension.y * partPropD[i].radius;
+        const int cx = renderParD.imageDIMx / sisPropD.cubeDimension.x * pos[2 * i];
+        const int cy = renderParD.imageDIMy / sisPropD.cubeDimension.y * pos[2 * i + 1];
+        if (cx - (int)ceilf(pR) < 0 || cy - (int)ceilf(pR) < 0) return -1;
+    }
+    uchar4* img = reinterpret_cast<uchar4*>(image);
+    const uchar4 bgc = make_uchar4(bg & 0xff, bg & 0xff, bg & 0xff, bg & 0xff);
+    for (size_t p = 0; p < size; ++p) img[p] = bgc;
+    renderParD.viewRotations = false;
+    for (uint i = 0; i < n; ++i) {
+        set_thread(i, n);
+        plotSpheresD(img, reinterpret_cast<float2*>(pos), theta, type.data(), pressure);
+    }
+    if (!viewRotations) return 0;
+    const uchar4 sentinel = make_uchar4(1, 2, 3, 4);
+    std::vector<uchar4> on(size, sentinel), off(size, sentinel);
+    std::vector<uint8_t> line(size, 0);
+    auto zero = [](uchar4 c) { return c.x == 0 && c.y == 0 && c.z == 0 && c.w == 0; };
+    int ambiguous = 0;
+    for (uint i = 0; i < n; ++i) {
+        const float pR = renderParD.imageDIMy / sisPropD.cubeDimension.y * partPropD[i].radius;
+        const int cx = renderParD.imageDIMx / sisPropD.cubeDimension.x * pos[2 * i];
+        const int cy = renderParD.imageDIMy / sisPropD.cubeDimension.y * pos[2 * i + 1];
+        const int h = (int)ceilf(pR);
+        // every pixel the call can write: its square, clamped to the last pixel
+        std::vector<size_t> px;
+        for (int y = cy - h; y < cy + h; ++y)
+            for (int x = cx - h; x < cx + h; ++x) {
+                size_t p = (size_t)(uint)x + (size_t)(uint)y * (uint)dimx;
+                px.push_back(p < size ? p : size - 1);
+            }
+        px.push_back(size - 1);
+        for (size_t p : px) on[p] = off[p] = sentinel;
+        set_thread(i, n);
+        renderParD.viewRotations = false;
+        plotSpheresD(off.data(), reinterpret_cast<float2*>(pos), theta, type.data(), pressure);
+        renderParD.viewRotations = true;
+        plotSpheresD(on.data(), reinterpret_cast<float2*>(pos), theta, type.data(), pressure);
+        for (size_t p : px) {
+            if (line[p] || !zero(on[p])) continue;
+            if (zero(off[p])) {
+                ++ambiguous;
+                if (ambiguousMask) ambiguousMask[p] = 1;
+            }
+            line[p] = 1;
+        }
+    }
+    for (size_t p = 0; p < size; ++p)
+        if (line[p]) img[p] = make_uchar4(0, 0, 0, 0);
+    return ambiguous;
 }
 
 /* The reference's block generators, one "CUDA thread" per particle:

@@ -12,14 +12,15 @@ Everything here runs on host cores from the CPU oracles (oracle/):
 * the same five derivatives from the FP64 tangent;
 * FP64 central differences (h = 1e-4 relative) of the FP64 oracle loss, with
   the branch signature of every run (whether a perturbation crossed a
-  contact, dashpot, slip, wall or floor branch of the unperturbed run).
+  contact, dashpot, slip, wall or floor branch of the unperturbed run), and
+  the same differences at h = 1e-6, 1e-8 and 1e-10 relative.
 
 The scene is fixed by its seed; its checksum is stored so that the test can
 confirm it generated the same initial state.  Run from the repository root:
 
     python tests/golden/make_adjoint_incline.py
 
-The runs are spread over a spawned process pool (about two minutes on eight
+The runs are spread over a spawned process pool (about six minutes on eight
 cores).
 """
 from __future__ import annotations
@@ -43,6 +44,9 @@ N, STEPS, EVERY = 16384, 2000, 100
 KN, ZETA, MU = 1e5, 0.3, 0.5
 DIR_SEEDS = (7, 8)
 H_REL = 1e-4
+# smaller steps of the FP64 central difference, to show where it stops
+# crossing branches and meets the FP64 tangent
+H_STUDY = (1e-6, 1e-8, 1e-10)
 OUT = os.path.join(HERE, "adjoint_incline_16k.json")
 
 
@@ -94,8 +98,9 @@ def main():
     jobs_t = [(p, w) for p in ("f32", "f64") for w in (0, 1)]
     jobs_l = [("kn", KN)]
     for name, x in base.items():
-        h = H_REL * x
-        jobs_l += [(name, x + h), (name, x - h)]
+        for hr in (H_REL,) + H_STUDY:
+            h = hr * x
+            jobs_l += [(name, x + h), (name, x - h)]
     ctx = mp.get_context("spawn")
     with ctx.Pool(min(len(jobs_t) + len(jobs_l), os.cpu_count() or 1)) as pool:
         rt = pool.map_async(_tangent, jobs_t)
@@ -109,13 +114,21 @@ def main():
         t[0:3] = d[0:3]
         t[3 + which] = d[3]
     base_loss, base_sig = [v for n_, x, v in losses if n_ == "kn" and x == KN][0]
-    fd, same = [], []
-    for name, x in base.items():
-        h = H_REL * x
-        (lp, sp), = [v for n_, xx, v in losses if n_ == name and xx == x + h]
-        (lm, sm), = [v for n_, xx, v in losses if n_ == name and xx == x - h]
-        fd.append((lp - lm) / (2.0 * h))
-        same.append(bool(sp == base_sig and sm == base_sig))
+    def central(hr):
+        fd, same = [], []
+        for name, x in base.items():
+            h = hr * x
+            (lp, sp), = [v for n_, xx, v in losses if n_ == name and xx == x + h]
+            (lm, sm), = [v for n_, xx, v in losses if n_ == name and xx == x - h]
+            fd.append((lp - lm) / (2.0 * h))
+            same.append(bool(sp == base_sig and sm == base_sig))
+        return fd, same
+
+    fd, same = central(H_REL)
+    study = []
+    for hr in H_STUDY:
+        f, sm_ = central(hr)
+        study.append({"h_rel": hr, "central_difference": f, "same_branches": sm_})
     out = {
         "workload": "differentiable: %d disks (radii U[0.9, 1.1] mm) released from a seeded "
                     "heap onto a 20-degree incline, %d steps, checkpoint every %d steps"
@@ -128,6 +141,7 @@ def main():
         "f64_tangent": tan["f64"]["d"], "f64_loss": tan["f64"]["loss"],
         "f64_loss_oracle": base_loss, "f64_signature": str(base_sig),
         "f64_central_difference": fd, "f64_fd_same_branches": same,
+        "f64_fd_step_study": study,
         "generated_s": round(time.time() - t0, 1),
     }
     with open(OUT, "w") as f:

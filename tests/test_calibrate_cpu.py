@@ -51,3 +51,34 @@ def test_column_specimens():
         assert np.all(d > s.radius[:, None] + s.radius[None, :])
         assert s.sys.gx >= 3 and s.sys.gy >= 3
         assert s.sys.Lx / s.sys.gx > 2 * 1.1e-3 and s.sys.Ly / s.sys.gy > 2 * 1.1e-3
+
+
+def test_profiles_conserve_area_and_differentiate():
+    """The column-height profile: every disk's area lands in its specimen's
+    bins (over bin width and packing), and autograd's dL/dx equals central
+    differences of the loss (the binning is piecewise linear)."""
+    import torch
+    sp = C.column_specimens(3, seed=5, nmin=200, nmax=400)
+    prof = C.Profiles(sp, "cpu")
+    x = torch.tensor(np.concatenate([s.pos[:, 0] for s in sp]), dtype=torch.float64)
+    h = prof(x)
+    r = np.concatenate([s.radius for s in sp]).astype(np.float64)
+    assert abs(float(h.sum()) * prof.bw * C.PACKING - np.pi * (r * r).sum()) < 1e-12
+    # per specimen: its disks only in its own bins
+    k = 0
+    for s in sp:
+        nb = int(np.ceil(s.sys.Lx / prof.bw))
+        hs = h[k:k + nb]
+        rs = s.radius.astype(np.float64)
+        assert abs(float(hs.sum()) * prof.bw * C.PACKING - np.pi * (rs * rs).sum()) < 1e-12
+        k += nb
+    rng = np.random.default_rng(1)
+    target = h + torch.tensor(rng.normal(scale=1e-3, size=h.shape[0]))
+    xs = (x + torch.tensor(rng.uniform(0, 5e-3, size=x.shape[0]))).requires_grad_(True)
+    prof.loss(prof(xs), target).backward()
+    for i in rng.choice(x.shape[0], size=8, replace=False):
+        e = torch.zeros_like(x)
+        e[i] = 1e-7
+        with torch.no_grad():
+            fd = (prof.loss(prof(xs + e), target) - prof.loss(prof(xs - e), target)) / 2e-7
+        assert abs(float(fd) - float(xs.grad[i])) <= 1e-6 * abs(float(fd)) + 1e-9

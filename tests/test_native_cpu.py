@@ -122,3 +122,11 @@ def test_batch_create_rejects_bad_specimens():
     assert lib.dem_batch_create(arr, 2, 0, C.byref(h)) == 1
     assert lib.dem_batch_create(None, 0, 0, C.byref(h)) == 1
     assert lib.dem_batch_specimen(None, 0, None, None) == 1
+
+
+def test_test_hooks_check_their_arguments():
+    lib = _lib.load()
+    assert lib.dem_debug_fail_allocation(-1) == 1
+    assert lib.dem_debug_fail_allocation(0) == 0
+    assert lib.dem_debug_live_allocations() == 0
+    assert lib.dem_debug_sort_hold(None, 0, 10) == 1

@@ -1,10 +1,13 @@
 """Headless output host logic: output.csv lines against the C printf
 restatement of the reference's writeOutputFile, the reference's elapsed-time
-and image-width arithmetic, and the PPM layout."""
+and image-width arithmetic, the PPM layout, and the CPU disk splat against
+the reference's own plotSpheresD built for the host."""
 import numpy as np
+import pytest
 
 from demso_b200 import output
-from oracle.oracle import RenderOracle
+from oracle.oracle import RenderOracle, ref_available
+from render_scenes import COLORS, reference_splat, splat_scene
 
 
 def test_followed_line_is_the_reference_format():
@@ -50,3 +53,21 @@ def test_render_oracle_draws_disks_and_lines():
     assert np.all(img[20, 15] == 0) and np.all(img[0, 0] == 0)
     covered = np.count_nonzero(img[..., 3])
     assert abs(covered + 4 - np.pi * 16) < 8
+
+
+@pytest.mark.skipif(not ref_available(), reason="reference host build absent")
+@pytest.mark.parametrize("seed", [0, 1, 2, 3])
+@pytest.mark.parametrize("lines,by_pressure", [(False, False), (True, False), (True, True)])
+def test_cpu_splat_is_the_reference_plotspheres(seed, lines, by_pressure):
+    """The restatement (oracle/dem_render.c) against the reference's own
+    plotSpheresD (particles_kernel.cuh:656-734) built for the host and run
+    in index order: equal everywhere except the few pixels whose disk/line
+    class the reference's output cannot decide (none without lines)."""
+    sc = splat_scene(seed)
+    ref, amb = reference_splat(sc, lines, by_pressure)
+    H = sc["height"]
+    mine = RenderOracle().render(H, H, 9, lines, by_pressure, 1.5, COLORS, 1.0, 1.0, sc["pos"],
+                                 sc["theta"], sc["type"], sc["radius"], sc["pressure"])
+    assert not lines or np.count_nonzero(np.all(ref == 0, axis=2)) > 5000
+    assert amb.sum() < 1e-4 * H * H and (lines or amb.sum() == 0)
+    assert np.array_equal(ref[~amb], mine[~amb])
