@@ -518,6 +518,9 @@ def main():
     ap.add_argument("--sweep", default=DEFAULT_SWEEP,
                     help="comma-separated sizes of the plain-at-scale sweep, 200 steps each "
                          "(default: %s; empty for none)" % DEFAULT_SWEEP)
+    ap.add_argument("--min-timed-s", type=float, default=MIN_TIMED_S,
+                    help="repeat the timed K-step call until this much device time is timed "
+                         "(at least %d repeats)" % MIN_REPEATS)
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the step kernel's default launch shape (128 threads x 8 "
                          "blocks per SM) instead of timing the shapes on the first steps")
@@ -597,7 +600,7 @@ def main():
             if dist is not None:
                 dist.all_reduce(first, op=dist.ReduceOp.MAX)
             target = int(min(MAX_REPEATS, max(MIN_REPEATS,
-                                              np.ceil(1e3 * MIN_TIMED_S / float(first.item())))))
+                                              np.ceil(1e3 * args.min_timed_s / float(first.item())))))
     # ---- stage timing: K more steps, launched one step at a time with CUDA
     # events around each stage (events cannot sit inside the device-side
     # loop); the roofline's kernel duration comes from this pass
@@ -662,38 +665,58 @@ def main():
         # buffer by one copy (dem_step_followed)
         rows = torch.zeros(args.steps * follow.size * 12, dtype=torch.float32).pin_memory()
         L = D.load()
+        p = lambda k: out_host[k].data_ptr()
+
+        def e2e_pass():
+            sim2.set_state(host["pos"], host["vel"], host["theta"], host["omega"],
+                           host["radius"], host["mass"], host["id"])
+            sim2.step_followed(args.steps, follow, rows)
+            D.check(L.dem_get_state(sim2.handle, p("pos"), p("vel"), p("theta"), p("omega"),
+                                    p("radius"), p("mass"), p("id"), None, None, None, None,
+                                    None, 1, D._stream()))
+            torch.cuda.synchronize()
+
         # warm-up outside the timed region: the step loop's graphs of both
-        # parities are captured here
+        # parities, and one whole pass of K steps (the followed-row ring grows
+        # to K steps and its loop graphs are captured)
         sim2.set_state(host["pos"], host["vel"], host["theta"], host["omega"], host["radius"],
                        host["mass"], host["id"])
         sim2.step_followed(3, follow, rows)
         sim2.step(1)
         sim2.step_followed(2, follow, rows)
-        torch.cuda.synchronize()
-        barrier()
-        t0 = time.perf_counter()
-        sim2.set_state(host["pos"], host["vel"], host["theta"], host["omega"], host["radius"],
-                       host["mass"], host["id"])
-        sim2.step_followed(args.steps, follow, rows)
-        p = lambda k: out_host[k].data_ptr()
-        D.check(L.dem_get_state(sim2.handle, p("pos"), p("vel"), p("theta"), p("omega"),
-                                p("radius"), p("mass"), p("id"), None, None, None, None, None, 1,
-                                D._stream()))
-        torch.cuda.synchronize()
-        e2e_s = time.perf_counter() - t0
+        e2e_pass()
+        # timed: the pass repeated (each one the state up, K steps with their
+        # rows, the state down) until MIN_TIMED_S, the median kept
+        times = []
+        target = None
+        while target is None or len(times) < target:
+            barrier()
+            t0 = time.perf_counter()
+            e2e_pass()
+            times.append(time.perf_counter() - t0)
+            if target is None:
+                # every rank makes the same number of passes
+                first = torch.tensor([times[0]], device="cuda", dtype=torch.float64)
+                if dist is not None:
+                    dist.all_reduce(first, op=dist.ReduceOp.MAX)
+                target = int(min(MAX_REPEATS, max(MIN_REPEATS,
+                                                  np.ceil(args.min_timed_s / float(first.item())))))
         last = rows.numpy().reshape(args.steps, follow.size, 12)[-1]
         if not np.array_equal(last[:, 0].view(np.uint32), follow):
             raise RuntimeError("the last step's followed rows were not written")
+        t = torch.tensor(times, device="cuda", dtype=torch.float64)
         if dist is not None:
-            t = torch.tensor([e2e_s], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
+        times = t.cpu().numpy()
+        e2e_s = float(np.median(times))
         state_bytes = sum(v.numel() * v.element_size() for v in host.values())
         e2e = {"value": n * world * args.steps / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": state_bytes / args.steps,
                "d2h_bytes_per_step": state_bytes / args.steps + 48 * follow.size,
                "path": "dem_set_state from pinned host memory, dem_step_followed (the "
-                       "followed rows of every step), dem_get_state to pinned host memory"}
+                       "followed rows of every step), dem_get_state to pinned host memory",
+               "repeats": int(len(times)), "statistic": "median (host wall clock)",
+               "ms_min": 1e3 * float(times.min()), "ms_max": 1e3 * float(times.max())}
         sim2.close()
 
     batched = None

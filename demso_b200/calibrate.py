@@ -14,23 +14,27 @@ hidden run is kept.
 
 Calibration walks the collapse with the model's own trajectory: iteration i
 takes window i (`window_steps` steps) from the state where the model's own
-run, with the parameters of the iterations before, left it, and takes one
-Adam step on (log kn, friction) down the gradient of
+run, with the parameters of the iterations before, left it -- the state in
+the context's order, so that the run continues bit for bit as if it had not
+stopped -- and takes one Adam step on (log kn, friction) down the gradient
+of
 
     L = sum over specimens s, shots q of the window:
         (1 / B_s) sum_b (h_s(x_b; q) - h*_s(x_b; q))^2 / H_s^2
 
-(B_s bins, H_s the column's initial height).  The window is cut into shots
+(B_s bins, H_s the column's initial height); the gradient is each
+specimen's gradient summed over the window, combined over the specimens by
+a trimmed mean (trimmed_total).  The window is cut into shots
 of `shot_steps` steps: each shot runs through the batched adjoint
 (checkpoint every `every` steps) from the model's state at its start, and
 its gradient is taken over that shot alone (the start state held fixed),
 which keeps the derivative of the dense, chaotic flow bounded: over a whole
 3,000-step window it overflows (measured: 1e18 and more, then NaN), while
 over 300 steps it agrees with finite differences.  The binning is piecewise
-linear in the positions, so dL/dx comes from torch's autograd of the
-profile and enters the adjoint as the position cotangent.  At the hidden
-parameters the model's run is the hidden run bit for bit (the step is
-deterministic), so L and its gradient are exactly zero.
+linear in the positions; its derivative dL/dx enters the adjoint as the
+position cotangent.  The profiles are summed in fixed point, so at the hidden
+parameters -- where the model's run is the hidden run bit for bit, the step
+being deterministic -- L and its gradient are exactly zero.
 
 Nothing here is on the stepping path; it drives the library through its
 public API (Batch, adjoint_forward / adjoint_backward, set_systems).
@@ -103,6 +107,25 @@ def param_gradient(g: np.ndarray, kn: float, zeta: float = ZETA):
     return dkn, dmu
 
 
+def specimen_gradients(g: np.ndarray, kn: float, zeta: float = ZETA) -> np.ndarray:
+    """Each specimen's dL/d(kn, friction), (S, 2), from its coefficient
+    gradients (S, 7) -- param_gradient row by row."""
+    return np.array([param_gradient(g[s:s + 1], kn, zeta) for s in range(g.shape[0])])
+
+
+def trimmed_total(per: np.ndarray, trim: float = 0.1) -> np.ndarray:
+    """The sum over specimens of per-specimen gradients (S, 2), estimated as
+    S times the mean of each column with the `trim` fraction of the largest
+    and of the smallest values left out.  A few specimens whose 300-step
+    derivative the chaotic flow has blown up would otherwise outweigh the
+    rest; the estimate is zero when every specimen's gradient is."""
+    S = per.shape[0]
+    k = int(math.floor(trim * S))
+    srt = np.sort(per, axis=0)
+    kept = srt[k:S - k] if S - 2 * k > 0 else srt
+    return S * kept.mean(axis=0)
+
+
 PROFILE_BIN = 4e-3   # m, bin width of the column-height profiles
 PACKING = 0.57       # area fraction of the initial lattice (radii U[0.9, 1.1] mm, pitch 2.35 mm)
 
@@ -113,8 +136,11 @@ class Profiles:
     Bin b of specimen s is centred at (b + 1/2) * bin_width; a disk at x adds
     its area to bins floor(u) and floor(u) + 1 (u = x / bin_width - 1/2) in
     proportion 1 - f and f (f = u - floor(u)), clamped to the box's bins; the
-    sums are divided by bin_width and PACKING.  Piecewise linear in x, so
-    autograd gives dL/dx for the adjoint."""
+    sums are divided by bin_width and PACKING.  The sums are taken in 64-bit
+    fixed point (2^-40 m), so they do not depend on the order the GPU adds
+    them in; dL/dx is the derivative of the piecewise-linear binning."""
+
+    FIXED = float(2 ** 40)
 
     def __init__(self, specimens, device, bin_width: float = PROFILE_BIN):
         import torch
@@ -133,11 +159,8 @@ class Profiles:
         h = np.array([sc.pos[:, 1].max() + sc.radius.max() for sc in specimens], np.float64)
         wb = np.repeat(1.0 / (np.array(nb) * h * h), nb)
         self.weight = torch.tensor(wb, dtype=torch.float64, device=device)
-        self.spec_of_bin = torch.tensor(np.repeat(np.arange(len(specimens)), nb),
-                                        dtype=torch.int64, device=device)
 
-    def __call__(self, x):
-        """Profiles (all bins of all specimens, float64) from x (n,), by id."""
+    def _bins(self, x):
         import torch
         u = x.to(torch.float64) / self.bw - 0.5
         k = torch.floor(u)
@@ -145,13 +168,29 @@ class Profiles:
         k = k.to(torch.int64)
         b0 = torch.clamp(self.first + k, self.first, self.last)
         b1 = torch.clamp(self.first + k + 1, self.first, self.last)
-        h = torch.zeros(self.nbins, dtype=torch.float64, device=x.device)
-        h = h.index_add(0, b0, self.scale * (1.0 - f))
-        return h.index_add(0, b1, self.scale * f)
+        return f, b0, b1
+
+    def __call__(self, x):
+        """Profiles (all bins of all specimens, float64) from x (n,), by id."""
+        import torch
+        f, b0, b1 = self._bins(x)
+        c0 = torch.round(self.scale * (1.0 - f) * self.FIXED).to(torch.int64)
+        c1 = torch.round(self.scale * f * self.FIXED).to(torch.int64)
+        h = torch.zeros(self.nbins, dtype=torch.int64, device=x.device)
+        h.index_add_(0, b0, c0)
+        h.index_add_(0, b1, c1)
+        return h.to(torch.float64) / self.FIXED
 
     def loss(self, h, target):
         d = h - target
-        return (self.weight * d * d).sum()
+        return float((self.weight * d * d).sum().item())
+
+    def grad(self, x, h, target):
+        """dL/dx (n,) of loss(profiles(x), target) (zero where a disk's two
+        bins are clamped into one)."""
+        f, b0, b1 = self._bins(x)
+        r = 2.0 * self.weight * (h - target)
+        return self.scale / self.bw * (r[b1] - r[b0])
 
 
 class Calibration:
@@ -181,18 +220,20 @@ class Calibration:
         self.batch.set_state(s["pos"], s["vel"], s["theta"], s["omega"], s["radius"], s["mass"],
                              s["id"])
 
-    def _by_id(self):
-        """The current state scattered into id order (a dict of CUDA tensors)."""
-        import torch
+    def _current(self):
+        """The current state in the context's order: the sorted order of the
+        last step, which a following step's stable sort breaks ties by.  A run
+        continued from it with dem_set_state is the uninterrupted run bit for
+        bit (a state re-set in another order, such as by id, is not)."""
         st = self.batch.get_state("cuda")
-        idx = st["id"].to(torch.int64)
-        out = {}
-        for k in ("pos", "vel", "theta", "omega", "radius", "mass"):
-            v = torch.empty_like(st[k])
-            v[idx] = st[k]
-            out[k] = v
-        out["id"] = self.initial["id"]
-        return out
+        return {k: st[k] for k in ("pos", "vel", "theta", "omega", "radius", "mass", "id")}
+
+    def _x_by_id(self, state):
+        """The x-coordinates of a context-order state, in id order."""
+        import torch
+        x = torch.empty_like(state["pos"][:, 0])
+        x[state["id"].to(torch.int64)] = state["pos"][:, 0]
+        return x
 
     def _systems(self, kn, mu):
         return [with_params(sc.sys, kn, mu) for sc in self.specimens]
@@ -204,10 +245,10 @@ class Calibration:
         import torch
         self.batch.set_systems(self._systems(kn, mu))
         self._set(self.initial)
-        self.targets = [self.profiles(self.initial["pos"][:, 0])]
+        self.targets = [self.profiles(self._x_by_id(self.initial))]
         for _ in range(self.windows * self.shots):
             self.batch.step(self.shot_steps)
-            self.targets.append(self.profiles(self._by_id()["pos"][:, 0]))
+            self.targets.append(self.profiles(self._x_by_id(self._current())))
         torch.cuda.synchronize()
         self.batch.check()
 
@@ -218,7 +259,7 @@ class Calibration:
         self._set(self.initial)
         if w:
             self.batch.step(w * self.window_steps)
-        return self._by_id()
+        return self._current()
 
     def shot_loss_and_grad(self, q: int, state, kn: float, mu: float):
         """Shot q (ending at target q + 1) from `state`: its loss at (kn, mu),
@@ -226,31 +267,36 @@ class Calibration:
         import torch
         self._set(state)
         self.batch.adjoint_forward(self.shot_steps, min(self.every, self.shot_steps))
-        fin = self._by_id()
-        x = fin["pos"][:, 0].detach().clone().requires_grad_(True)
-        loss = self.profiles.loss(self.profiles(x), self.targets[q + 1])
-        loss.backward()
-        lam_pos = torch.zeros_like(fin["pos"])
-        lam_pos[:, 0] = x.grad.to(torch.float32)
+        fin = self._current()  # before the backward, which restores checkpoints
+        x = self._x_by_id(fin)
+        h = self.profiles(x)
+        loss = self.profiles.loss(h, self.targets[q + 1])
+        lam_pos = torch.zeros((self.n, 2), dtype=torch.float32, device="cuda")
+        lam_pos[:, 0] = self.profiles.grad(x, h, self.targets[q + 1]).to(torch.float32)
         lam_vel = torch.zeros_like(lam_pos)
         lam_om = torch.zeros(self.n, dtype=torch.float32, device="cuda")
         g = self.batch.adjoint_backward(lam_pos.contiguous(), lam_vel, lam_om)
-        return float(loss.item()), param_gradient(g, kn), fin
+        return loss, specimen_gradients(np.asarray(g).reshape(-1, 7), kn), fin
 
     def loss_and_grad(self, w: int, kn: float, mu: float, state):
         """Loss of window w from the model's state `state` at its start (the
-        sum over its shots), its gradient, and the model's state at its
+        sum over its shots), its gradient (each specimen's summed over the
+        shots, then combined by trimmed_total), and the model's state at its
         end."""
         self.batch.set_systems(self._systems(kn, mu))
-        loss, dkn, dmu = 0.0, 0.0, 0.0
+        loss = 0.0
+        per = np.zeros((len(self.specimens), 2))
         for j in range(self.shots):
-            l, (a, b), state = self.shot_loss_and_grad(w * self.shots + j, state, kn, mu)
-            loss, dkn, dmu = loss + l, dkn + a, dmu + b
-        return loss, (dkn, dmu), state
+            l, g, state = self.shot_loss_and_grad(w * self.shots + j, state, kn, mu)
+            loss += l
+            per += g
+        dkn, dmu = trimmed_total(per)
+        return loss, (float(dkn), float(dmu)), state
 
     def run(self, kn0=1e5, mu0=0.4, iters=50, lr=(0.25, 0.04), betas=(0.5, 0.9)):
         """Adam on (log kn, friction); iteration i takes window i mod windows,
-        continuing the model's own run (from the initial columns at window 0)."""
+        continuing the model's own run where window i - 1 left it (from the
+        initial columns at window 0)."""
         x = np.array([math.log(kn0), mu0])
         m = np.zeros(2)
         v = np.zeros(2)

@@ -1086,8 +1086,17 @@ extern "C" int dem_set_state(DemContext* c, uint32_t n, const float* pos, const 
     DEM_TRY_CUDA(cudaStreamSynchronize(st), "set_state sync");
     float rmax;
     memcpy(&rmax, &rbits, 4);
+    rmax = (n > 0 && std::isfinite(rmax)) ? rmax : INFINITY;
+    // the same particle count and largest radius give the same kernel
+    // parameters (and specimen table), so the captured graphs stay valid;
+    // only the first step's full sort is forced, as after every new state
+    if (n == c->n && n > 0 && memcmp(&rmax, &c->rmax, sizeof(float)) == 0) {
+        c->keysValid = false;
+        c->haveOrder = false;
+        return DEM_OK;
+    }
     c->n = n;
-    c->rmax = (n > 0 && std::isfinite(rmax)) ? rmax : INFINITY;
+    c->rmax = rmax;
     if (c->nspec) {
         for (uint32_t sp = 0; sp < c->nspec; ++sp) set_rmax(c->hTable[sp], c->rmax);
         set_rmax(c->P, c->rmax);

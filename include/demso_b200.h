@@ -188,7 +188,10 @@ int dem_set_system(DemContext* ctx, const DemSystem* sys);
 /* State transfer in the reference layout, any order of particles; ids must
  * be a permutation of 0..n-1 (loc is indexed by id).  `host` != 0: the
  * pointers are host memory (pinned or pageable), else device memory.
- * type may be NULL. */
+ * type may be NULL.  Reads the largest radius back (synchronises `stream`)
+ * and clears the error word; the next step sorts from scratch.  The step
+ * graphs already captured stay valid when n and the largest radius are those
+ * of the previous state, and are captured again otherwise. */
 int dem_set_state(DemContext* ctx, uint32_t n, const float* pos, const float* vel,
                   const float* theta, const float* omega, const float* radius,
                   const float* mass, const uint32_t* id, const uint32_t* type, int host,
