@@ -356,6 +356,9 @@ struct DemContext {
     // capture-time fork of the sort phase: the full path's branch
     cudaStream_t forkStream = nullptr;
     cudaEvent_t forkEv = nullptr, joinEv = nullptr;
+    // the incremental sort's movers, placed beside its stayers
+    cudaStream_t moverStream = nullptr;
+    cudaEvent_t moverForkEv = nullptr, moverJoinEv = nullptr;
     // The device-side step loop of multi-step dem_step calls: loopGraph[p]
     // runs pairs of incremental steps from parity p in a WHILE node while the
     // count in loopCtl[1] (copied from loopCtl[0], written before each launch)
@@ -472,7 +475,8 @@ cudaError_t enqueue_full_sort(DemContext* c, int a, cudaStream_t st, int* launch
 cudaError_t enqueue_inc_tail(DemContext* c, int a, cudaStream_t st, int* launches) {
     const int b = a ^ 1;
     return enqueue_incremental_tail(c->inc, c->n, c->keys, c->skey[a], c->cells[a], c->skey[b],
-                                    c->cells[b], c->first[b], sort_move(c, a), st, launches);
+                                    c->cells[b], c->first[b], sort_move(c, a), st, launches,
+                                    c->moverStream, c->moverForkEv, c->moverJoinEv);
 }
 
 // The incremental sort launched directly (the host chose it).
@@ -952,7 +956,13 @@ int init_context(DemContext* c, uint32_t capacity, uint32_t numCells, DemContext
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->loopStream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->forkEv, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->joinEv, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->moverStream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->moverForkEv, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->moverJoinEv, cudaEventDisableTiming);
     if (e != cudaSuccess) {
+        if (c->moverJoinEv) cudaEventDestroy(c->moverJoinEv);
+        if (c->moverForkEv) cudaEventDestroy(c->moverForkEv);
+        if (c->moverStream) cudaStreamDestroy(c->moverStream);
         if (c->joinEv) cudaEventDestroy(c->joinEv);
         if (c->forkEv) cudaEventDestroy(c->forkEv);
         if (c->loopStream) cudaStreamDestroy(c->loopStream);
@@ -979,6 +989,9 @@ extern "C" int dem_destroy(DemContext* c) {
     if (c->forkStream) cudaStreamDestroy(c->forkStream);
     if (c->loopStream) cudaStreamDestroy(c->loopStream);
     if (c->forkEv) cudaEventDestroy(c->forkEv);
+    if (c->moverJoinEv) cudaEventDestroy(c->moverJoinEv);
+    if (c->moverForkEv) cudaEventDestroy(c->moverForkEv);
+    if (c->moverStream) cudaStreamDestroy(c->moverStream);
     if (c->joinEv) cudaEventDestroy(c->joinEv);
     dev_free(c->followRows);
     dev_free(c->followIds);

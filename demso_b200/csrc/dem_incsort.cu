@@ -99,6 +99,9 @@ cells_reduce_kernel(const uint2* __restrict__ prevCells, const uint32_t* __restr
                           (errFlag != nullptr && (*errFlag & kSortTimeoutBit) != 0u);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         ctrl[kCtrlPath] = needFull ? 1u : 0u;
+        // the movers' kernels read this copy: place_stayers, which may run
+        // beside them, clears the count for the step kernel
+        ctrl[kCtrlMoverSnap] = ctrl[kCtrlMovers];
         if (setFull) cudaGraphSetConditional(full, needFull ? 1u : 0u);
     }
     if (needFull) return;
@@ -190,7 +193,7 @@ __global__ void arrivals_scatter_kernel(const uint4* __restrict__ movers,
                                         const uint2* __restrict__ arrInfo,
                                         uint32_t* __restrict__ arrSlots) {
     if (ctrl[kCtrlPath]) return;
-    const uint32_t count = min(ctrl[kCtrlMovers], cap);
+    const uint32_t count = min(ctrl[kCtrlMoverSnap], cap);
     for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < count;
          m += gridDim.x * blockDim.x) {
         const uint4 r = movers[m];
@@ -215,7 +218,7 @@ __global__ void place_movers_kernel(const uint4* __restrict__ movers,
                                     const uint2* __restrict__ newCells,
                                     uint32_t* __restrict__ newSortedKey, SortMove mv) {
     if (ctrl[kCtrlPath]) return;
-    const uint32_t count = min(ctrl[kCtrlMovers], cap);
+    const uint32_t count = min(ctrl[kCtrlMoverSnap], cap);
     for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < count;
          m += gridDim.x * blockDim.x) {
         const uint4 r = movers[m];
@@ -242,7 +245,7 @@ place_stayers_kernel(uint32_t n, const uint32_t* __restrict__ keys,
                      uint32_t* __restrict__ ctrl) {
     if (ctrl[kCtrlPath]) return;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) ctrl[kCtrlMovers] = 0u;  // movers were consumed by the previous kernels
+    if (i == 0) ctrl[kCtrlMovers] = 0u;  // the step kernel counts the next step's movers
     if (i >= n) return;
     const uint32_t o = prevSortedKey[i];
     const uint32_t k = keys[i];
@@ -350,7 +353,8 @@ cudaError_t enqueue_incremental_head(const IncSort& s, const uint2* prevCells,
 cudaError_t enqueue_incremental_tail(const IncSort& s, uint32_t n, const uint32_t* keys,
                                      const uint32_t* prevSortedKey, const uint2* prevCells,
                                      uint32_t* newSortedKey, uint2* newCells, uint32_t* newFirst,
-                                     const SortMove& mv, cudaStream_t st, int* launches) {
+                                     const SortMove& mv, cudaStream_t st, int* launches,
+                                     cudaStream_t side, cudaEvent_t forkEv, cudaEvent_t joinEv) {
     const uint32_t C = s.numCells;
     const uint32_t items = cell_items(C);
     const size_t nb = cell_blocks(C);
@@ -360,17 +364,34 @@ cudaError_t enqueue_incremental_tail(const IncSort& s, uint32_t n, const uint32_
                                                           C, items, s.partials, newCells,
                                                           newFirst, s.stayBase, s.arrInfo,
                                                           s.ctrl);
+    // the movers (two small kernels) on `side` when given, beside the
+    // stayers: both only read what cells_apply wrote, and write disjoint slots
+    const bool fork = side && forkEv && joinEv;
+    cudaStream_t ms = st;
+    if (fork) {
+        cudaError_t e = cudaEventRecord(forkEv, st);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(side, forkEv, 0);
+        if (e != cudaSuccess) return e;
+        ms = side;
+    }
     const unsigned mb = std::min<unsigned>(blocks_for(s.moverCap, kThreads), 296u);
-    arrivals_scatter_kernel<<<mb, kThreads, 0, st>>>(s.movers, s.ctrl, s.moverCap, s.arrInfo,
+    arrivals_scatter_kernel<<<mb, kThreads, 0, ms>>>(s.movers, s.ctrl, s.moverCap, s.arrInfo,
                                                      s.arrSlots);
-    place_movers_kernel<<<mb, kThreads, 0, st>>>(s.movers, s.ctrl, s.moverCap, s.arrInfo,
+    place_movers_kernel<<<mb, kThreads, 0, ms>>>(s.movers, s.ctrl, s.moverCap, s.arrInfo,
                                                  s.arrSlots, newCells, newSortedKey, mv);
     if (n) {
         place_stayers_kernel<<<blocks_for(n, kThreads), kThreads, 0, st>>>(
             n, keys, prevSortedKey, prevCells, s.stayBase, newSortedKey, mv, s.ctrl);
     }
     if (launches) *launches += 5;
-    return cudaGetLastError();
+    cudaError_t e = cudaGetLastError();
+    if (fork) {
+        // join the movers' branch even after an error
+        cudaError_t ej = cudaEventRecord(joinEv, side);
+        if (ej == cudaSuccess) ej = cudaStreamWaitEvent(st, joinEv, 0);
+        if (e == cudaSuccess) e = ej;
+    }
+    return e;
 }
 
 cudaError_t enqueue_full(const IncSort& s, uint32_t n, uint32_t keyBits, uint32_t* keys,

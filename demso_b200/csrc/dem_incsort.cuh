@@ -38,6 +38,7 @@ namespace dem {
 constexpr uint32_t kCtrlNeedFull = 0;        // ctrl[0]: non-zero -> full path next step
 constexpr uint32_t kCtrlMovers = 1;          // ctrl[1]: movers recorded by the step kernel
 constexpr uint32_t kCtrlPath = 2;            // ctrl[2]: this step runs the full path
+constexpr uint32_t kCtrlMoverSnap = 3;       // ctrl[3]: this step's movers, kept by the first kernel
 constexpr uint32_t kHasLeavers = 0x80000000u;  // flag bit in stayBase
 
 // The state the sort phase moves: positions and radii from the previous
@@ -76,14 +77,18 @@ IncSort carve_incsort(void* base, uint32_t n, uint32_t numCells);
 // order the step kernel just stepped; `keys` are the new keys.  `head` (the
 // first kernel) reads whether the full path is due, keeps the answer in
 // ctrl[kCtrlPath] for the kernels of `tail`, and with setFull passes it to
-// the graph conditional handle `full`.
+// the graph conditional handle `full`.  With a `side` stream (and two events)
+// `tail` places the movers on it, beside the stayers on `st` -- the two write
+// disjoint slots -- and joins it back into `st` before returning.
 cudaError_t enqueue_incremental_head(const IncSort& s, const uint2* prevCells,
                                      cudaGraphConditionalHandle full, bool setFull,
                                      cudaStream_t st, int* launches);
 cudaError_t enqueue_incremental_tail(const IncSort& s, uint32_t n, const uint32_t* keys,
                                      const uint32_t* prevSortedKey, const uint2* prevCells,
                                      uint32_t* newSortedKey, uint2* newCells, uint32_t* newFirst,
-                                     const SortMove& mv, cudaStream_t st, int* launches);
+                                     const SortMove& mv, cudaStream_t st, int* launches,
+                                     cudaStream_t side = nullptr, cudaEvent_t forkEv = nullptr,
+                                     cudaEvent_t joinEv = nullptr);
 
 // Full path: onesweep sort of `keys`, cell ranges, gather, reset of the
 // incremental counters.  `perm` and `keys` are overwritten.
