@@ -19,13 +19,13 @@ from dataclasses import dataclass, field
 from typing import Optional, Sequence
 
 from . import _lib
-from ._lib import (CTX_ACCEL, CTX_AUTOTUNE, CTX_DIRECT, CTX_PRESSURE, DEM_MAX_MATERIALS, DemError,
-                   check, load)
+from ._lib import (CTX_ACCEL, CTX_AUTOTUNE, CTX_CALLER_STATE, CTX_DIRECT, CTX_PRESSURE,
+                   DEM_MAX_MATERIALS, STATE_PAD, DemError, check, load)
 
 __all__ = ["Material", "System", "DemError", "calcHash", "sortParticles",
            "reorderDataAndFindCellStart", "collide", "integrateSystem", "Simulation", "Batch",
            "sort_scratch_bytes", "load", "CTX_PRESSURE", "CTX_ACCEL", "CTX_DIRECT",
-           "CTX_AUTOTUNE"]
+           "CTX_AUTOTUNE", "CTX_CALLER_STATE", "STATE_PAD"]
 
 
 @dataclass
@@ -92,6 +92,16 @@ def _ptr(t) -> Optional[int]:
     if not t.is_contiguous():
         raise ValueError("expected a contiguous tensor")
     return t.data_ptr()
+
+
+class _DeviceSpan:
+    """A device array the library owns, exposed through
+    ``__cuda_array_interface__`` so that ``torch.as_tensor`` wraps it without
+    a copy."""
+
+    def __init__(self, ptr: int, shape: tuple, typestr: str):
+        self.__cuda_array_interface__ = {"shape": shape, "typestr": typestr,
+                                         "data": (ptr, False), "version": 3, "strides": None}
 
 
 def _stream(stream=None) -> Optional[int]:
@@ -182,11 +192,13 @@ class Simulation:
         else:
             self._h = _handle
         self.n = 0
+        self._adopted = None
 
     def close(self) -> None:
         if self._h:
             load().dem_destroy(self._h)
             self._h = None
+        self._adopted = None
 
     def __del__(self):
         try:
@@ -250,6 +262,48 @@ class Simulation:
                                    int(host), st))
         if host:
             torch.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
+        return out
+
+    _SET_FIELDS = ("pos", "vel", "theta", "omega", "radius", "mass", "id", "type")
+
+    def adopt_state(self, first: dict, second: dict, n: int, stream=None) -> None:
+        """Steps in caller-owned CUDA tensors (dem_adopt_state): the
+        reference's two ping-pong sets of ParticlesValues (functions.cu:68-149)
+        as dicts of ``_SET_FIELDS``.  ``first`` holds the initial state of n
+        particles; ``pos`` and ``radius`` hold n + STATE_PAD rows.  This object
+        keeps the tensors alive until the next adopt_state or close."""
+        import ctypes as C
+        sets = []
+        for d in (first, second):
+            ss = _lib.DemStateSet()
+            for k in self._SET_FIELDS:
+                setattr(ss, k, _ptr(d.get(k)))
+            sets.append(ss)
+        check(load().dem_adopt_state(self._h, int(n), C.byref(sets[0]), C.byref(sets[1]),
+                                     _stream(stream)))
+        self._adopted = (first, second)
+        self.n = int(n)
+
+    def state_view(self) -> dict:
+        """The current state without a copy (dem_state_view): tensors over the
+        buffers that hold it, valid until the next step, set_state or
+        adopt_state, plus ``set`` (0 or 1), the set that holds every field but
+        the positions."""
+        import ctypes as C
+        import torch
+        v = _lib.DemStateSet()
+        which = C.c_int(0)
+        check(load().dem_state_view(self._h, C.byref(v), C.byref(which)))
+        n = self.n
+        shapes = {"pos": ((n, 2), "<f4"), "vel": ((n, 2), "<f4"), "theta": ((n,), "<f4"),
+                  "omega": ((n,), "<f4"), "radius": ((n,), "<f4"), "mass": ((n,), "<f4"),
+                  "id": ((n,), "<i4"), "type": ((n,), "<i4")}
+        out = {}
+        for k, (shape, ts) in shapes.items():
+            ptr = getattr(v, k)
+            out[k] = None if ptr is None else torch.as_tensor(_DeviceSpan(ptr, shape, ts),
+                                                              device="cuda")
+        out["set"] = which.value
         return out
 
     def step(self, nsteps: int = 1, stream=None) -> None:

@@ -18,6 +18,8 @@ CTX_PRESSURE = 1
 CTX_ACCEL = 2
 CTX_DIRECT = 4
 CTX_AUTOTUNE = 8
+CTX_CALLER_STATE = 16
+STATE_PAD = 8  # DEM_STATE_PAD
 STEP_VARIANTS = 4  # DEM_STEP_VARIANTS
 NUM_STAGES = 3  # DEM_NUM_STAGES: sort, reorder, collide + integrate
 ADJ_NUM_COEF = 7  # DEM_ADJ_NUM_COEF
@@ -76,6 +78,11 @@ class DemRenderParams(C.Structure):
                 ("viewRotations", C.c_uint32), ("colorByPressure", C.c_uint32),
                 ("maxPressure", C.c_float), ("color", (C.c_float * 3) * DEM_MAX_MATERIALS)]
 
+class DemStateSet(C.Structure):
+    _fields_ = [("pos", C.c_void_p), ("vel", C.c_void_p), ("theta", C.c_void_p),
+                ("omega", C.c_void_p), ("radius", C.c_void_p), ("mass", C.c_void_p),
+                ("id", C.c_void_p), ("type", C.c_void_p)]
+
 # (name, restype, argtypes)
 _P = C.c_void_p
 _U = C.c_uint32
@@ -100,6 +107,8 @@ SIGNATURES = [
     ("dem_set_system", C.c_int, [_P, _SYS]),
     ("dem_set_state", C.c_int, [_P, _U] + [_P] * 8 + [C.c_int, _P]),
     ("dem_get_state", C.c_int, [_P] + [_P] * 12 + [C.c_int, _P]),
+    ("dem_adopt_state", C.c_int, [_P, _U, C.POINTER(DemStateSet), C.POINTER(DemStateSet), _P]),
+    ("dem_state_view", C.c_int, [_P, C.POINTER(DemStateSet), C.POINTER(C.c_int)]),
     ("dem_step", C.c_int, [_P, _U, _P]),
     ("dem_get_cells", C.c_int, [_P, _P, _P, _P]),
     ("dem_check", C.c_int, [_P, _P]),

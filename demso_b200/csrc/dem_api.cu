@@ -897,9 +897,14 @@ int init_context(DemContext* c, uint32_t capacity, uint32_t numCells, DemContext
     // the sorted positions and radii are read up to kFilterPad - 1 elements
     // past the last particle by the step kernel's candidate filter
     const size_t f4p = al256(4 * (N + kFilterPad)), f8p = al256(8 * (N + kFilterPad));
+    // the particle state: two dynamic and two static sets, unless the
+    // caller's buffers are adopted instead (DEM_CTX_CALLER_STATE)
+    const bool ownState = !(c->flags & DEM_CTX_CALLER_STATE);
     size_t total = 0;
-    total += 2 * (f8p + f8 + 2 * f4);            // dyn sets
-    total += 2 * (f4p + 2 * f4 + (c->typed ? f4 : 0));  // static sets
+    if (ownState) {
+        total += 2 * (f8p + f8 + 2 * f4);                    // dyn sets
+        total += 2 * (f4p + 2 * f4 + (c->typed ? f4 : 0));   // static sets
+    }
     total += 4 * f4 + 2 * f4;                    // loc, keys, perm, src, sorted keys x2
     total += 2 * cells8 + 2 * first4;            // cell ranges and first particles x2
     total += f4 + f8 + f4;                       // pressure, acc, alpha
@@ -919,7 +924,7 @@ int init_context(DemContext* c, uint32_t capacity, uint32_t numCells, DemContext
     }
     char* p = static_cast<char*>(c->block);
     auto take = [&p](size_t b) { char* q = p; p += b; return q; };
-    for (int s = 0; s < 2; ++s) {
+    for (int s = 0; s < 2 && ownState; ++s) {
         c->dyn[s].pos = reinterpret_cast<float2*>(take(f8p));
         c->dyn[s].vel = reinterpret_cast<float2*>(take(f8));
         c->dyn[s].theta = reinterpret_cast<float*>(take(f4));
@@ -1064,33 +1069,26 @@ extern "C" int dem_batch_set_systems(DemContext* c, const DemSystem* specs,
     return DEM_OK;
 }
 
-extern "C" int dem_set_state(DemContext* c, uint32_t n, const float* pos, const float* vel,
-                             const float* theta, const float* omega, const float* radius,
-                             const float* mass, const uint32_t* id, const uint32_t* type, int host,
-                             void* stream) {
-    if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+namespace {
+// Particle counts a context takes: up to its capacity, a batch exactly its
+// capacity.
+int check_count(const DemContext* c, uint32_t n) {
     if (n > c->capacity) return fail(DEM_ERR_CAPACITY, "n %u > capacity %u", n, c->capacity);
     if (c->nspec && n != c->capacity)
         return fail(DEM_ERR_INVALID_ARG, "a batch takes all %u particles, specimen by specimen",
                     c->capacity);
-    if (n && (!pos || !vel || !theta || !omega || !radius || !mass || !id))
-        return fail(DEM_ERR_INVALID_ARG, "dem_set_state: NULL buffer");
-    if (c->typed && n && !type)
-        return fail(DEM_ERR_INVALID_ARG, "type array required with more than one material");
-    cudaStream_t st = (cudaStream_t)stream;
+    return DEM_OK;
+}
+
+bool has_state_sets(const DemContext* c) { return c->dyn[0].pos != nullptr; }
+
+// A new state of n particles is in the current sets (set c->cur, positions
+// in dyn[0].pos): clears the error word, reads the largest radius back and
+// keeps or drops the captured graphs.
+int accept_state(DemContext* c, uint32_t n, cudaStream_t st) {
     // the new state replaces the one any recorded error was about
     DEM_TRY_CUDA(cudaMemsetAsync(c->errFlag, 0, 4, st), "clear error word");
-    const cudaMemcpyKind k = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
     const int a = c->cur;
-    DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[0].pos, pos, 8ull * n, k, st), "set pos");
-    DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[a].vel, vel, 8ull * n, k, st), "set vel");
-    DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[a].theta, theta, 4ull * n, k, st), "set theta");
-    DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[a].omega, omega, 4ull * n, k, st), "set omega");
-    DEM_TRY_CUDA(cudaMemcpyAsync(c->stat[a].radius, radius, 4ull * n, k, st), "set radius");
-    DEM_TRY_CUDA(cudaMemcpyAsync(c->stat[a].mass, mass, 4ull * n, k, st), "set mass");
-    DEM_TRY_CUDA(cudaMemcpyAsync(c->stat[a].id, id, 4ull * n, k, st), "set id");
-    if (c->typed)
-        DEM_TRY_CUDA(cudaMemcpyAsync(c->stat[a].type, type, 4ull * n, k, st), "set type");
     // the largest radius bounds every contact distance (neighbour culling)
     uint32_t rbits = 0;
     DEM_TRY_CUDA(launch_max_radius(c->stat[a].radius, n, c->errFlag + 1, st), "max radius");
@@ -1125,12 +1123,131 @@ extern "C" int dem_set_state(DemContext* c, uint32_t n, const float* pos, const 
     c->haveOrder = false;
     return DEM_OK;
 }
+}  // namespace
+
+extern "C" int dem_set_state(DemContext* c, uint32_t n, const float* pos, const float* vel,
+                             const float* theta, const float* omega, const float* radius,
+                             const float* mass, const uint32_t* id, const uint32_t* type, int host,
+                             void* stream) {
+    if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    int rc = check_count(c, n);
+    if (rc) return rc;
+    if (!has_state_sets(c))
+        return fail(DEM_ERR_INVALID_ARG, "no state buffers: call dem_adopt_state first");
+    if (n && (!pos || !vel || !theta || !omega || !radius || !mass || !id))
+        return fail(DEM_ERR_INVALID_ARG, "dem_set_state: NULL buffer");
+    if (c->typed && n && !type)
+        return fail(DEM_ERR_INVALID_ARG, "type array required with more than one material");
+    cudaStream_t st = (cudaStream_t)stream;
+    const cudaMemcpyKind k = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    const int a = c->cur;
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[0].pos, pos, 8ull * n, k, st), "set pos");
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[a].vel, vel, 8ull * n, k, st), "set vel");
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[a].theta, theta, 4ull * n, k, st), "set theta");
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->dyn[a].omega, omega, 4ull * n, k, st), "set omega");
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->stat[a].radius, radius, 4ull * n, k, st), "set radius");
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->stat[a].mass, mass, 4ull * n, k, st), "set mass");
+    DEM_TRY_CUDA(cudaMemcpyAsync(c->stat[a].id, id, 4ull * n, k, st), "set id");
+    if (c->typed)
+        DEM_TRY_CUDA(cudaMemcpyAsync(c->stat[a].type, type, 4ull * n, k, st), "set type");
+    return accept_state(c, n, st);
+}
+
+static_assert(DEM_STATE_PAD == kFilterPad, "adopted sets carry the step kernel's read padding");
+
+extern "C" int dem_adopt_state(DemContext* c, uint32_t n, const DemStateSet* first,
+                               const DemStateSet* second, void* stream) {
+    if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    int rc = check_count(c, n);
+    if (rc) return rc;
+    if (n == 0) return fail(DEM_ERR_INVALID_ARG, "dem_adopt_state: n must be > 0");
+    if (!first || !second) return fail(DEM_ERR_INVALID_ARG, "dem_adopt_state: NULL set");
+    // every array of both sets: its address, its length in bytes and its
+    // alignment; they must be present, aligned and pairwise disjoint
+    struct Span { const void* p; size_t bytes; size_t align; const char* what; };
+    std::vector<Span> spans;
+    const DemStateSet* sets[2] = {first, second};
+    for (int s = 0; s < 2; ++s) {
+        const DemStateSet& d = *sets[s];
+        spans.push_back({d.pos, 8ull * (n + DEM_STATE_PAD), 8, "pos"});
+        spans.push_back({d.vel, 8ull * n, 8, "vel"});
+        spans.push_back({d.theta, 4ull * n, 4, "theta"});
+        spans.push_back({d.omega, 4ull * n, 4, "omega"});
+        spans.push_back({d.radius, 4ull * (n + DEM_STATE_PAD), 4, "radius"});
+        spans.push_back({d.mass, 4ull * n, 4, "mass"});
+        spans.push_back({d.id, 4ull * n, 4, "id"});
+        if (c->typed) spans.push_back({d.type, 4ull * n, 4, "type"});
+    }
+    for (const Span& x : spans) {
+        if (!x.p) return fail(DEM_ERR_INVALID_ARG, "dem_adopt_state: NULL %s", x.what);
+        if (misaligned(x.p, x.align))
+            return fail(DEM_ERR_INVALID_ARG, "dem_adopt_state: %s is not %zu-byte aligned", x.what,
+                        x.align);
+    }
+    for (size_t i = 0; i < spans.size(); ++i)
+        for (size_t j = i + 1; j < spans.size(); ++j) {
+            const uintptr_t a0 = (uintptr_t)spans[i].p, b0 = (uintptr_t)spans[j].p;
+            if (a0 < b0 + spans[j].bytes && b0 < a0 + spans[i].bytes)
+                return fail(DEM_ERR_INVALID_ARG, "dem_adopt_state: %s of set %zu overlaps %s of set %zu",
+                            spans[i].what, i / (spans.size() / 2), spans[j].what,
+                            j / (spans.size() / 2));
+        }
+    for (const Span& x : spans) {
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, x.p) != cudaSuccess || at.type != cudaMemoryTypeDevice ||
+            at.device != c->device) {
+            cudaGetLastError();
+            return fail(DEM_ERR_INVALID_ARG, "dem_adopt_state: %s is not device memory of device %d",
+                        x.what, c->device);
+        }
+    }
+    DynSet dyn[2];
+    StatSet stat[2];
+    for (int s = 0; s < 2; ++s) {
+        const DemStateSet& d = *sets[s];
+        dyn[s].pos = reinterpret_cast<float2*>(d.pos);
+        dyn[s].vel = reinterpret_cast<float2*>(d.vel);
+        dyn[s].theta = d.theta;
+        dyn[s].omega = d.omega;
+        stat[s].radius = d.radius;
+        stat[s].mass = d.mass;
+        stat[s].id = d.id;
+        stat[s].type = c->typed ? d.type : nullptr;
+    }
+    // the captured graphs hold the buffers' addresses
+    if (memcmp(dyn, c->dyn, sizeof(dyn)) != 0 || memcmp(stat, c->stat, sizeof(stat)) != 0)
+        drop_graphs(c);
+    memcpy(c->dyn, dyn, sizeof(dyn));
+    memcpy(c->stat, stat, sizeof(stat));
+    c->cur = 0;
+    return accept_state(c, n, (cudaStream_t)stream);
+}
+
+extern "C" int dem_state_view(DemContext* c, DemStateSet* out, int* setIndex) {
+    if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    if (!out) return fail(DEM_ERR_INVALID_ARG, "dem_state_view: NULL output");
+    if (!has_state_sets(c))
+        return fail(DEM_ERR_INVALID_ARG, "no state buffers: call dem_adopt_state first");
+    const int a = c->cur;
+    out->pos = reinterpret_cast<float*>(c->dyn[0].pos);
+    out->vel = reinterpret_cast<float*>(c->dyn[a].vel);
+    out->theta = c->dyn[a].theta;
+    out->omega = c->dyn[a].omega;
+    out->radius = c->stat[a].radius;
+    out->mass = c->stat[a].mass;
+    out->id = c->stat[a].id;
+    out->type = c->typed ? c->stat[a].type : nullptr;
+    if (setIndex) *setIndex = a;
+    return DEM_OK;
+}
 
 extern "C" int dem_get_state(DemContext* c, float* pos, float* vel, float* theta, float* omega,
                              float* radius, float* mass, uint32_t* id, uint32_t* type,
                              uint32_t* loc, float* pressure, float* acc, float* alpha, int host,
                              void* stream) {
     if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    if (!has_state_sets(c))
+        return fail(DEM_ERR_INVALID_ARG, "no state buffers: call dem_adopt_state first");
     cudaStream_t st = (cudaStream_t)stream;
     const cudaMemcpyKind k = host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     const uint32_t n = c->n;
@@ -1510,6 +1627,8 @@ extern "C" int dem_render(DemContext* c, const DemRenderParams* rp, void* image,
     int rc = check_render(rp);
     if (rc) return rc;
     if (!image) return fail(DEM_ERR_INVALID_ARG, "dem_render: NULL image");
+    if (!has_state_sets(c))
+        return fail(DEM_ERR_INVALID_ARG, "no state buffers: call dem_adopt_state first");
     const size_t words = (size_t)rp->imageDIMx * rp->imageDIMy;
     if (c->renderOwnerWords < words) {
         dev_free(c->renderOwner);

@@ -178,6 +178,8 @@ typedef struct DemContext DemContext;
                                  (one host read-back per step; for per-kernel profiling) */
 #define DEM_CTX_AUTOTUNE 8u   /* choose the step kernel's launch shape on the first steps
                                  (dem_get_step_variant) */
+#define DEM_CTX_CALLER_STATE 16u /* allocate no particle state: the caller's buffers
+                                    are handed over by dem_adopt_state */
 
 int dem_create(const DemSystem* sys, uint32_t capacity, uint32_t flags, DemContext** out);
 int dem_destroy(DemContext* ctx);
@@ -227,6 +229,48 @@ int dem_batch_set_systems(DemContext* ctx, const DemSystem* specs, uint32_t numS
 int dem_get_state(DemContext* ctx, float* pos, float* vel, float* theta, float* omega,
                   float* radius, float* mass, uint32_t* id, uint32_t* type, uint32_t* loc,
                   float* pressure, float* acc, float* alpha, int host, void* stream);
+
+/* One set of particle-state buffers in device memory, the reference's
+ * ParticlesValues pos1/vel1/theta1/omega1/ID1/type1 (or the ...2 set),
+ * with per-particle radius and mass.  `pos` and `radius` hold
+ * n + DEM_STATE_PAD elements: the step reads whole groups of sorted
+ * positions and radii past the last particle (the values there are never
+ * used).  float2 arrays (pos, vel) 8-byte aligned, the others 4-byte. */
+#define DEM_STATE_PAD 8u
+typedef struct DemStateSet {
+    float* pos;       /* 2 (n + DEM_STATE_PAD) floats, x and y interleaved */
+    float* vel;       /* 2 n */
+    float* theta;     /* n */
+    float* omega;     /* n */
+    float* radius;    /* n + DEM_STATE_PAD */
+    float* mass;      /* n */
+    uint32_t* id;     /* n */
+    uint32_t* type;   /* n; ignored (may be NULL) with one material */
+} DemStateSet;
+
+/* The reference's "adopt caller buffers" form of the state: allocateVectors
+ * (functions.cu:68-149) leaves the two ping-pong sets to the caller, and
+ * its step loop (main.cu:395-430) alternates between them.  The context
+ * keeps no copy: it steps in `first` and `second` (two distinct,
+ * non-overlapping sets of device buffers that outlive the context or the
+ * next dem_adopt_state) for as long as it holds them.  `first` holds the
+ * initial state of n particles in the layout of dem_set_state; `second` is
+ * scratch.  Which buffers hold the state after a step is given by
+ * dem_state_view; dem_set_state and dem_get_state copy into and out of the
+ * adopted buffers.  Reads the largest radius back (synchronises `stream`),
+ * clears the error word, and captures the step graphs again when a buffer,
+ * n or the largest radius changed.  A context created with
+ * DEM_CTX_CALLER_STATE allocates no state of its own and takes its state
+ * only this way. */
+int dem_adopt_state(DemContext* ctx, uint32_t n, const DemStateSet* first,
+                    const DemStateSet* second, void* stream);
+/* Device pointers of the current state (n particles in cell-sorted order),
+ * adopted buffers or the context's own: positions in the first set's pos,
+ * the other fields in set *setIndex (0 first, 1 second; may be NULL).
+ * Valid until the next step, dem_set_state or dem_adopt_state; reading them
+ * on another stream needs the usual synchronisation.  type is NULL with one
+ * material. */
+int dem_state_view(DemContext* ctx, DemStateSet* out, int* setIndex);
 
 /* Advances `nsteps` full steps (hash, sort, reorder, collide, integrate).
  * Once the context holds a previous order (after its first step) and is

@@ -44,6 +44,8 @@ def test_abi_version_and_struct_sizes():
     # DemSystem: 4 + 8 + 8 + 4 + 8 + 4 + 4 + 4 bytes + DEM_MAX_MATERIALS * 24
     assert C.sizeof(_lib.DemSystem) == 44 + _lib.DEM_MAX_MATERIALS * 24
     assert C.sizeof(_lib.DemMaterial) == 24
+    assert C.sizeof(_lib.DemStateSet) == 8 * 8  # eight pointers
+    assert _lib.STATE_PAD == 8
 
 
 def _sys(**kw):
@@ -102,6 +104,8 @@ def test_bad_arguments_are_status_codes_not_crashes():
     assert lib.dem_get_followed_async(None, ids, 2, rows, None) == 1
     assert lib.dem_adj_forward(None, 10, 5, None) == 1
     assert lib.dem_adj_backward(None, None, None, None, None, None) == 1
+    assert lib.dem_adopt_state(None, 10, None, None, None) == 1
+    assert lib.dem_state_view(None, None, None) == 1
     assert lib.dem_destroy(None) == 0
     # n = 0 is a no-op
     assert lib.dem_calc_hash(s, None, None, None, 0, None) == 0
