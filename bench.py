@@ -6,9 +6,12 @@ One step = one DEM time step (sort, reorder, collide + integrate) of the
 4,194,304-disk "plain at scale" scene: log-normal radii (median 1 mm,
 sigma 0.15, clipped [0.6, 1.6] mm), seeded random sequential placement to
 area fraction 0.55 in a 4.1 m x 6.11 m walled box, 1024 x 1024 grid, dt 2e-6.
-With N > 1 (torchrun, one rank per GPU) every rank steps its own replica
-(seed = rank): the plain step of one box has a halo exchange that is not
-built, so this is weak scaling by replicas.
+With N > 1 (torchrun, one rank per GPU) the ranks step ONE scene of N x 4M
+disks (the 4M scene stacked N times upward) cut into slabs of cell rows: each
+rank steps its slab's halo window with the fused context and the ranks
+exchange bands over NCCL every --period steps (demso_b200.slab), the same
+bits as one domain; --replicas instead steps an independent 4M-disk scene
+per rank.  Weak scaling either way (4M disks per GPU).
 
 `value` is whole-job particle-steps/s over K timed steps issued as one
 dem_step call (device time, CUDA events, max over ranks); the library runs
@@ -502,6 +505,153 @@ def measure_sweep(sizes, steps: int = 200, warmup: int = 50):
     return rows
 
 
+# ------------------------------------------------------------------ slabs
+def main_slabs(args, world, rank, local, dist):
+    """N > 1: one scene of N x n disks (the n-disk plain-at-scale scene
+    stacked N times upward, n disks per GPU) cut into N slabs of cell rows
+    (demso_b200.slab): every rank steps its slab's halo window with the fused
+    context and the ranks exchange bands over NCCL every `period` steps.
+    `value` counts the scene's N x n disks (not the windows' halo and parked
+    particles) over the device time of K steps, max over ranks."""
+    import ctypes as C
+    import torch
+    import demso_b200 as D
+    from demso_b200 import scenes
+    from demso_b200.slab import ContextStepper, DistExchange, HaloSlab, run, scene_bounds
+
+    sc = scenes.stacked_plain(args.n, world)
+    total = sc.n
+    bounds = scene_bounds(sc.sys, sc.pos, world)
+    stepper = ContextStepper(sc.sys, float(sc.radius.max()))
+    slab = HaloSlab(sc.sys, rank, world, bounds, args.period, stepper)
+    # this rank's window of the initial state, in pinned host memory (the
+    # end-to-end pass uploads it from there)
+    from demso_b200.slab import cell_rows
+    rows = cell_rows(sc.sys, sc.pos)
+    keep = np.nonzero((rows >= slab.wlo) & (rows < slab.whi))[0]
+    host = {}
+    for k in ("pos", "vel", "theta", "omega", "radius", "mass", "id"):
+        a = np.ascontiguousarray(getattr(sc, k)[keep])
+        host[k] = torch.from_numpy(a.view(np.int32) if a.dtype == np.uint32 else a).pin_memory()
+    host["type"] = None
+    del sc, rows, keep
+    comm = torch.device("cuda" if args.comm_backend == "nccl" else "cpu")
+    ex = DistExchange(rank, world, comm)
+
+    def reduce_max(values):
+        t = torch.tensor(values, device=comm, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return t.cpu().numpy()
+
+    def load():
+        dev = {k: (None if v is None else v.to("cuda", non_blocking=True))
+               for k, v in host.items()}
+        stepper.set_window([dev], (slab.wlo, slab.whi))
+
+    load()
+    # warm-up: every graph of the window's context (both parities, the step
+    # loop) and at least two band exchanges, untimed
+    run(slab, ex, max(args.warmup, 2 * args.period + 3))
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    clocks = Clocks(local)
+    clocks.start()
+    reps, target = [], None
+    while target is None or len(reps) < target:
+        dist.barrier()
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        run(slab, ex, args.steps)
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        reps.append(ev[0].elapsed_time(ev[1]))
+        if target is None:
+            first = float(reduce_max([reps[0]])[0])
+            target = int(min(MAX_REPEATS, max(MIN_REPEATS,
+                                              np.ceil(1e3 * args.min_timed_s / first))))
+    clk = clocks.stop()
+    reps = reduce_max(reps)
+    elapsed = float(np.median(reps))
+    value = total * args.steps / (elapsed * 1e-3)
+    stepper.sim.check()
+    sim = stepper.sim
+    kernels_per_step = sim.kernels_per_step()
+
+    # the window's stage times (one step per launch, events around the
+    # stages) for the step kernel's roofline; no exchange in this pass
+    D.check(D.load().dem_profile_begin(sim.handle, args.period))
+    sim.step(args.period)
+    torch.cuda.synchronize()
+    ms = (C.c_float * D._lib.NUM_STAGES)()
+    nprof = C.c_uint32(0)
+    D.check(D.load().dem_profile_end(sim.handle, ms, C.byref(nprof)))
+    stage_ms = [ms[i] / max(1, nprof.value) for i in range(3)]
+    hbm, kind = peaks()
+    cells = stepper.sys.num_cells
+    cap = stepper.capacity
+    bytes_launch = STEP_KERNEL_BYTES_PER_PARTICLE * cap + STEP_KERNEL_BYTES_PER_CELL * cells
+    achieved = bytes_launch / (stage_ms[2] * 1e-3) / 1e9
+
+    # end to end: the window uploaded from pinned host memory, K steps with
+    # their exchanges, the slab's own rows downloaded
+    e2e = None
+    if not args.no_e2e:
+        times, target = [], None
+        down = 0
+        while target is None or len(times) < target:
+            dist.barrier()
+            t0 = time.perf_counter()
+            load()
+            run(slab, ex, args.steps)
+            own = slab.own().cpu()
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+            down = own.numel() * own.element_size()
+            if target is None:
+                first = float(reduce_max([times[0]])[0])
+                target = int(min(MAX_REPEATS, max(MIN_REPEATS,
+                                                  np.ceil(args.min_timed_s / first))))
+        times = reduce_max(times)
+        up = sum(v.numel() * v.element_size() for v in host.values() if v is not None)
+        e2e = {"value": total * args.steps / float(np.median(times)), "unit": UNIT,
+               "h2d_bytes_per_step": up / args.steps, "d2h_bytes_per_step": down / args.steps,
+               "path": "each rank: its window set from pinned host memory, K steps with "
+                       "the band exchanges, its own rows downloaded",
+               "repeats": int(len(times)), "statistic": "median (host wall clock), max over ranks"}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": elapsed / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": dict(config_dict(args.n, None),
+                               workload="%d stacked copies of the plain-at-scale scene of %d "
+                                        "disks (%d disks in one box %.4g m x %.4g m, %d x %d "
+                                        "grid)" % (world, args.n, total, stepper.sys.Lx,
+                                                   stepper.sys.Ly, stepper.sys.gx,
+                                                   stepper.sys.gy),
+                               n_particles=total,
+                               parallelism="slab decomposition over %d ranks: halo windows of "
+                                           "%d rows, bands exchanged every %d steps over NCCL"
+                                           % (world, slab.halo, args.period),
+                               slab_rows=bounds, window_capacity=cap),
+                "timed_repeats": {"count": int(len(reps)), "statistic": "median",
+                                  "timed_s": float(np.sum(reps)) * 1e-3},
+                "roofline": {"bound": "hbm", "kernel": "step_kernel of rank 0's window",
+                             "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                             "frac": achieved / hbm, "peak_kind": kind, "traffic": None,
+                             "bytes_per_launch": bytes_launch},
+                "stage_ms_per_step": {"sort_reorder": stage_ms[0],
+                                      "collide_integrate": stage_ms[2]},
+                "cpu_baseline": None, "e2e": e2e, "clocks": clk,
+                "gpu_launches": kernels_per_step * args.steps,
+                "kernels_per_step": kernels_per_step}
+        print(json.dumps(line), flush=True)
+    stepper.close()
+    dist.destroy_process_group()
+    return 0
+
+
 # ------------------------------------------------------------------ our arm
 def main():
     ap = argparse.ArgumentParser()
@@ -509,7 +659,7 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=500)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--n", "--particles", dest="n", type=int, default=N_DEFAULT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
@@ -527,6 +677,14 @@ def main():
     ap.add_argument("--direct", action="store_true",
                     help="launch each kernel directly instead of through CUDA graphs "
                          "(for per-kernel profilers; one host read-back per step)")
+    ap.add_argument("--period", type=int, default=25,
+                    help="N > 1: steps between the slabs' band exchanges")
+    ap.add_argument("--comm-backend", default="nccl", choices=["nccl", "gloo"],
+                    help="N > 1: process-group backend; gloo moves the bands through host "
+                         "memory (for running several ranks on one GPU in tests)")
+    ap.add_argument("--replicas", action="store_true",
+                    help="N > 1: every rank steps its own n-disk scene instead of one slab "
+                         "of a shared N x n-disk scene")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -540,12 +698,15 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
+    torch.cuda.set_device(local % torch.cuda.device_count())
     dist = None
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group(args.comm_backend, timeout=datetime.timedelta(seconds=120))
+
+    if world > 1 and not args.replicas:
+        return main_slabs(args, world, rank, local, dist)
 
     def barrier():
         if dist is not None:

@@ -109,6 +109,7 @@ SIGNATURES = [
     ("dem_get_state", C.c_int, [_P] + [_P] * 12 + [C.c_int, _P]),
     ("dem_adopt_state", C.c_int, [_P, _U, C.POINTER(DemStateSet), C.POINTER(DemStateSet), _P]),
     ("dem_state_view", C.c_int, [_P, C.POINTER(DemStateSet), C.POINTER(C.c_int)]),
+    ("dem_row_slots", C.c_int, [_P, _U, _U, C.POINTER(_U), C.POINTER(_U), _P]),
     ("dem_step", C.c_int, [_P, _U, _P]),
     ("dem_get_cells", C.c_int, [_P, _P, _P, _P]),
     ("dem_check", C.c_int, [_P, _P]),

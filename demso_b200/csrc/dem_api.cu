@@ -351,6 +351,7 @@ struct DemContext {
     size_t renderOwnerWords = 0;
     bool keysValid = false;  // keys[] holds the cell of every particle of the current state
     bool haveOrder = false;  // the last step recorded its movers: incremental sort possible
+    bool inSortOrder = false;  // the state is in the order of its last sort (skey/first[cur])
     float rmax = INFINITY;   // largest radius of the current state (culling bound)
     cudaStream_t capStream = nullptr, bodyStream = nullptr;
     // capture-time fork of the sort phase: the full path's branch
@@ -1086,6 +1087,7 @@ bool has_state_sets(const DemContext* c) { return c->dyn[0].pos != nullptr; }
 // in dyn[0].pos): clears the error word, reads the largest radius back and
 // keeps or drops the captured graphs.
 int accept_state(DemContext* c, uint32_t n, cudaStream_t st) {
+    c->inSortOrder = false;
     // the new state replaces the one any recorded error was about
     DEM_TRY_CUDA(cudaMemsetAsync(c->errFlag, 0, 4, st), "clear error word");
     const int a = c->cur;
@@ -1315,6 +1317,7 @@ int step_direct(DemContext* c, uint32_t nsteps, cudaStream_t st) {
         }
         c->cur ^= 1;
         c->haveOrder = true;
+        c->inSortOrder = true;
     }
     return DEM_OK;
 }
@@ -1392,6 +1395,7 @@ extern "C" int dem_step(DemContext* c, uint32_t nsteps, void* stream) {
         }
         c->cur ^= 1;
         c->haveOrder = true;
+        c->inSortOrder = true;
     }
     return DEM_OK;
 }
@@ -1433,6 +1437,30 @@ extern "C" int dem_get_cells(DemContext* c, uint32_t* cellStart, uint32_t* cellE
     DEM_TRY_CUDA(launch_unpack_cells(c->cells[c->cur], c->numCells, cellStart, cellEnd,
                                      (cudaStream_t)stream),
                  "unpack cells");
+    return DEM_OK;
+}
+
+extern "C" int dem_row_slots(DemContext* c, uint32_t rowLo, uint32_t rowHi, uint32_t* first,
+                             uint32_t* count, void* stream) {
+    if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
+    if (c->nspec) return fail(DEM_ERR_INVALID_ARG, "dem_row_slots takes a single scene");
+    if (!first || !count) return fail(DEM_ERR_INVALID_ARG, "dem_row_slots: NULL output");
+    const uint32_t gx = c->sys.gridSize[0], gy = c->sys.gridSize[1];
+    if (rowLo > rowHi || rowHi > gy)
+        return fail(DEM_ERR_INVALID_ARG, "rows [%u, %u) outside the grid's %u rows", rowLo, rowHi,
+                    gy);
+    if (!c->inSortOrder)
+        return fail(DEM_ERR_INVALID_ARG, "the state is not in the order of a sort: step first");
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint32_t* f = c->first[c->cur];
+    uint32_t w[2];
+    DEM_TRY_CUDA(cudaMemcpyAsync(&w[0], f + (size_t)rowLo * gx, 4, cudaMemcpyDeviceToHost, st),
+                 "row slots");
+    DEM_TRY_CUDA(cudaMemcpyAsync(&w[1], f + (size_t)rowHi * gx, 4, cudaMemcpyDeviceToHost, st),
+                 "row slots");
+    DEM_TRY_CUDA(cudaStreamSynchronize(st), "row slots sync");
+    *first = w[0];
+    *count = w[1] - w[0];
     return DEM_OK;
 }
 
@@ -1813,6 +1841,7 @@ int step_recorded(DemContext* c, cudaStream_t st, char* rec) {
                      "record");
     c->cur ^= 1;
     c->haveOrder = true;
+    c->inSortOrder = true;
     return DEM_OK;
 }
 
@@ -1832,6 +1861,7 @@ int restore_checkpoint(DemContext* c, const Snapshot& s, cudaStream_t st) {
     DEM_TRY_CUDA(cudaMemcpyAsync(c->stat[a].id, s.id, 4 * n, cudaMemcpyDeviceToDevice, st), "restore id");
     c->keysValid = false;
     c->haveOrder = false;
+    c->inSortOrder = false;
     return DEM_OK;
 }
 

@@ -213,6 +213,39 @@ def plain_at_scale(n=4194304, seed=0, grid="2r", dt=2e-6, phi=0.55) -> Scene:
                    name="plain_at_scale_%d" % n)
 
 
+def stacked(scene: Scene, copies: int, by_cell: bool = False) -> Scene:
+    """`copies` of a scene stacked upward in one box of the same width and
+    `copies` times the height, on one grid of the same cells (copies a power
+    of two).  Disks are numbered copy by copy, or in cell order with
+    `by_cell`."""
+    if copies == 1:
+        return scene
+    if copies < 1 or copies & (copies - 1):
+        raise ValueError("copies must be a power of two (the grid's rows are)")
+    b = scene.sys
+    sys = System(Lx=b.Lx, Ly=b.Ly * copies, gx=b.gx, gy=b.gy * copies, dt=b.dt,
+                 gravity=b.gravity, knWall=b.knWall, ktWall=b.ktWall, materials=b.materials)
+    pos = np.concatenate([scene.pos.astype(np.float64) + np.array([0.0, c * b.Ly])
+                          for c in range(copies)]).astype(np.float32)
+    tile = lambda a: None if a is None else np.concatenate([a] * copies)
+    vel, radius = tile(scene.vel), tile(scene.radius)
+    omega, theta, type_ = tile(scene.omega), tile(scene.theta), tile(scene.type)
+    if by_cell:
+        order = np.argsort(cell_hash(pos, sys), kind="stable")
+        pos, vel, radius, omega, theta = (a[order] for a in (pos, vel, radius, omega, theta))
+        type_ = None if type_ is None else type_[order]
+    return _finish(sys, pos, vel, radius, omega=omega, theta=theta, type_=type_,
+                   name="%s_x%d" % (scene.name, copies))
+
+
+def stacked_plain(n=4194304, copies=1, seed=0, dt=2e-6) -> Scene:
+    """The workload of a slab decomposition over `copies` GPUs: `copies`
+    plain-at-scale scenes of n disks (n per GPU) stacked upward, numbered
+    in cell order.  Copies do not overlap: each copy's disks lie inside its
+    own walls."""
+    return stacked(plain_at_scale(n, seed=seed, dt=dt), copies, by_cell=True)
+
+
 def cell_hash(pos, sys: System) -> np.ndarray:
     """The reference's cell index of each position (particles_kernel.cuh:114-130),
     with the same float32 operations."""

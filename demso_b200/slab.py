@@ -1,38 +1,52 @@
 """Multi-GPU slab decomposition of the plain step, one process per GPU.
 
-The cell grid is cut into slabs of whole cell rows, one per rank, balanced
-by particle count at the start.  Cells are numbered row by row, so rank r's
-cells are one contiguous range of cell keys, and the global sorted order of
-the reference's step (a stable sort by cell key) is the concatenation of the
-ranks' own sorted orders.  Each step, on every rank:
+The cell grid is cut into slabs of whole cell rows, one per rank, balanced by
+particle count at the start (``partition_rows``).  Cells are numbered row by
+row, so the particles of rank r's rows [y0, y1) are one contiguous range of
+the global sorted order, and the global order is the concatenation of the
+ranks' ranges.
 
-1. the cell key of every particle is computed; particles whose row now
-   belongs to another rank are sent there (torch.distributed send/recv, NCCL
-   over NVLink on GPUs);
-2. the particles received from every rank are concatenated in rank order --
-   the order they hold in the global sorted order of the previous step --
-   with the rank's own staying particles in their place, and stably sorted
-   by key: exactly the global stable sort restricted to the slab;
-3. the slab's bottom row goes to rank r - 1 and its top row to rank r + 1 as
-   ghosts; [ghosts below] + [slab] + [ghosts above] is then a contiguous
-   window of the global sorted state, and the collide over it gives every
-   slab particle the forces of the single-domain step, in the same order
-   (the 3x3 neighbourhood of a slab cell lies in the window; cells beyond it
-   are more than one row away and, across the grid's periodic wrap, a box
-   height away, so they hold no contact);
-4. the slab's particles are integrated.
+Each rank steps a *window*: its own rows plus ``halo`` rows on either side,
+with the library's fused context (incremental sort, collide, integrate and
+next hash on the GPU, replayed as CUDA graphs) -- the single-GPU hot path,
+unchanged.  The window is the single-domain scene cut at its edges, so a
+particle near a cut misses its neighbours beyond it and drifts from the
+single-domain result.  That error reaches at most two more rows a step: one
+through the 3 x 3 cell neighbourhood and one through the particle's own
+displacement, which is below one cell per step (the reference's own 3 x 3
+search rests on the same bound).  With ``halo = 2 * period + 2`` rows every
+own row is still exact after ``period`` steps.  The ranks then exchange bands:
+each sends its ``halo`` lowest own rows to rank r - 1 and its ``halo`` highest
+own rows to rank r + 1 (NCCL send/recv over NVLink on GPUs), and rebuilds its
+window as [rows from below] + [own rows] + [rows from above].
 
-The result is the single-domain step bit for bit.  The compute runs through
-a backend with four operations (cell keys, stable order, cell ranges +
-collide, integrate): ``CudaBackend`` uses the library's per-stage entry
-points on CUDA tensors; the tests also drive the same decomposition with the
-CPU oracle over gloo.
+Rows are cut by the keys of the last sort, which ordered every window, so each
+part is a contiguous slot range (``dem_row_slots``), in the global order
+restricted to it, and the rebuilt window is the global sorted state
+restricted to the window.  Its next sort, a stable sort of that order, is the
+global stable sort restricted: the decomposition reproduces the
+single-domain step bit for bit.
+
+A window's particle count changes with every rebuild (particles cross slab
+boundaries).  The context keeps a fixed count, so that its captured graphs
+stay valid: the window is padded with parked particles, one per cell in rows
+two or more rows away from the window (no window particle ever visits their
+cells), at rest; one of them has the scene's largest radius, so the
+context's largest radius never changes either.  Particles carry window-local
+ids (the context indexes loc by id) and a table back to the global ids.
+
+``run`` drives one rank over ``torch.distributed`` (``DistExchange``);
+``run_group`` drives several slabs in one process, exchanging through local
+copies (``LocalExchange``), which tests the decomposition on one GPU.  The
+stepping is behind a small interface (``ContextStepper`` on the GPU; the tests
+add one over the CPU oracle and run the same code over gloo).
 """
 from __future__ import annotations
 
 import numpy as np
 
 FIELDS = ("pos", "vel", "theta", "omega", "radius", "mass", "id", "type")
+ROW_WIDTH = 10  # packed row: pos(2) vel(2) theta omega radius mass, id and type bits
 
 
 def partition_rows(row_counts, world: int):
@@ -54,268 +68,408 @@ def partition_rows(row_counts, world: int):
     return bounds
 
 
+def halo_rows(period: int) -> int:
+    """Rows a window holds on either side of its slab for `period` steps
+    between exchanges."""
+    return 2 * int(period) + 2
+
+
+def check_bounds(bounds, halo: int):
+    """Every slab needs 2 * halo + 3 rows: its two bands are disjoint and a
+    window leaves rows free for the parked particles."""
+    for r in range(len(bounds) - 1):
+        if bounds[r + 1] - bounds[r] < 2 * halo + 3 and len(bounds) > 2:
+            raise ValueError("slab %d has %d rows; the halo of %d rows needs %d" %
+                             (r, bounds[r + 1] - bounds[r], halo, 2 * halo + 3))
+
+
 def pack(st: dict):
-    """(m, 10) float32 rows: pos, vel, theta, omega, radius, mass, then the
-    id and type words as raw bits."""
+    """(m, ROW_WIDTH) float32 rows of a state dict of torch tensors."""
     import torch
     m = st["pos"].shape[0]
-    typ = st["type"] if st.get("type") is not None else torch.zeros(m, dtype=torch.int32,
-                                                                     device=st["pos"].device)
-    cols = [st["pos"], st["vel"], st["theta"][:, None], st["omega"][:, None],
-            st["radius"][:, None], st["mass"][:, None], st["id"].view(torch.float32)[:, None],
-            typ.view(torch.float32)[:, None]]
+    typ = st.get("type")
+    if typ is None:
+        typ = torch.zeros(m, dtype=torch.int32, device=st["pos"].device)
+    cols = [st["pos"].reshape(m, 2), st["vel"].reshape(m, 2), st["theta"][:, None],
+            st["omega"][:, None], st["radius"][:, None], st["mass"][:, None],
+            st["id"].view(torch.float32)[:, None], typ.view(torch.float32)[:, None]]
     return torch.cat(cols, dim=1).contiguous()
 
 
 def unpack(rows, typed: bool) -> dict:
     import torch
-    rows = rows.contiguous()
-    st = {"pos": rows[:, 0:2].contiguous(), "vel": rows[:, 2:4].contiguous(),
-          "theta": rows[:, 4].contiguous(), "omega": rows[:, 5].contiguous(),
-          "radius": rows[:, 6].contiguous(), "mass": rows[:, 7].contiguous(),
-          "id": rows[:, 8].contiguous().view(torch.int32),
-          "type": rows[:, 9].contiguous().view(torch.int32) if typed else None}
-    return st
+    return {"pos": rows[:, 0:2].contiguous(), "vel": rows[:, 2:4].contiguous(),
+            "theta": rows[:, 4].contiguous(), "omega": rows[:, 5].contiguous(),
+            "radius": rows[:, 6].contiguous(), "mass": rows[:, 7].contiguous(),
+            "id": rows[:, 8].contiguous().view(torch.int32),
+            "type": rows[:, 9].contiguous().view(torch.int32) if typed else None}
 
 
-def take(st: dict, idx) -> dict:
-    return {k: (None if v is None else v[idx].contiguous()) for k, v in st.items()}
+def fields(part, typed: bool) -> dict:
+    """A window part as a dict of per-field tensors: packed rows (a band
+    received from a neighbour) are unpacked, dicts pass through."""
+    return part if isinstance(part, dict) else unpack(part, typed)
 
 
-class Exchange:
-    """Variable-size row exchange between ranks (torch.distributed)."""
+def concat(parts, typed: bool) -> dict:
+    """Parts (packed rows or field dicts) joined field by field."""
+    import torch
+    fs = [fields(p, typed) for p in parts if p is not None]
+    out = {}
+    for k in FIELDS:
+        if k == "type" and not typed:
+            out[k] = None
+            continue
+        out[k] = torch.cat([f[k] for f in fs])  # a new tensor, even from one part
+    return out
+
+
+def cell_rows(sys, pos) -> np.ndarray:
+    """Grid row of each position (the reference's calcGridPos, as
+    scenes.cell_hash computes it)."""
+    from .scenes import cell_hash
+    return (cell_hash(np.asarray(pos, np.float32), sys) >> np.uint32(sys.gx.bit_length() - 1)
+            ).astype(np.int64)
+
+
+class HaloSlab:
+    """Rank `rank`'s slab: own rows bounds[rank] .. bounds[rank + 1] and a
+    window of `halo` more rows on either side, stepped by `stepper`."""
+
+    def __init__(self, sys, rank: int, world: int, bounds, period: int, stepper, halo=None):
+        self.sys, self.rank, self.world = sys, rank, world
+        self.bounds = list(bounds)
+        self.period = int(period)
+        if world == 1:
+            self.halo = 0
+        else:
+            self.halo = halo_rows(period) if halo is None else int(halo)
+        check_bounds(self.bounds, self.halo)
+        self.y0, self.y1 = self.bounds[rank], self.bounds[rank + 1]
+        self.wlo = max(0, self.y0 - self.halo)
+        self.whi = min(sys.gy, self.y1 + self.halo)
+        self.stepper = stepper
+        self.rebuilds = 0
+        self.moved_rows = 0  # rows received from the neighbours, all exchanges
+
+    def load(self, state_all: dict):
+        """The window's particles of a global state (host arrays, any
+        order), in that order."""
+        rows = cell_rows(self.sys, state_all["pos"])
+        keep = np.nonzero((rows >= self.wlo) & (rows < self.whi))[0]
+        part = {k: (None if v is None else np.ascontiguousarray(np.asarray(v)[keep]))
+                for k, v in state_all.items() if k in FIELDS}
+        self.stepper.set_window([self.stepper.from_host(part)], (self.wlo, self.whi))
+
+    def advance(self, k: int):
+        self.stepper.step(int(k))
+
+    def _rows(self, lo: int, hi: int, packed: bool = True):
+        first, count = self.stepper.slots(lo, hi)
+        return self.stepper.take(first, count, packed)
+
+    def bands(self):
+        """(rows for rank - 1, rows for rank + 1): the slab's `halo` lowest and
+        highest rows, by the keys of the last sort."""
+        down = self._rows(self.y0, self.y0 + self.halo) if self.rank > 0 else None
+        up = self._rows(self.y1 - self.halo, self.y1) if self.rank < self.world - 1 else None
+        return down, up
+
+    def own(self, packed: bool = True):
+        """The slab's own rows in the global order restricted to them:
+        packed rows, or a dict of per-field tensors."""
+        return self._rows(self.y0, self.y1, packed)
+
+    def rebuild(self, below, above):
+        """New window: rows from rank - 1, own rows, rows from rank + 1."""
+        self.moved_rows += sum(int(p.shape[0]) for p in (below, above) if p is not None)
+        self.stepper.set_window([below, self.own(packed=False), above], (self.wlo, self.whi))
+        self.rebuilds += 1
+
+
+class LocalExchange:
+    """Bands between slabs held by one process (tests the decomposition on
+    one device)."""
+
+    @staticmethod
+    def exchange(outgoing):
+        """outgoing[r] = (down, up) of slab r; returns (below, above) per slab."""
+        n = len(outgoing)
+        return [(outgoing[r - 1][1] if r > 0 else None,
+                 outgoing[r + 1][0] if r < n - 1 else None) for r in range(n)]
+
+
+class DistExchange:
+    """Bands between neighbouring ranks over torch.distributed (NCCL on GPUs,
+    gloo on CPU): the counts first, then the rows, each as one batch of
+    point-to-point operations."""
 
     def __init__(self, rank: int, world: int, device):
         self.rank, self.world, self.device = rank, world, device
 
-    def all_to_all(self, outgoing):
-        """outgoing[d]: (m_d, 10) rows for rank d (own entry kept locally);
-        returns the rows received from every rank, in rank order."""
+    def _swap(self, send, recv_shapes=None):
         import torch
         import torch.distributed as dist
-        counts = torch.tensor([o.shape[0] for o in outgoing], dtype=torch.int64,
+        ops, got = [], {}
+        for peer, t in send.items():
+            ops.append(dist.P2POp(dist.isend, t, peer))
+        for peer, shape in (recv_shapes or {}).items():
+            buf = torch.empty(shape, dtype=torch.float32 if len(shape) == 2 else torch.int64,
                               device=self.device)
-        table = [torch.empty_like(counts) for _ in range(self.world)]
-        dist.all_gather(table, counts)
-        table = torch.stack(table).cpu().numpy()     # table[src, dst]
-        ops, incoming = [], []
-        for src in range(self.world):
-            if src == self.rank:
-                incoming.append(outgoing[src])
-                continue
-            n = int(table[src, self.rank])
-            buf = torch.empty((n, 10), dtype=torch.float32, device=self.device)
-            incoming.append(buf)
-            if n:
-                ops.append(dist.P2POp(dist.irecv, buf, src))
-        for dst in range(self.world):
-            if dst != self.rank and outgoing[dst].shape[0]:
-                ops.append(dist.P2POp(dist.isend, outgoing[dst].contiguous(), dst))
+            got[peer] = buf
+            ops.append(dist.P2POp(dist.irecv, buf, peer))
         if ops:
             for req in dist.batch_isend_irecv(ops):
                 req.wait()
-        return incoming
+        return got
 
-    def neighbours(self, down, up):
-        """Send `down` to rank - 1 and `up` to rank + 1; returns the rows
-        received from rank - 1 and rank + 1 (empty at the ends)."""
+    def exchange(self, down, up):
         import torch
-        empty = lambda: torch.empty((0, 10), dtype=torch.float32, device=self.device)
-        out = [empty() for _ in range(self.world)]
+        peers = {}
         if self.rank > 0:
-            out[self.rank - 1] = down
+            peers[self.rank - 1] = down
         if self.rank < self.world - 1:
-            out[self.rank + 1] = up
-        got = self.all_to_all(out)
-        below = got[self.rank - 1] if self.rank > 0 else empty()
-        above = got[self.rank + 1] if self.rank < self.world - 1 else empty()
+            peers[self.rank + 1] = up
+        counts = {p: torch.tensor([int(t.shape[0])], dtype=torch.int64, device=self.device)
+                  for p, t in peers.items()}
+        got = self._swap(counts, {p: (1,) for p in peers})
+        sizes = {p: int(t.item()) for p, t in got.items()}
+        send = {p: t.to(self.device).contiguous() for p, t in peers.items() if t.shape[0]}
+        rows = self._swap(send, {p: (m, ROW_WIDTH) for p, m in sizes.items() if m})
+        empty = lambda: torch.empty((0, ROW_WIDTH), dtype=torch.float32, device=self.device)
+        below = rows.get(self.rank - 1, empty()) if self.rank > 0 else None
+        above = rows.get(self.rank + 1, empty()) if self.rank < self.world - 1 else None
         return below, above
 
-
-class SlabStep:
-    """One rank's slab of a decomposed scene.  ``state`` holds the rank's
-    particles (torch tensors on the backend's device) in their order of the
-    last step; ``step(k)`` advances k steps; ``gather()`` returns the global
-    sorted state on rank 0 (None elsewhere)."""
-
-    def __init__(self, sys, state_all: dict, rank: int, world: int, backend, bounds=None):
-        import torch
-        self.sys, self.rank, self.world, self.be = sys, rank, world, backend
-        self.typed = state_all.get("type") is not None and len(sys.materials) > 1
-        full = {k: (None if (k == "type" and not self.typed) else
-                    backend.tensor(state_all[k], k)) for k in FIELDS}
-        keys = backend.keys(sys, full).to(torch.int64)
-        rows = keys // sys.gx
-        if bounds is None:
-            counts = torch.bincount(rows.cpu(), minlength=sys.gy).numpy()
-            bounds = partition_rows(counts, world)
-        self.bounds = bounds
-        owner = np.zeros(sys.gy, np.int64)
-        for r in range(world):
-            owner[bounds[r]:bounds[r + 1]] = r
-        self.owner = torch.from_numpy(owner).to(full["pos"].device)
-        self.state = take(full, torch.nonzero(self.owner[rows] == rank).flatten())
-        self.ex = Exchange(rank, world, backend.comm_device)
-        self.migrated = 0
-        self.ghosts = 0
-
-    def _step(self):
-        import torch
-        be, sys = self.be, self.sys
-        st = self.state
-        rows = be.keys(sys, st).to(torch.int64) // sys.gx
-        dest = self.owner[rows]
-        rowsets = pack(st)
-        outgoing = [rowsets[dest == d].to(be.comm_device) for d in range(self.world)]
-        incoming = self.ex.all_to_all(outgoing)
-        self.migrated += sum(int(incoming[s].shape[0]) for s in range(self.world)
-                             if s != self.rank)
-        seq = unpack(torch.cat([t.to(st["pos"].device) for t in incoming]), self.typed)
-        keys = be.keys(sys, seq)
-        perm = be.stable_order(sys, keys)
-        owned = take(seq, perm)
-        krow = keys[perm].to(torch.int64) // sys.gx
-        y0, y1 = self.bounds[self.rank], self.bounds[self.rank + 1]
-        packed = pack(owned)
-        bottom = packed[krow == y0].to(be.comm_device)
-        top = packed[krow == y1 - 1].to(be.comm_device)
-        below, above = self.ex.neighbours(bottom, top)
-        dev = owned["pos"].device
-        lo, m = int(below.shape[0]), int(packed.shape[0])
-        self.ghosts += lo + int(above.shape[0])
-        window = unpack(torch.cat([below.to(dev), packed, above.to(dev)]), self.typed)
-        acc, alpha, pressure = be.collide(sys, window)
-        sl = slice(lo, lo + m)
-        self.state = be.integrate(sys, owned, acc[sl], alpha[sl], pressure[sl])
-
-    def step(self, k: int = 1):
-        for _ in range(int(k)):
-            self._step()
-
-    def gather(self):
-        """The global state in the single-domain sorted order, on rank 0."""
+    def gather(self, rows):
+        """Every rank's rows, concatenated in rank order, on rank 0 (None
+        elsewhere)."""
         import torch
         import torch.distributed as dist
-        rows = pack(self.state).to(self.be.comm_device)
-        empty = lambda: torch.empty((0, 10), dtype=torch.float32, device=self.be.comm_device)
-        out = [empty() for _ in range(self.world)]
-        out[0] = rows
-        got = self.ex.all_to_all(out) if self.world > 1 else [rows]
+        n = torch.tensor([int(rows.shape[0])], dtype=torch.int64, device=self.device)
+        table = [torch.empty_like(n) for _ in range(self.world)]
+        dist.all_gather(table, n)
+        sizes = [int(t.item()) for t in table]
         if self.rank != 0:
+            if sizes[self.rank]:
+                dist.send(rows.to(self.device).contiguous(), 0)
             return None
-        return unpack(torch.cat(got), self.typed)
+        out = [rows.to(self.device)]
+        for src in range(1, self.world):
+            buf = torch.empty((sizes[src], ROW_WIDTH), dtype=torch.float32, device=self.device)
+            if sizes[src]:
+                dist.recv(buf, src)
+            out.append(buf)
+        return torch.cat(out)
 
 
-class CudaBackend:
-    """The library's per-stage entry points (calcHash, sortParticles,
-    reorderDataAndFindCellStart, collide, integrateSystem) on CUDA tensors;
-    collectives over NCCL."""
+def _rounds(steps: int, period: int):
+    done = 0
+    while done < steps:
+        k = min(period, steps - done)
+        done += k
+        yield k, done < steps
 
-    def __init__(self, device="cuda"):
+
+def run(slab: HaloSlab, ex: DistExchange, steps: int):
+    """`steps` steps of one rank's slab, exchanging bands every slab.period
+    steps (every rank calls this with the same arguments)."""
+    for k, more in _rounds(steps, slab.period):
+        slab.advance(k)
+        if more and slab.world > 1:
+            below, above = ex.exchange(*slab.bands())
+            slab.rebuild(below, above)
+
+
+def run_group(slabs, steps: int):
+    """`steps` steps of all slabs of a decomposition held by this process."""
+    period = slabs[0].period
+    for k, more in _rounds(steps, period):
+        for s in slabs:
+            s.advance(k)
+        if more and len(slabs) > 1:
+            got = LocalExchange.exchange([s.bands() for s in slabs])
+            for s, (below, above) in zip(slabs, got):
+                s.rebuild(below, above)
+
+
+class ContextStepper:
+    """A window stepped by the library's context (``Simulation``) on the GPU.
+
+    The window is padded to a fixed particle count (parked particles, see the
+    module docstring) so that the context's graphs survive rebuilds; a window
+    that outgrows the count gets a new context with room to spare."""
+
+    SPARE = 0.05  # capacity above the first window's particle count
+
+    def __init__(self, sys, rmax: float, flags=None, device="cuda"):
         import torch
+        from . import CTX_PRESSURE
+        self.sys = sys
+        self.rmax = float(rmax)
+        self.flags = CTX_PRESSURE if flags is None else flags
         self.device = torch.device(device)
-        self.comm_device = self.device
+        self.typed = len(sys.materials) > 1
+        self.sim = None
+        self.capacity = 0
+        self.gid = None     # global id of every window-local id (-1: parked)
+        self.m = 0          # real particles of the window
+        self._park = None
 
-    def tensor(self, a, field):
+    def from_host(self, part: dict) -> dict:
         import torch
-        a = np.ascontiguousarray(a)
-        if a.dtype == np.uint32:
-            a = a.view(np.int32)
-        return torch.from_numpy(a).to(self.device)
+        t = {}
+        for k in FIELDS:
+            v = part.get(k)
+            if v is None:
+                t[k] = None
+                continue
+            a = np.ascontiguousarray(v)
+            if a.dtype == np.uint32:
+                a = a.view(np.int32)
+            t[k] = torch.from_numpy(a).to(self.device)
+        return t
 
-    def keys(self, sys, st):
+    def _free_rows(self, window):
+        """Rows two or more rows away from the window."""
+        wlo, whi = window
+        return [y for y in range(self.sys.gy) if y < wlo - 1 or y >= whi + 1]
+
+    def _parked(self, count: int, window) -> dict:
+        """`count` parked particles in cells of rows two or more rows away
+        from the window, one per cell (built once per window and count
+        bound, then sliced)."""
         import torch
-        from . import calcHash
-        m = st["pos"].shape[0]
-        h = torch.empty(m, dtype=torch.int32, device=self.device)
-        ix = torch.empty(m, dtype=torch.int32, device=self.device)
-        if m:
-            calcHash(sys, st["pos"], ix, h, m)
-        return h
+        key = window
+        if self._park is None or self._park[0] != key or self._park[1] < count:
+            sys = self.sys
+            free = self._free_rows(window)
+            cells = len(free) * sys.gx
+            size = min(cells, max(count, self.capacity))
+            if count > size:
+                raise ValueError("no room for %d parked particles (%d free cells)" %
+                                 (count, cells))
+            k = np.arange(size)
+            ys = np.asarray(free, np.int64)[k // sys.gx]
+            xs = k % sys.gx
+            cw, ch = sys.Lx / sys.gx, sys.Ly / sys.gy
+            pos = np.stack([(xs + 0.5) * cw, (ys + 0.5) * ch], axis=1).astype(np.float32)
+            radius = np.full(size, min(0.25 * min(cw, ch), self.rmax), np.float32)
+            radius[0] = np.float32(self.rmax)  # keeps the context's largest radius fixed
+            from .scenes import disk_mass
+            dev = self.device
+            st = {"pos": torch.from_numpy(pos).to(dev),
+                  "vel": torch.zeros((size, 2), device=dev),
+                  "theta": torch.zeros(size, device=dev), "omega": torch.zeros(size, device=dev),
+                  "radius": torch.from_numpy(radius).to(dev),
+                  "mass": torch.from_numpy(disk_mass(radius).astype(np.float32)).to(dev),
+                  "id": torch.full((size,), -1, dtype=torch.int32, device=dev),
+                  "type": torch.zeros(size, dtype=torch.int32, device=dev)}
+            self._park = (key, size, st)
+        st = self._park[2]
+        return {k: v[:count] for k, v in st.items()}
 
-    def stable_order(self, sys, keys):
+    def set_window(self, parts, window):
         import torch
-        from . import sortParticles
-        m = keys.shape[0]
-        h = keys.clone()
-        ix = torch.arange(m, dtype=torch.int32, device=self.device)
-        if m:
-            sortParticles(h, ix, m, max(1, sys.key_bits))
-        return ix.to(torch.int64)
+        from . import Simulation
+        # bands that crossed through host memory (a gloo transport) come back
+        parts = [p.to(self.device) if torch.is_tensor(p) else p for p in parts]
+        st = concat(parts, self.typed)
+        m = int(st["pos"].shape[0])
+        parking = bool(self._free_rows(window))
+        # without free rows (one slab) the window is the whole scene: no padding
+        want = int(m * (1.0 + self.SPARE)) + 64 if parking else m
+        if self.sim is None or m + (1 if parking else 0) > self.capacity or \
+                (not parking and m != self.capacity):
+            if self.sim is not None:
+                self.sim.close()
+            self.capacity = want
+            self.sim = Simulation(self.sys, capacity=self.capacity, flags=self.flags)
+        if parking:
+            st = concat([st, self._parked(self.capacity - m, window)], self.typed)
+        self.gid = st["id"]
+        self.m = m
+        ids = torch.arange(self.capacity, dtype=torch.int32, device=self.device)
+        self.sim.set_state(st["pos"], st["vel"], st["theta"], st["omega"], st["radius"],
+                           st["mass"], ids, st["type"] if self.typed else None)
 
-    def collide(self, sys, w):
-        import torch
-        from . import collide, reorderDataAndFindCellStart
-        m = w["pos"].shape[0]
-        nc = sys.num_cells
-        dev = self.device
-        f = lambda *s: torch.empty(*s, dtype=torch.float32, device=dev)
-        i = lambda *s: torch.empty(*s, dtype=torch.int32, device=dev)
-        acc, alpha, pr = f((m, 2)), f(m), f(m)
-        if m == 0:
-            return acc, alpha, pr
-        keys = self.keys(sys, w)
-        ident = torch.arange(m, dtype=torch.int32, device=dev)
-        cs, ce = i(nc), torch.zeros(nc, dtype=torch.int32, device=dev)
-        s = {k: torch.empty_like(v) for k, v in w.items() if v is not None}
-        loc = i(m)  # sortedLoc[id]: the window's particles get local ids here
-        typed = w.get("type") is not None
-        reorderDataAndFindCellStart(sys, cs, ce, s["pos"], s["vel"], s["theta"], s["omega"],
-                                    s["radius"], s["mass"], s["id"], loc,
-                                    s["type"] if typed else None, keys, ident, w["pos"],
-                                    w["vel"], w["theta"], w["omega"], w["radius"], w["mass"],
-                                    ident, w["type"] if typed else None, m, nc)
-        collide(sys, s["pos"], s["vel"], acc, s["omega"], alpha, s["type"] if typed else None,
-                s["radius"], s["mass"], cs, ce, m, nc, pressure=pr)
-        return acc, alpha, pr
+    def step(self, k: int):
+        self.sim.step(k)
 
-    def integrate(self, sys, st, acc, alpha, pressure):
-        from . import integrateSystem
-        out = {k: (None if v is None else v.clone()) for k, v in st.items()}
-        m = out["pos"].shape[0]
-        if m:
-            integrateSystem(sys, out["pos"], out["vel"], acc.contiguous(), out["theta"],
-                            out["omega"], alpha.contiguous(), out["type"], out["radius"],
-                            out["mass"], pressure.contiguous(), m)
-        return out
+    def slots(self, lo: int, hi: int):
+        import ctypes as C
+        from ._lib import check, load
+        f, c = C.c_uint32(0), C.c_uint32(0)
+        check(load().dem_row_slots(self.sim.handle, lo, hi, C.byref(f), C.byref(c), None))
+        return f.value, c.value
+
+    def take(self, first: int, count: int, packed: bool = True):
+        """Slots [first, first + count) of the current state with their
+        global ids: packed rows, or a dict of tensors (views of the state
+        but the ids; valid until the next step or set_window copies them)."""
+        v = self.sim.state_view()
+        sl = slice(first, first + count)
+        st = {k: (None if v.get(k) is None else v[k][sl]) for k in FIELDS}
+        st["id"] = self.gid[st["id"].long()]
+        return pack(st) if packed else st
+
+    def close(self):
+        if self.sim is not None:
+            self.sim.close()
+            self.sim = None
+
+
+def scene_bounds(sys, pos, world: int):
+    """Slab boundaries balancing the particle counts of a global state."""
+    rows = cell_rows(sys, pos)
+    return partition_rows(np.bincount(rows, minlength=sys.gy), world)
 
 
 def main(argv=None):
-    """Plain-at-scale scene decomposed over the ranks of a torchrun launch:
+    """A tall plain-at-scale scene (`ranks` copies of the n-disk scene stacked
+    upward) decomposed over the ranks of a torchrun launch:
 
         torchrun --nproc-per-node N --master-addr 127.0.0.1 -m demso_b200.slab --n 4194304
     """
     import argparse
+    import datetime
     import json
     import os
-    import time
     import torch
     import torch.distributed as dist
     from . import scenes
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=1 << 20)
     ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--period", type=int, default=20)
     args = ap.parse_args(argv)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    import datetime
     dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        sc = scenes.plain_at_scale(args.n)
-        s = SlabStep(sc.sys, sc.state(), rank, world, CudaBackend())
-        s.step(2)
+        sc = scenes.stacked_plain(args.n, world)
+        bounds = scene_bounds(sc.sys, sc.pos, world)
+        slab = HaloSlab(sc.sys, rank, world, bounds, args.period,
+                        ContextStepper(sc.sys, float(sc.radius.max())))
+        slab.load(sc.state())
+        ex = DistExchange(rank, world, torch.device("cuda"))
+        run(slab, ex, 2 * args.period)
         torch.cuda.synchronize()
         dist.barrier()
-        t0 = time.perf_counter()
-        s.step(args.steps)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        run(slab, ex, args.steps)
+        e1.record()
         torch.cuda.synchronize()
-        dt = torch.tensor([time.perf_counter() - t0], device="cuda")
+        dt = torch.tensor([e0.elapsed_time(e1)], device="cuda")
         dist.all_reduce(dt, op=dist.ReduceOp.MAX)
         if rank == 0:
             print(json.dumps({"particles": sc.n, "ranks": world, "steps": args.steps,
-                              "particle_steps_per_s": sc.n * args.steps / float(dt.item()),
-                              "bounds": s.bounds}))
+                              "period": args.period, "halo_rows": slab.halo,
+                              "particle_steps_per_s": sc.n * args.steps / (float(dt.item()) * 1e-3),
+                              "bounds": bounds}))
+        slab.stepper.close()
     finally:
         dist.destroy_process_group()
 

@@ -330,6 +330,15 @@ int dem_debug_fail_allocation(int nth);
 long long dem_debug_live_allocations(void);
 int dem_debug_sort_hold(DemContext* ctx, uint32_t holdTile, uint32_t spinLimit);
 
+/* The slots [*first, *first + *count) of the current state whose cell (the
+ * sort key of the last step's sort, which ordered the state) lies in grid
+ * rows [rowLo, rowHi): one contiguous range, since keys are numbered row by
+ * row.  A slab decomposition cuts its bands and its own rows this way.  Needs
+ * a step since the last dem_set_state / dem_adopt_state; single scenes only;
+ * synchronises `stream`.  No reference counterpart. */
+int dem_row_slots(DemContext* ctx, uint32_t rowLo, uint32_t rowHi, uint32_t* first,
+                  uint32_t* count, void* stream);
+
 /* Number of kernels one dem_step(ctx, 1, ...) launches (library kernels
  * only; the cellStart memset is not counted). */
 int dem_kernels_per_step(DemContext* ctx);
