@@ -396,6 +396,20 @@ struct DemContext {
     uint32_t adjSteps = 0, adjEvery = 0, adjWindows = 0;
     uint32_t adjN = 0;     // particles and largest radius of the checkpointed run
     float adjRmax = 0.0f;  // (the backward restores checkpoints without re-deriving them)
+    // dem_adj_backward's buffers (the window's per-step record, the tangent
+    // and reduction scratch), kept across calls and grown on demand, and its
+    // two loops (recompute pairs of each parity, reverse steps), kept while
+    // the buffers, the record's layout and the caller's cotangent buffers
+    // they were captured with are unchanged
+    void* adjRec = nullptr;
+    size_t adjRecBytes = 0;
+    void* adjTmp = nullptr;
+    size_t adjTmpBytes = 0;
+    cudaGraphExec_t adjRecLoop[2] = {};
+    cudaGraphExec_t adjRevLoop = nullptr;
+    const void* adjRevKey[3] = {};
+    size_t adjRevStepBytes = 0;
+    uint32_t adjRevN = 0;
     // the step kernel's launch shape (step_variant_shape) and its autotuner
     // (DEM_CTX_AUTOTUNE): the first kTuneSteps steps run the variants in turn,
     // each timed by a pair of events, then the one with the smallest median
@@ -423,6 +437,15 @@ void drop_tune_graphs(DemContext* c) {
         }
 }
 
+void drop_adj_graphs(DemContext* c) {
+    for (int p = 0; p < 2; ++p) {
+        if (c->adjRecLoop[p]) cudaGraphExecDestroy(c->adjRecLoop[p]);
+        c->adjRecLoop[p] = nullptr;
+    }
+    if (c->adjRevLoop) cudaGraphExecDestroy(c->adjRevLoop);
+    c->adjRevLoop = nullptr;
+}
+
 void drop_loop_graphs(DemContext* c) {
     for (int p = 0; p < 2; ++p) {
         if (c->loopGraph[p]) cudaGraphExecDestroy(c->loopGraph[p]);
@@ -430,6 +453,7 @@ void drop_loop_graphs(DemContext* c) {
         if (c->followGraph[p]) cudaGraphExecDestroy(c->followGraph[p]);
         c->followGraph[p] = nullptr;
     }
+    drop_adj_graphs(c);
 }
 
 void drop_graphs(DemContext* c) {
@@ -1003,6 +1027,8 @@ extern "C" int dem_destroy(DemContext* c) {
     dev_free(c->followIds);
     dev_free(c->followRing);
     dev_free(c->adjCheck);
+    dev_free(c->adjRec);
+    dev_free(c->adjTmp);
     dev_free(c->renderOwner);
     dev_free(c->ctlBlock);
     dev_free(c->dTable);
@@ -1936,15 +1962,38 @@ extern "C" int dem_adj_backward(DemContext* c, float* lamPos, float* lamVel, flo
     const size_t tmpBytes = 2 * al256(8ull * n) + 2 * al256(4ull * n) + al256(8ull * n) +
                             al256(adj_acc_bytes(n)) + al256(8ull * DEM_ADJ_NUM_COEF * ns) +
                             al256(4ull * (ns + 1));
-    char* rec = nullptr;
-    char* tmp = nullptr;
-    DEM_TRY_CUDA(dev_alloc(&rec, stepBytes * c->adjEvery), "cudaMalloc adjoint record");
-    cudaError_t e = dev_alloc(&tmp, tmpBytes);
-    if (e != cudaSuccess) {
-        dev_free(rec);
-        return cuda_fail(e, "cudaMalloc adjoint scratch");
+    // the record and scratch persist in the context; a loop captured with
+    // other buffers, another record layout or other cotangent buffers is
+    // rebuilt
+    const size_t recBytes = stepBytes * c->adjEvery;
+    if (c->adjRecBytes < recBytes || c->adjTmpBytes < tmpBytes) drop_adj_graphs(c);
+    if (c->adjRecBytes < recBytes) {
+        dev_free(c->adjRec);
+        c->adjRec = nullptr;
+        c->adjRecBytes = 0;
+        DEM_TRY_CUDA(dev_alloc(&c->adjRec, recBytes), "cudaMalloc adjoint record");
+        c->adjRecBytes = recBytes;
     }
-    char* q = tmp;
+    if (c->adjTmpBytes < tmpBytes) {
+        dev_free(c->adjTmp);
+        c->adjTmp = nullptr;
+        c->adjTmpBytes = 0;
+        DEM_TRY_CUDA(dev_alloc(&c->adjTmp, tmpBytes), "cudaMalloc adjoint scratch");
+        c->adjTmpBytes = tmpBytes;
+    }
+    if (c->adjRevStepBytes != stepBytes || c->adjRevN != n) drop_adj_graphs(c);
+    if (c->adjRevKey[0] != lamPos || c->adjRevKey[1] != lamVel || c->adjRevKey[2] != lamOmega) {
+        if (c->adjRevLoop) cudaGraphExecDestroy(c->adjRevLoop);
+        c->adjRevLoop = nullptr;
+    }
+    c->adjRevStepBytes = stepBytes;
+    c->adjRevN = n;
+    c->adjRevKey[0] = lamPos;
+    c->adjRevKey[1] = lamVel;
+    c->adjRevKey[2] = lamOmega;
+    char* rec = static_cast<char*>(c->adjRec);
+    cudaError_t e = cudaSuccess;
+    char* q = static_cast<char*>(c->adjTmp);
     float2* tlx = reinterpret_cast<float2*>(q); q += al256(8ull * n);
     float2* tlv = reinterpret_cast<float2*>(q); q += al256(8ull * n);
     float* tlw = reinterpret_cast<float*>(q); q += al256(4ull * n);
@@ -1958,7 +2007,8 @@ extern "C" int dem_adj_backward(DemContext* c, float* lamPos, float* lamVel, flo
     if (e == cudaSuccess && first)
         e = cudaMemcpyAsync(first, c->partOff.data(), 4ull * (ns + 1), cudaMemcpyHostToDevice, st);
     const size_t snap = snapshot_bytes(n);
-    cudaGraphExec_t recLoop[2] = {}, revLoop = nullptr;
+    cudaGraphExec_t* recLoop = c->adjRecLoop;
+    cudaGraphExec_t& revLoop = c->adjRevLoop;
     for (int w = (int)c->adjWindows - 1; w >= 0 && rc == DEM_OK && e == cudaSuccess; --w) {
         rc = restore_checkpoint(c, carve_snapshot(static_cast<char*>(c->adjCheck) + snap * w, n),
                                 st);
@@ -2025,15 +2075,14 @@ extern "C" int dem_adj_backward(DemContext* c, float* lamPos, float* lamVel, flo
         }
         e = cudaGraphLaunch(revLoop, st);
     }
-    // (a graph still in flight is freed when it completes)
-    for (cudaGraphExec_t g : {recLoop[0], recLoop[1], revLoop})
-        if (g) cudaGraphExecDestroy(g);
     if (rc == DEM_OK && e == cudaSuccess) e = adj_sum_coef(acc, n, first, ns, sum, st);
     if (rc == DEM_OK && e == cudaSuccess)
         e = cudaMemcpyAsync(grad, sum, 8ull * DEM_ADJ_NUM_COEF * ns, cudaMemcpyDeviceToHost, st);
-    if (rc == DEM_OK && e == cudaSuccess) e = cudaStreamSynchronize(st);
-    dev_free(rec);
-    dev_free(tmp);
+    // the buffers and loops stay for the next call: wait for this one's work
+    // even when it failed part way
+    const cudaError_t es = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = es;
+    if (rc != DEM_OK || e != cudaSuccess) drop_adj_graphs(c);
     if (rc) return rc;
     if (e != cudaSuccess) return cuda_fail(e, "adjoint backward");
     return DEM_OK;

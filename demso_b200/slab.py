@@ -425,12 +425,94 @@ def scene_bounds(sys, pos, world: int):
     return partition_rows(np.bincount(rows, minlength=sys.gy), world)
 
 
+def local_main(args):
+    """The decomposition of `args.local` ranks held by one process on one
+    GPU (slabs stepped one after another, bands exchanged by local copies),
+    timed against the single-domain context on the same scene: the compute
+    cost a rank adds by stepping a halo window and rebuilding it every
+    `period` steps, without the transfers between GPUs.  Prints one JSON
+    line."""
+    import json
+    import torch
+    from . import CTX_PRESSURE, Simulation, scenes
+    world = int(args.local)
+    torch.cuda.set_device(0)
+    sc = scenes.stacked_plain(args.n, world)
+    bounds = scene_bounds(sc.sys, sc.pos, world)
+    rmax = float(sc.radius.max())
+    slabs = [HaloSlab(sc.sys, r, world, bounds, args.period, ContextStepper(sc.sys, rmax))
+             for r in range(world)]
+    for s in slabs:
+        s.load(sc.state())
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    # warm-up: every window's graphs and two exchanges
+    run_group(slabs, 2 * args.period + 3)
+    torch.cuda.synchronize()
+    # timed: `steps` steps in rounds of `period`; the windows' steps and the
+    # rebuilds (band cut, exchange by copies, new window state) timed apart
+    step_ms, rebuild_ms = 0.0, 0.0
+    for k, more in _rounds(args.steps, args.period):
+        a, b, c = ev(), ev(), ev()
+        a.record()
+        for s in slabs:
+            s.advance(k)
+        b.record()
+        if more and world > 1:
+            got = LocalExchange.exchange([s.bands() for s in slabs])
+            for s, (below, above) in zip(slabs, got):
+                s.rebuild(below, above)
+        c.record()
+        torch.cuda.synchronize()
+        step_ms += a.elapsed_time(b)
+        rebuild_ms += b.elapsed_time(c)
+    caps = [s.stepper.capacity for s in slabs]
+    moved = sum(s.moved_rows for s in slabs)
+    for s in slabs:
+        s.stepper.sim.check()
+        s.stepper.close()
+    # the single domain: the fused context on the whole scene
+    t = lambda x: torch.from_numpy(np.ascontiguousarray(x).view(np.int32) if x.dtype == np.uint32
+                                   else np.ascontiguousarray(x))
+    sim = Simulation(sc.sys, capacity=sc.n, flags=CTX_PRESSURE)
+    sim.set_state(t(sc.pos), t(sc.vel), t(sc.theta), t(sc.omega), t(sc.radius), t(sc.mass),
+                  t(sc.id))
+    sim.step(2 * args.period + 3)
+    sim.step(2)
+    sim.step(1)
+    sim.step(2)
+    torch.cuda.synchronize()
+    a, b = ev(), ev()
+    a.record()
+    sim.step(args.steps)
+    b.record()
+    torch.cuda.synchronize()
+    single_ms = a.elapsed_time(b)
+    sim.check()
+    sim.close()
+    rounds = -(-args.steps // args.period)
+    print(json.dumps({
+        "workload": "%d stacked copies of the %d-disk plain-at-scale scene (%d disks, %d x %d "
+                    "grid), %d slabs on one GPU" % (world, args.n, sc.n, sc.sys.gx, sc.sys.gy,
+                                                    world),
+        "steps": args.steps, "period": args.period, "halo_rows": slabs[0].halo,
+        "slab_rows": bounds, "window_capacity": caps,
+        "single_domain_ms_per_step": single_ms / args.steps,
+        "windows_ms_per_step": step_ms / args.steps,
+        "rebuilds_ms_per_step": rebuild_ms / args.steps,
+        "rebuild_ms_each": rebuild_ms / max(1, rounds - 1),
+        "per_rank_ms_per_step": (step_ms + rebuild_ms) / args.steps / world,
+        "per_rank_over_single_share": (step_ms + rebuild_ms) / single_ms,
+        "rows_exchanged_per_round": moved / max(1, rounds - 1)}), flush=True)
+
+
 def main(argv=None):
     """A tall plain-at-scale scene (`ranks` copies of the n-disk scene stacked
     upward) decomposed over the ranks of a torchrun launch:
 
         torchrun --nproc-per-node N --master-addr 127.0.0.1 -m demso_b200.slab --n 4194304
-    """
+
+    With ``--local N`` the N slabs run in this one process on one GPU
+    (``local_main``)."""
     import argparse
     import datetime
     import json
@@ -442,7 +524,11 @@ def main(argv=None):
     ap.add_argument("--n", type=int, default=1 << 20)
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--period", type=int, default=20)
+    ap.add_argument("--local", type=int, default=0,
+                    help="hold this many slabs in one process on one GPU (no torchrun)")
     args = ap.parse_args(argv)
+    if args.local:
+        return local_main(args)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
