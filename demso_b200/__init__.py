@@ -20,12 +20,13 @@ from typing import Optional, Sequence
 
 from . import _lib
 from ._lib import (CTX_ACCEL, CTX_AUTOTUNE, CTX_CALLER_STATE, CTX_DIRECT, CTX_PRESSURE,
+                   CTX_RESIDENT,
                    DEM_MAX_MATERIALS, STATE_PAD, DemError, check, load)
 
 __all__ = ["Material", "System", "DemError", "calcHash", "sortParticles",
            "reorderDataAndFindCellStart", "collide", "integrateSystem", "Simulation", "Batch",
            "sort_scratch_bytes", "load", "CTX_PRESSURE", "CTX_ACCEL", "CTX_DIRECT",
-           "CTX_AUTOTUNE", "CTX_CALLER_STATE", "STATE_PAD"]
+           "CTX_AUTOTUNE", "CTX_CALLER_STATE", "CTX_RESIDENT", "STATE_PAD"]
 
 
 @dataclass

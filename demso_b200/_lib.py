@@ -19,6 +19,7 @@ CTX_ACCEL = 2
 CTX_DIRECT = 4
 CTX_AUTOTUNE = 8
 CTX_CALLER_STATE = 16
+CTX_RESIDENT = 32
 STATE_PAD = 8  # DEM_STATE_PAD
 STEP_VARIANTS = 4  # DEM_STEP_VARIANTS
 NUM_STAGES = 3  # DEM_NUM_STAGES: sort, reorder, collide + integrate

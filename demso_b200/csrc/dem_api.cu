@@ -14,6 +14,7 @@
 #include "dem_common.cuh"
 #include "dem_incsort.cuh"
 #include "dem_kernels.cuh"
+#include "dem_resident.cuh"
 #include "dem_sort.cuh"
 
 using namespace dem;
@@ -401,6 +402,17 @@ struct DemContext {
     // two loops (recompute pairs of each parity, reverse steps), kept while
     // the buffers, the record's layout and the caller's cotangent buffers
     // they were captured with are unchanged
+    // DEM_CTX_RESIDENT (batches): the specimens packed into bins, the bins'
+    // queue word and the blocks' scratch, made at the first resident call;
+    // resPlanned with resBins == 0 means the batch does not fit (a specimen
+    // too large for one bin), and the graph path steps it
+    bool resPlanned = false;
+    uint32_t resBins = 0, resMaxN = 0, resMaxC = 0;
+    int resBlocks = 0;
+    ResBin* dResBins = nullptr;
+    ResEntry* dResEntries = nullptr;
+    uint32_t* resQueue = nullptr;
+    void* resWork = nullptr;
     void* adjRec = nullptr;
     size_t adjRecBytes = 0;
     void* adjTmp = nullptr;
@@ -1029,6 +1041,10 @@ extern "C" int dem_destroy(DemContext* c) {
     dev_free(c->adjCheck);
     dev_free(c->adjRec);
     dev_free(c->adjTmp);
+    dev_free(c->dResBins);
+    dev_free(c->dResEntries);
+    dev_free(c->resQueue);
+    dev_free(c->resWork);
     dev_free(c->renderOwner);
     dev_free(c->ctlBlock);
     dev_free(c->dTable);
@@ -1348,10 +1364,79 @@ int step_direct(DemContext* c, uint32_t nsteps, cudaStream_t st) {
     return DEM_OK;
 }
 
+namespace {
+
+bool has_attraction_host(const KParams& P);
+
+constexpr int kNotResident = -1;
+
+// A multi-step call of a batch created with DEM_CTX_RESIDENT as one
+// persistent launch (dem_resident.cu).  Returns kNotResident, having done
+// nothing, when the batch has types, attraction, a control particle, stage
+// profiling or a specimen too large for one bin: the graph path steps it.
+// After the launch the state is in the order of its last sort, as after the
+// graph path, but no mover record exists: the next graph-path step sorts
+// from scratch (the same permutation, the sort being stable).
+int resident_step(DemContext* c, uint32_t nsteps, cudaStream_t st) {
+    if (c->typed || c->ctlOn || c->profiling || !has_state_sets(c) ||
+        c->partOff.size() != (size_t)c->nspec + 1 || c->partOff.back() != c->n)
+        return kNotResident;
+    for (uint32_t s = 0; s < c->nspec; ++s)
+        if (has_attraction_host(c->hTable[s])) return kNotResident;
+    if (!c->resPlanned) {
+        std::vector<uint32_t> cells(c->nspec);
+        for (uint32_t s = 0; s < c->nspec; ++s) cells[s] = c->hTable[s].gx * c->hTable[s].gy;
+        std::vector<ResEntry> entries;
+        std::vector<ResBin> bins;
+        uint32_t maxN = 0, maxC = 0;
+        c->resPlanned = true;
+        if (!resident_plan(c->partOff, cells, entries, bins, maxN, maxC) || bins.empty()) {
+            c->resBins = 0;
+            return kNotResident;
+        }
+        const int blocks = resident_blocks((uint32_t)bins.size(), c->device);
+        DEM_TRY_CUDA(dev_alloc(&c->dResBins, sizeof(ResBin) * bins.size()), "cudaMalloc bins");
+        DEM_TRY_CUDA(dev_alloc(&c->dResEntries, sizeof(ResEntry) * entries.size()),
+                     "cudaMalloc bin entries");
+        DEM_TRY_CUDA(dev_alloc(&c->resQueue, sizeof(uint32_t)), "cudaMalloc bin queue");
+        DEM_TRY_CUDA(dev_alloc(&c->resWork, resident_work_bytes(maxN) * (size_t)blocks),
+                     "cudaMalloc resident scratch");
+        DEM_TRY_CUDA(cudaMemcpyAsync(c->dResBins, bins.data(), sizeof(ResBin) * bins.size(),
+                                     cudaMemcpyHostToDevice, st),
+                     "bins");
+        DEM_TRY_CUDA(cudaMemcpyAsync(c->dResEntries, entries.data(),
+                                     sizeof(ResEntry) * entries.size(), cudaMemcpyHostToDevice, st),
+                     "bin entries");
+        DEM_TRY_CUDA(cudaStreamSynchronize(st), "bins");
+        c->resBins = (uint32_t)bins.size();
+        c->resMaxN = maxN;
+        c->resMaxC = maxC;
+        c->resBlocks = blocks;
+    }
+    if (c->resBins == 0) return kNotResident;
+    const int a = c->cur;
+    ResIO io{c->dyn[0].pos, c->dyn[a].vel, c->dyn[a].theta, c->dyn[a].omega, c->stat[a].radius,
+             c->stat[a].mass, c->stat[a].id, c->loc, c->pressure, c->acc, c->alpha};
+    DEM_TRY_CUDA(launch_resident(c->dTable, c->dResBins, c->resBins, c->dResEntries, c->resMaxN,
+                                 c->resMaxC, c->resQueue, c->resWork, c->resBlocks, io, c->n,
+                                 nsteps, c->errFlag, st),
+                 "resident step");
+    c->keysValid = false;
+    c->haveOrder = false;
+    c->inSortOrder = false;
+    return DEM_OK;
+}
+
+}  // namespace
+
 extern "C" int dem_step(DemContext* c, uint32_t nsteps, void* stream) {
     if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
     if (nsteps == 0 || c->n == 0) return DEM_OK;
     cudaStream_t st = (cudaStream_t)stream;
+    if (c->nspec && (c->flags & DEM_CTX_RESIDENT)) {
+        int rc = resident_step(c, nsteps, st);
+        if (rc != kNotResident) return rc;
+    }
     if (!c->keysValid) {
         if (c->nspec)
             DEM_TRY_CUDA(launch_calc_hash_batched(c->dTable, c->spec, c->dyn[0].pos, c->keys, c->n,

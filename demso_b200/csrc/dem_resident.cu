@@ -1,0 +1,569 @@
+// Resident batched step (DEM_CTX_RESIDENT): a multi-step dem_step call of a
+// batch runs as ONE persistent launch.  Specimens are packed into bins of up
+// to kResMaxParticles particles and kResMaxCells cells; each thread block
+// (one per multiprocessor, 1024 threads) takes bins from a queue, loads a
+// bin's state into shared memory and runs every step of the call there:
+//
+//   sort     : only when some particle changed cell in the last step (and
+//              on the first step): a stable block-wide sort of the slots by
+//              cell -- one-bit LSD passes over the cell bits that differ,
+//              with warp ballots -- then the first-particle array of every
+//              cell and the state gathered into the new order;
+//   collide  : every particle against the particles of its 3 x 3 cells,
+//              cells y-outer, x-inner, each cell's particles in slot order,
+//              one subtotal per cell (collideD, particles_kernel.cuh:459-549,
+//              with collideCell :346-385 and collideSpheres :236-307), the
+//              neighbours read from shared memory; forces, moments and
+//              pressures to the block's scratch;
+//   integrate: integrateSystemD + collideBoundary (particles_kernel.cuh:
+//              388-456, 580-627) in place, then the particle's new cell.
+//
+// The sort is the reference's stable sort by cell restricted to the bin, and
+// the sums are added in the reference's order, so every specimen follows the
+// same trajectory bit for bit as in the graph path of the batch or alone.
+// Velocities, spins, radii and positions -- what neighbours read -- live in
+// shared memory (24 B per particle); angles, masses and ids are read and
+// written only by the particle's own thread and live in the block's global
+// scratch, which stays in L2.
+#include <algorithm>
+
+#include "dem_resident.cuh"
+
+namespace dem {
+namespace {
+
+constexpr int kResThreads = 1024;
+constexpr int kResWarps = kResThreads / 32;
+constexpr uint32_t kSlotBits = 13;  // bin slots < kResMaxParticles = 2^13
+constexpr uint32_t kSlotMask = (1u << kSlotBits) - 1u;
+constexpr int kResPer = (int)(kResMaxParticles / kResThreads);  // slots per thread
+static_assert(kResMaxParticles == (1u << kSlotBits), "slot field of the sort values");
+static_assert(kResMaxCells <= (1u << kSlotBits), "cell field of the sort values");
+static_assert(kResWarps == 32, "the block scan is one warp over the warps' totals");
+
+inline __host__ __device__ uint32_t round64(uint32_t n) { return (n + 63u) & ~63u; }
+
+// The block's global scratch: the state stashed by the sort, the collide's
+// results, and the angle, mass and id of every slot (two sets: the sort
+// gathers from one into the other).  Arrays of nb (a multiple of 64) words
+// or pairs, addressed from one base so that few registers hold them.
+struct Work {
+    char* base;
+    uint32_t nb;
+    __device__ __forceinline__ float2* stashPos() const { return reinterpret_cast<float2*>(base); }
+    __device__ __forceinline__ float2* stashVel() const {
+        return reinterpret_cast<float2*>(base + 8ull * nb);
+    }
+    __device__ __forceinline__ float2* F() const {
+        return reinterpret_cast<float2*>(base + 16ull * nb);
+    }
+    __device__ __forceinline__ float* stashOm() const {
+        return reinterpret_cast<float*>(base + 24ull * nb);
+    }
+    __device__ __forceinline__ float* stashRad() const {
+        return reinterpret_cast<float*>(base + 28ull * nb);
+    }
+    __device__ __forceinline__ float* M() const { return reinterpret_cast<float*>(base + 32ull * nb); }
+    __device__ __forceinline__ float* Pr() const { return reinterpret_cast<float*>(base + 36ull * nb); }
+    __device__ __forceinline__ float* theta(int k) const {
+        return reinterpret_cast<float*>(base + (40ull + 12ull * k) * nb);
+    }
+    __device__ __forceinline__ float* mass(int k) const {
+        return reinterpret_cast<float*>(base + (44ull + 12ull * k) * nb);
+    }
+    __device__ __forceinline__ uint32_t* id(int k) const {
+        return reinterpret_cast<uint32_t*>(base + (48ull + 12ull * k) * nb);
+    }
+};
+
+__host__ __device__ inline size_t work_bytes_per_block(uint32_t maxN) {
+    return (size_t)64 * round64(maxN);
+}
+
+// Shared memory of a block: positions, velocities, spins, radii (nb each),
+// the first-particle array (round64(maxC + 1) words), the bin's entries and
+// the scan words.  The sort's two value arrays alias the positions, which
+// the sort has stashed first.
+__host__ __device__ inline size_t smem_bytes(uint32_t maxN, uint32_t maxC) {
+    const size_t nb = round64(maxN);
+    return 24 * nb + 4 * (size_t)round64(maxC + 1) + sizeof(ResEntry) * kResMaxEntries +
+           4 * (2 * kResWarps + 4);
+}
+
+extern __shared__ __align__(16) unsigned char smraw[];
+
+struct Smem {
+    uint32_t nb, nc;  // particle and cell capacity of the arrays
+    __device__ __forceinline__ float2* pos() const { return reinterpret_cast<float2*>(smraw); }
+    __device__ __forceinline__ float2* vel() const {
+        return reinterpret_cast<float2*>(smraw + 8u * nb);
+    }
+    __device__ __forceinline__ float* omega() const {
+        return reinterpret_cast<float*>(smraw + 16u * nb);
+    }
+    __device__ __forceinline__ float* radius() const {
+        return reinterpret_cast<float*>(smraw + 20u * nb);
+    }
+    __device__ __forceinline__ uint32_t* first() const {
+        return reinterpret_cast<uint32_t*>(smraw + 24u * nb);
+    }
+    __device__ __forceinline__ ResEntry* ent() const {
+        return reinterpret_cast<ResEntry*>(smraw + 24u * nb + 4u * nc);
+    }
+    __device__ __forceinline__ uint32_t* scan() const {
+        return reinterpret_cast<uint32_t*>(smraw + 24u * nb + 4u * nc +
+                                           (uint32_t)sizeof(ResEntry) * kResMaxEntries);
+    }
+    __device__ __forceinline__ uint32_t* sortA() const { return reinterpret_cast<uint32_t*>(smraw); }
+    __device__ __forceinline__ uint32_t* sortB() const {
+        return reinterpret_cast<uint32_t*>(smraw) + nb;
+    }
+};
+
+// The particle's cell in its specimen's grid, wrapped (calcGridPos +
+// calcGridHash, particles_kernel.cuh:114-130; grid_pos_fast gives the
+// reference's quotient bit for bit).
+__device__ __forceinline__ uint32_t local_cell(const KParams& P, float2 p) {
+    const int2 g = grid_pos_fast(P, p);
+    return (uint32_t)(g.y & (int)(P.gy - 1u)) * P.gx + (uint32_t)(g.x & (int)(P.gx - 1u));
+}
+
+// Entry of a bin slot: the last entry whose first slot is <= i.
+__device__ __forceinline__ uint32_t entry_of(const ResEntry* ent, uint32_t count, uint32_t i) {
+    uint32_t lo = 0, hi = count;  // ent[lo].slot <= i < ent[hi].slot
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (ent[mid].slot <= i) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Stable sort of the n values (cell << kSlotBits | slot) in `a`, by their
+// cell bits: one LSD pass per cell bit on which the values differ
+// (`differ`).  Lane l of warp w holds elements w * 32 * per + k * 32 + l, so
+// each warp's elements are one contiguous run and its ballots give the
+// ranks.  Returns the array holding the sorted values (a or b).
+__device__ uint32_t* block_sort(uint32_t* a, uint32_t* b, uint32_t n, uint32_t differ,
+                                uint32_t* scan) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t per = (n + kResThreads - 1u) / kResThreads;
+    const uint32_t wbase = (uint32_t)warp * 32u * per;
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll 1
+    for (uint32_t bit = kSlotBits; bit < 2 * kSlotBits; ++bit) {
+        if (!((differ >> bit) & 1u)) continue;  // every value agrees here: the pass is the identity
+        uint32_t v[kResPer];
+        unsigned zm[kResPer];
+        uint32_t zeros = 0;
+#pragma unroll
+        for (int k = 0; k < kResPer; ++k) {
+            v[k] = 0u;
+            zm[k] = 0u;
+            if ((uint32_t)k < per) {
+                const uint32_t e = wbase + (uint32_t)k * 32u + (uint32_t)lane;
+                const bool ok = e < n;
+                if (ok) v[k] = a[e];
+                zm[k] = __ballot_sync(0xffffffffu, ok && !((v[k] >> bit) & 1u));
+                zeros += (uint32_t)__popc(zm[k]);
+            }
+        }
+        if (lane == 0) scan[warp] = zeros;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t x = scan[lane];
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+                if (lane >= d) x += y;
+            }
+            scan[kResWarps + lane] = x;  // inclusive
+        }
+        __syncthreads();
+        const uint32_t total0 = scan[2 * kResWarps - 1];
+        const uint32_t zBefore = warp ? scan[kResWarps + warp - 1] : 0u;
+        const uint32_t oBefore = min(n, wbase) - zBefore;
+        uint32_t zr = 0, orr = 0;
+#pragma unroll
+        for (int k = 0; k < kResPer; ++k) {
+            if ((uint32_t)k < per) {
+                const uint32_t e = wbase + (uint32_t)k * 32u + (uint32_t)lane;
+                const bool ok = e < n;
+                const unsigned z = zm[k];
+                const unsigned o = __ballot_sync(0xffffffffu, ok) & ~z;
+                if (ok) {
+                    const uint32_t dst = ((z >> lane) & 1u)
+                                             ? zBefore + zr + (uint32_t)__popc(z & lt)
+                                             : total0 + oBefore + orr + (uint32_t)__popc(o & lt);
+                    b[dst] = v[k];
+                }
+                zr += (uint32_t)__popc(z);
+                orr += (uint32_t)__popc(o);
+            }
+        }
+        uint32_t* t = a;
+        a = b;
+        b = t;
+        __syncthreads();  // the pass is complete before the next one reads it
+    }
+    return a;
+}
+
+// First index of the sorted values whose cell is >= c.
+__device__ __forceinline__ uint32_t lower_cell(const uint32_t* v, uint32_t n, uint32_t c) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if ((v[mid] >> kSlotBits) < c) lo = mid + 1u;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Forces on particle i from its 3 x 3 cells, in the reference's order; the
+// neighbours' fields from shared memory.  With culling (the specimen's
+// cells wider than 2 rmax and the particle inside the box by the margin) a
+// column or row of cells farther than r + rmax is skipped: it holds no
+// contact, and its subtotal would be +0.
+__device__ __forceinline__ void res_collide(const KParams& P, uint32_t cellOff, uint32_t i,
+                                            float2 p, float2 v, float w, float r, const Smem& S,
+                                            float2& force, float& moment, float& pr) {
+    force = make_float2(0.0f, 0.0f);
+    moment = 0.0f;
+    pr = 0.0f;
+    const int2 gr = grid_pos_fast(P, p);
+    const int gx = gr.x & (int)(P.gx - 1u), gy = gr.y & (int)(P.gy - 1u);
+    int y0 = -1, y1 = 1, x0 = -1, x1 = 1;
+    if (P.cull && p.x > P.cullMargin && p.x < P.Lx - P.cullMargin && p.y > P.cullMargin &&
+        p.y < P.Ly - P.cullMargin) {
+        const float reach = (r + P.rmax) * 1.0001f + P.cullMargin;
+        const float X0 = (float)gx * P.cellW, Y0 = (float)gy * P.cellH;
+        if (p.x - X0 > reach) x0 = 0;
+        if (X0 + P.cellW - p.x > reach) x1 = 0;
+        if (p.y - Y0 > reach) y0 = 0;
+        if (Y0 + P.cellH - p.y > reach) y1 = 0;
+    }
+    const int mx = (int)(P.gx - 1u), my = (int)(P.gy - 1u);
+#pragma unroll 1
+    for (int dy = y0; dy <= y1; ++dy) {
+        const uint32_t row = cellOff + (uint32_t)((gy + dy) & my) * P.gx;
+#pragma unroll 1
+        for (int dx = x0; dx <= x1; ++dx) {
+            const uint32_t h = row + (uint32_t)((gx + dx) & mx);
+            const uint32_t a = S.first()[h], b = S.first()[h + 1];
+            float2 fc = make_float2(0.0f, 0.0f);
+#pragma unroll 1
+            for (uint32_t j = a; j < b; ++j) {
+                if (j == i) continue;
+                const float2 pj = S.pos()[j];
+                const float ax = pj.x - p.x, ay = pj.y - p.y;
+                const float d2 = ax * ax + ay * ay;
+                const float rj = S.radius()[j];
+                const float cd = r + rj;
+                // d2 > cd^2 (1 + 2e-6) implies sqrtf(d2) >= cd: no contact
+                if (d2 <= cd * cd * 1.000002f && sqrtf(d2) < cd) {
+                    const float2 f = pair_force(p, pj, v, S.vel()[j], w, S.omega()[j], r, rj,
+                                                P.pair[0], P.dt, moment, pr);
+                    fc.x += f.x;
+                    fc.y += f.y;
+                }
+            }
+            force.x += fc.x;
+            force.y += fc.y;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kResThreads, 1)
+resident_kernel(const KParams* __restrict__ table, const ResBin* __restrict__ bins,
+                uint32_t numBins, const ResEntry* __restrict__ entries,
+                uint32_t* __restrict__ queue, uint32_t maxN, uint32_t maxC, char* workBase,
+                ResIO io, uint32_t nTotal, uint32_t nsteps, uint32_t* __restrict__ errFlag) {
+    __shared__ uint32_t sBin;
+    const Smem S{round64(maxN), round64(maxC + 1)};
+    const Work W{workBase + work_bytes_per_block(maxN) * blockIdx.x, round64(maxN)};
+    const uint32_t tid = threadIdx.x;
+#pragma unroll 1
+    for (;;) {
+        __syncthreads();  // the previous bin is written back
+        if (tid == 0) sBin = atomicAdd(queue, 1u);
+        __syncthreads();
+        const uint32_t bi = sBin;
+        if (bi >= numBins) break;
+        const ResBin bin = bins[bi];
+        const uint32_t n = bin.n, ne = bin.count;
+        if (tid < ne) S.ent()[tid] = entries[bin.first + tid];
+        __syncthreads();
+        // the bin's state: each specimen's slots of the batch into its slots
+        // of the bin
+#pragma unroll 1
+        for (uint32_t e = 0; e < ne; ++e) {
+            const ResEntry E = S.ent()[e];
+#pragma unroll 1
+            for (uint32_t j = tid; j < E.n; j += kResThreads) {
+                const uint32_t s = E.slot + j, g = E.gslot + j;
+                S.pos()[s] = io.pos[g];
+                S.vel()[s] = io.vel[g];
+                S.omega()[s] = io.omega[g];
+                S.radius()[s] = io.radius[g];
+                W.theta(0)[s] = io.theta[g];
+                W.mass(0)[s] = io.mass[g];
+                W.id(0)[s] = io.id[g];
+            }
+        }
+        // the entry of each slot this thread owns (slots tid + k * 1024),
+        // 8 bits each
+        const uint32_t per = (n + kResThreads - 1u) / kResThreads;
+        uint32_t entPack[2] = {0u, 0u};
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kResPer; ++k) {
+            const uint32_t i = tid + (uint32_t)k * kResThreads;
+            if ((uint32_t)k < per && i < n)
+                entPack[k >> 2] |= entry_of(S.ent(), ne, i) << ((k & 3) * 8);
+        }
+        int buf = 0;
+        bool needSort = true;
+#pragma unroll 1
+        for (uint32_t step = 0; step < nsteps; ++step) {
+            if (needSort) {
+                // ---- sort.  The state is stashed first, so that the value
+                // arrays may overwrite the positions; the values (cell << 13 |
+                // slot) are then made from the stashed positions.
+#pragma unroll 1
+                for (int k = 0; k < kResPer; ++k) {
+                    const uint32_t i = tid + (uint32_t)k * kResThreads;
+                    if ((uint32_t)k >= per || i >= n) break;
+                    W.stashPos()[i] = S.pos()[i];
+                    W.stashVel()[i] = S.vel()[i];
+                    W.stashOm()[i] = S.omega()[i];
+                    W.stashRad()[i] = S.radius()[i];
+                }
+                if (tid == 0) {
+                    S.scan()[2 * kResWarps] = 0u;
+                    S.scan()[2 * kResWarps + 1] = 0xffffffffu;
+                }
+                __syncthreads();  // stash complete, words initialised
+                uint32_t orv = 0u, andv = 0xffffffffu;
+#pragma unroll 1
+                for (int k = 0; k < kResPer; ++k) {
+                    const uint32_t i = tid + (uint32_t)k * kResThreads;
+                    if ((uint32_t)k >= per || i >= n) break;
+                    const ResEntry& E = S.ent()[(entPack[k >> 2] >> ((k & 3) * 8)) & 0xffu];
+                    const uint32_t v =
+                        ((E.cellOff + local_cell(table[E.spec], W.stashPos()[i])) << kSlotBits) | i;
+                    S.sortA()[i] = v;
+                    orv |= v;
+                    andv &= v;
+                }
+                orv = __reduce_or_sync(0xffffffffu, orv);
+                andv = __reduce_and_sync(0xffffffffu, andv);
+                if ((tid & 31) == 0) {
+                    atomicOr(&S.scan()[2 * kResWarps], orv);
+                    atomicAnd(&S.scan()[2 * kResWarps + 1], andv);
+                }
+                __syncthreads();
+                // the cell bits on which the values differ (the passes use
+                // other scan words)
+                const uint32_t differ = S.scan()[2 * kResWarps] & ~S.scan()[2 * kResWarps + 1];
+                const uint32_t* sorted = block_sort(S.sortA(), S.sortB(), n, differ, S.scan());
+                // first particle of every cell of the bin (bin.cells + 1
+                // entries); each new slot's old slot to the scratch
+#pragma unroll 1
+                for (uint32_t c = tid; c <= bin.cells; c += kResThreads)
+                    S.first()[c] = lower_cell(sorted, n, c);
+                uint32_t* from = reinterpret_cast<uint32_t*>(W.M());
+#pragma unroll 1
+                for (int k = 0; k < kResPer; ++k) {
+                    const uint32_t i = tid + (uint32_t)k * kResThreads;
+                    if ((uint32_t)k >= per || i >= n) break;
+                    from[i] = sorted[i] & kSlotMask;
+                }
+                __syncthreads();  // the values are read; the state arrays are free
+#pragma unroll 1
+                for (int k = 0; k < kResPer; ++k) {
+                    const uint32_t i = tid + (uint32_t)k * kResThreads;
+                    if ((uint32_t)k >= per || i >= n) break;
+                    const uint32_t f = from[i];
+                    S.pos()[i] = W.stashPos()[f];
+                    S.vel()[i] = W.stashVel()[f];
+                    S.omega()[i] = W.stashOm()[f];
+                    S.radius()[i] = W.stashRad()[f];
+                    W.theta(buf ^ 1)[i] = W.theta(buf)[f];
+                    W.mass(buf ^ 1)[i] = W.mass(buf)[f];
+                    W.id(buf ^ 1)[i] = W.id(buf)[f];
+                }
+                buf ^= 1;
+                __syncthreads();
+            }
+            // ---- collide: forces from the neighbours' current state
+#pragma unroll 1
+            for (int k = 0; k < kResPer; ++k) {
+                const uint32_t i = tid + (uint32_t)k * kResThreads;
+                if ((uint32_t)k >= per || i >= n) break;
+                const ResEntry& E = S.ent()[(entPack[k >> 2] >> ((k & 3) * 8)) & 0xffu];
+                const KParams& P = table[E.spec];
+                float2 f;
+                float moment, pr;
+                res_collide(P, E.cellOff, i, S.pos()[i], S.vel()[i], S.omega()[i], S.radius()[i], S, f,
+                            moment, pr);
+                W.F()[i] = f;
+                W.M()[i] = moment;
+                W.Pr()[i] = pr;
+            }
+            __syncthreads();
+            // ---- integrate in place (each thread reads and writes only its
+            // own slots), then the new cell
+            const bool last = step + 1u == nsteps;
+            bool mover = false;
+#pragma unroll 1
+            for (int k = 0; k < kResPer; ++k) {
+                const uint32_t i = tid + (uint32_t)k * kResThreads;
+                if ((uint32_t)k >= per || i >= n) break;
+                const ResEntry& E = S.ent()[(entPack[k >> 2] >> ((k & 3) * 8)) & 0xffu];
+                const KParams& P = table[E.spec];
+                Dyn s;
+                s.p = S.pos()[i];
+                s.v = S.vel()[i];
+                s.w = S.omega()[i];
+                s.th = W.theta(buf)[i];
+                const float r = S.radius()[i];
+                const float m = W.mass(buf)[i];
+                const float2 f = W.F()[i];
+                const float moment = W.M()[i];
+                float pr = W.Pr()[i];
+                const uint32_t cellBefore = local_cell(P, s.p);
+                // F/m and M/I as the reference divides them; without contacts
+                // F and M are +0 and the quotients exactly +0 (the step
+                // kernel's shortcut, the same bits)
+                const bool quiet = f.x == 0.0f && f.y == 0.0f && moment == 0.0f && m > 0.0f &&
+                                   m < INFINITY;
+                const float two_mrr = 2.0f * m * r * r;
+                float2 a;
+                float al;
+                if (quiet && two_mrr >= 1e-30f && two_mrr <= 1e30f) {
+                    a = make_float2(0.0f, 0.0f);
+                    al = 0.0f;
+                } else {
+                    a = make_float2(f.x / m, f.y / m);
+                    al = moment / inertia_of(m, r);
+                }
+                integrate_one(P, s, a, al, r, m, 0u, pr);
+                S.pos()[i] = s.p;
+                S.vel()[i] = s.v;
+                S.omega()[i] = s.w;
+                W.theta(buf)[i] = s.th;
+                if (!(isfinite(s.p.x) && isfinite(s.p.y))) atomicOr(errFlag, 1u);
+                if (local_cell(P, s.p) != cellBefore) mover = true;
+                if (last) {
+                    const uint32_t g = E.gslot + (i - E.slot);
+                    if (io.pressure) io.pressure[g] = pr;
+                    if (io.acc) io.acc[g] = a;
+                    if (io.alpha) io.alpha[g] = al;
+                }
+            }
+            needSort = __syncthreads_or(mover) != 0;
+        }
+        // the bin's state back into the batch, in the order of its last sort
+#pragma unroll 1
+        for (uint32_t e = 0; e < ne; ++e) {
+            const ResEntry E = S.ent()[e];
+#pragma unroll 1
+            for (uint32_t j = tid; j < E.n; j += kResThreads) {
+                const uint32_t s = E.slot + j, g = E.gslot + j;
+                io.pos[g] = S.pos()[s];
+                io.vel[g] = S.vel()[s];
+                io.omega[g] = S.omega()[s];
+                io.radius[g] = S.radius()[s];
+                io.theta[g] = W.theta(buf)[s];
+                io.mass[g] = W.mass(buf)[s];
+                const uint32_t id = W.id(buf)[s];
+                io.id[g] = id;
+                if (id < nTotal) io.loc[id] = g;  // ids outside 0..N-1 have no loc entry
+            }
+        }
+    }
+}
+
+}  // namespace
+
+bool resident_plan(const std::vector<uint32_t>& partOff, const std::vector<uint32_t>& cells,
+                   std::vector<ResEntry>& entries, std::vector<ResBin>& bins, uint32_t& maxN,
+                   uint32_t& maxC) {
+    const uint32_t ns = (uint32_t)cells.size();
+    if (partOff.size() != (size_t)ns + 1u) return false;
+    std::vector<uint32_t> order(ns);
+    for (uint32_t s = 0; s < ns; ++s) order[s] = s;
+    auto count = [&](uint32_t s) { return partOff[s + 1] - partOff[s]; };
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t a, uint32_t b) { return count(a) > count(b); });
+    struct Open {
+        uint32_t n, c;
+        std::vector<uint32_t> specs;
+    };
+    std::vector<Open> open;
+    for (uint32_t s : order) {
+        const uint32_t n = count(s), c = cells[s];
+        if (n == 0) continue;  // nothing to step
+        if (n > kResMaxParticles || c > kResMaxCells) return false;
+        size_t b = 0;
+        for (; b < open.size(); ++b)
+            if (open[b].n + n <= kResMaxParticles && open[b].c + c <= kResMaxCells &&
+                open[b].specs.size() < kResMaxEntries)
+                break;
+        if (b == open.size()) open.push_back(Open{0u, 0u, {}});
+        open[b].n += n;
+        open[b].c += c;
+        open[b].specs.push_back(s);
+    }
+    std::stable_sort(open.begin(), open.end(),
+                     [](const Open& a, const Open& b) { return a.n > b.n; });
+    entries.clear();
+    bins.clear();
+    maxN = 0;
+    maxC = 0;
+    for (const Open& o : open) {
+        ResBin b{(uint32_t)entries.size(), (uint32_t)o.specs.size(), o.n, o.c};
+        uint32_t slot = 0, cell = 0;
+        for (uint32_t s : o.specs) {
+            entries.push_back(ResEntry{s, partOff[s], slot, count(s), cell, cells[s]});
+            slot += count(s);
+            cell += cells[s];
+        }
+        bins.push_back(b);
+        maxN = std::max(maxN, o.n);
+        maxC = std::max(maxC, o.c);
+    }
+    return true;
+}
+
+size_t resident_work_bytes(uint32_t maxN) { return work_bytes_per_block(maxN); }
+
+size_t resident_smem_bytes(uint32_t maxN, uint32_t maxC) { return smem_bytes(maxN, maxC); }
+
+int resident_blocks(uint32_t numBins, int device) {
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        sms <= 0)
+        sms = 1;
+    return (int)std::min<uint32_t>(numBins, (uint32_t)sms);
+}
+
+cudaError_t launch_resident(const KParams* table, const ResBin* bins, uint32_t numBins,
+                            const ResEntry* entries, uint32_t maxN, uint32_t maxC,
+                            uint32_t* queue, void* work, int blocks, ResIO io, uint32_t nTotal,
+                            uint32_t nsteps, uint32_t* errFlag, cudaStream_t st) {
+    if (numBins == 0 || nsteps == 0) return cudaSuccess;
+    const size_t smem = smem_bytes(maxN, maxC);
+    cudaError_t e = cudaFuncSetAttribute(resident_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(queue, 0, sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    resident_kernel<<<blocks, kResThreads, smem, st>>>(table, bins, numBins, entries, queue, maxN,
+                                                       maxC, static_cast<char*>(work), io, nTotal,
+                                                       nsteps, errFlag);
+    return cudaGetLastError();
+}
+
+}  // namespace dem

@@ -180,6 +180,9 @@ typedef struct DemContext DemContext;
                                  (dem_get_step_variant) */
 #define DEM_CTX_CALLER_STATE 16u /* allocate no particle state: the caller's buffers
                                     are handed over by dem_adopt_state */
+#define DEM_CTX_RESIDENT 32u  /* batches: run each dem_step call as one persistent
+                                 launch in which every specimen is stepped inside one
+                                 multiprocessor's shared memory (see dem_batch_create) */
 
 int dem_create(const DemSystem* sys, uint32_t capacity, uint32_t flags, DemContext** out);
 int dem_destroy(DemContext* ctx);
@@ -208,7 +211,20 @@ int dem_set_state(DemContext* ctx, uint32_t n, const float* pos, const float* ve
  * Cell keys carry a per-specimen offset, so the one stable sort of the batch
  * is each specimen's own stable sort and every specimen evolves bit for bit
  * as it would alone.  No counterpart in the reference (one scene per
- * process). */
+ * process).
+ *
+ * With DEM_CTX_RESIDENT in `flags`, a dem_step call on the batch is one
+ * persistent kernel launch: the specimens are packed into bins of at most
+ * 8,192 particles, 8,192 cells and 64 specimens, and each thread block (one
+ * per multiprocessor) takes bins from a queue and runs all the call's steps
+ * of a bin inside its shared memory (positions, velocities, spins and radii;
+ * the sort only on steps after a particle changed cell).  The trajectories
+ * are those of the graph path bit for bit.  The first such call packs the
+ * bins and allocates their scratch (about 64 B per particle of the largest
+ * bin, per multiprocessor) and synchronises `stream`.  A batch with more
+ * than one material, attraction, a control particle or a specimen too large
+ * for one bin, and calls made while profiling, take the graph path instead.
+ * After a resident call the next graph-path step sorts from scratch. */
 int dem_batch_create(const DemSystem* specs, uint32_t numSpecimens, uint32_t flags,
                      DemContext** out);
 /* Slots [*firstSlot, *firstSlot + *count) of the state hold specimen s (fixed
