@@ -37,6 +37,9 @@ constexpr int kResWarps = kResThreads / 32;
 constexpr uint32_t kSlotBits = 13;  // bin slots < kResMaxParticles = 2^13
 constexpr uint32_t kSlotMask = (1u << kSlotBits) - 1u;
 constexpr int kResPer = (int)(kResMaxParticles / kResThreads);  // slots per thread
+// Steps on which at most this many particles of a bin changed cell re-sort
+// the bin incrementally; more take the full block sort.
+constexpr uint32_t kResMaxMovers = 32;
 static_assert(kResMaxParticles == (1u << kSlotBits), "slot field of the sort values");
 static_assert(kResMaxCells <= (1u << kSlotBits), "cell field of the sort values");
 static_assert(kResWarps == 32, "the block scan is one warp over the warps' totals");
@@ -74,10 +77,14 @@ struct Work {
     __device__ __forceinline__ uint32_t* id(int k) const {
         return reinterpret_cast<uint32_t*>(base + (48ull + 12ull * k) * nb);
     }
+    // the bin cell of every slot after the last integrate
+    __device__ __forceinline__ uint32_t* key() const {
+        return reinterpret_cast<uint32_t*>(base + 64ull * nb);
+    }
 };
 
 __host__ __device__ inline size_t work_bytes_per_block(uint32_t maxN) {
-    return (size_t)64 * round64(maxN);
+    return (size_t)68 * round64(maxN);
 }
 
 // Shared memory of a block: positions, velocities, spins, radii (nb each),
@@ -87,7 +94,7 @@ __host__ __device__ inline size_t work_bytes_per_block(uint32_t maxN) {
 __host__ __device__ inline size_t smem_bytes(uint32_t maxN, uint32_t maxC) {
     const size_t nb = round64(maxN);
     return 24 * nb + 4 * (size_t)round64(maxC + 1) + sizeof(ResEntry) * kResMaxEntries +
-           4 * (2 * kResWarps + 4);
+           4 * (2 * kResWarps + 4) + sizeof(uint4) * kResMaxMovers;
 }
 
 extern __shared__ __align__(16) unsigned char smraw[];
@@ -113,6 +120,12 @@ struct Smem {
     __device__ __forceinline__ uint32_t* scan() const {
         return reinterpret_cast<uint32_t*>(smraw + 24u * nb + 4u * nc +
                                            (uint32_t)sizeof(ResEntry) * kResMaxEntries);
+    }
+    // (slot, cell before, cell after) of the particles that changed cell
+    __device__ __forceinline__ uint4* movers() const {
+        return reinterpret_cast<uint4*>(smraw + 24u * nb + 4u * nc +
+                                        (uint32_t)sizeof(ResEntry) * kResMaxEntries +
+                                        4u * (2u * kResWarps + 4u));
     }
     __device__ __forceinline__ uint32_t* sortA() const { return reinterpret_cast<uint32_t*>(smraw); }
     __device__ __forceinline__ uint32_t* sortB() const {
@@ -280,6 +293,7 @@ resident_kernel(const KParams* __restrict__ table, const ResBin* __restrict__ bi
                 uint32_t* __restrict__ queue, uint32_t maxN, uint32_t maxC, char* workBase,
                 ResIO io, uint32_t nTotal, uint32_t nsteps, uint32_t* __restrict__ errFlag) {
     __shared__ uint32_t sBin;
+    __shared__ uint32_t sMovers;  // particles that changed cell in the last step
     const Smem S{round64(maxN), round64(maxC + 1)};
     const Work W{workBase + work_bytes_per_block(maxN) * blockIdx.x, round64(maxN)};
     const uint32_t tid = threadIdx.x;
@@ -323,10 +337,88 @@ resident_kernel(const KParams* __restrict__ table, const ResBin* __restrict__ bi
                 entPack[k >> 2] |= entry_of(S.ent(), ne, i) << ((k & 3) * 8);
         }
         int buf = 0;
-        bool needSort = true;
+        bool needSort = true, fullSort = true;  // a bin's first sort is a full sort
+        if (tid == 0) sMovers = 0u;
 #pragma unroll 1
         for (uint32_t step = 0; step < nsteps; ++step) {
-            if (needSort) {
+            if (needSort && !fullSort && sMovers <= kResMaxMovers) {
+                // ---- incremental sort: the few particles that changed cell
+                // move to their places in the stable order by cell, the others
+                // keep their order (the same permutation as the full sort)
+                const uint32_t nm = sMovers;
+                const uint4* __restrict__ mv = S.movers();
+                uint32_t* __restrict__ first = S.first();
+                uint32_t moved = 0u;  // bit k: owned slot k changes
+#pragma unroll 1
+                for (int k = 0; k < kResPer; ++k) {
+                    const uint32_t i = tid + (uint32_t)k * kResThreads;
+                    if ((uint32_t)k >= per || i >= n) break;
+                    const uint32_t key = W.key()[i];  // the cell after the last integrate
+                    // movers before slot i; movers before (key, i) in the
+                    // new order; whether slot i is one
+                    uint32_t rb = 0u, ib = 0u;
+                    bool isMover = false;
+#pragma unroll 1
+                    for (uint32_t m = 0; m < nm; ++m) {
+                        const uint4 e = mv[m];
+                        rb += e.x < i ? 1u : 0u;
+                        ib += (e.z < key || (e.z == key && e.x < i)) ? 1u : 0u;
+                        isMover |= e.x == i;
+                    }
+                    uint32_t dst;
+                    if (!isMover) {
+                        // a stayer: the stayers before it, the movers placed before it
+                        dst = i - rb + ib;
+                    } else {
+                        // a mover: the stayers of lower cells and of its new cell
+                        // before it in the old order, then the movers placed before it
+                        const uint32_t q = min(max(i, first[key]), first[key + 1u]);
+                        uint32_t rq = 0u;
+#pragma unroll 1
+                        for (uint32_t m = 0; m < nm; ++m) rq += mv[m].x < q ? 1u : 0u;
+                        dst = q - rq + ib;
+                    }
+                    if (dst != i) {
+                        moved |= 1u << k;
+                        W.stashPos()[dst] = S.pos()[i];
+                        W.stashVel()[dst] = S.vel()[i];
+                        W.stashOm()[dst] = S.omega()[i];
+                        W.stashRad()[dst] = S.radius()[i];
+                        W.F()[dst] = make_float2(W.theta(buf)[i], W.mass(buf)[i]);
+                        reinterpret_cast<uint32_t*>(W.M())[dst] = W.id(buf)[i];
+                    }
+                }
+                __syncthreads();  // every destination stashed; the old first array read
+                // the slots that change take what was stashed for them (a
+                // permutation: the slots that receive are the slots that give)
+#pragma unroll 1
+                for (int k = 0; k < kResPer; ++k) {
+                    if (!((moved >> k) & 1u)) continue;
+                    const uint32_t i = tid + (uint32_t)k * kResThreads;
+                    S.pos()[i] = W.stashPos()[i];
+                    S.vel()[i] = W.stashVel()[i];
+                    S.omega()[i] = W.stashOm()[i];
+                    S.radius()[i] = W.stashRad()[i];
+                    const float2 tm = W.F()[i];
+                    W.theta(buf)[i] = tm.x;
+                    W.mass(buf)[i] = tm.y;
+                    W.id(buf)[i] = reinterpret_cast<const uint32_t*>(W.M())[i];
+                }
+                // first slot of every cell: one more for every mover that now
+                // comes before the cell, one fewer for every mover that did
+#pragma unroll 1
+                for (uint32_t c = tid; c <= bin.cells; c += kResThreads) {
+                    int d = 0;
+#pragma unroll 1
+                    for (uint32_t m = 0; m < nm; ++m) {
+                        const uint4 e = mv[m];
+                        d += (e.z < c ? 1 : 0) - (e.y < c ? 1 : 0);
+                    }
+                    first[c] = (uint32_t)((int)first[c] + d);
+                }
+                __syncthreads();
+                if (tid == 0) sMovers = 0u;
+            } else if (needSort) {
                 // ---- sort.  The state is stashed first, so that the value
                 // arrays may overwrite the positions; the values (cell << 13 |
                 // slot) are then made from the stashed positions.
@@ -395,6 +487,8 @@ resident_kernel(const KParams* __restrict__ table, const ResBin* __restrict__ bi
                 }
                 buf ^= 1;
                 __syncthreads();
+                if (tid == 0) sMovers = 0u;
+                fullSort = false;
             }
             // ---- collide: forces from the neighbours' current state
 #pragma unroll 1
@@ -454,7 +548,15 @@ resident_kernel(const KParams* __restrict__ table, const ResBin* __restrict__ bi
                 S.omega()[i] = s.w;
                 W.theta(buf)[i] = s.th;
                 if (!(isfinite(s.p.x) && isfinite(s.p.y))) atomicOr(errFlag, 1u);
-                if (local_cell(P, s.p) != cellBefore) mover = true;
+                const uint32_t cellAfter = local_cell(P, s.p);
+                W.key()[i] = E.cellOff + cellAfter;
+                if (cellAfter != cellBefore) {
+                    mover = true;
+                    const uint32_t slot = atomicAdd(&sMovers, 1u);
+                    if (slot < kResMaxMovers)
+                        S.movers()[slot] = make_uint4(i, E.cellOff + cellBefore,
+                                                      E.cellOff + cellAfter, 0u);
+                }
                 if (last) {
                     const uint32_t g = E.gslot + (i - E.slot);
                     if (io.pressure) io.pressure[g] = pr;

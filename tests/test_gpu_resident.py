@@ -82,6 +82,16 @@ def test_resident_hot_specimens_sort_every_step():
     assert_same_state(run(specimens, [80], True), run(specimens, [80], False))
 
 
+def test_resident_few_movers_per_step():
+    """Gases at a few m/s: a handful of particles change cell on most steps,
+    so most steps re-sort incrementally (at most 32 movers in a bin) and the
+    busier ones sort in full."""
+    specimens = [scenes.agitated_gas(n=n, seed=90 + k, vel_std=v, omega_std=50.0)
+                 for k, (n, v) in enumerate(((2000, 2.0), (3500, 1.0), (1200, 3.0), (800, 0.5),
+                                             (5000, 0.3)))]
+    assert_same_state(run(specimens, [150], True), run(specimens, [150], False))
+
+
 def test_resident_from_unsorted_state_and_across_calls():
     specimens = scenes.specimen_batch(num=40, seed=11, nmin=64, nmax=3000)
     ref = run(specimens, [47], False, shuffle_seed=2)
