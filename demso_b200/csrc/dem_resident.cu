@@ -32,17 +32,23 @@
 namespace dem {
 namespace {
 
-constexpr int kResThreads = 1024;
+#ifndef DEM_RES_THREADS
+#define DEM_RES_THREADS 1024
+#endif
+constexpr int kResThreads = DEM_RES_THREADS;  // one block per multiprocessor
 constexpr int kResWarps = kResThreads / 32;
 constexpr uint32_t kSlotBits = 13;  // bin slots < kResMaxParticles = 2^13
 constexpr uint32_t kSlotMask = (1u << kSlotBits) - 1u;
-constexpr int kResPer = (int)(kResMaxParticles / kResThreads);  // slots per thread
+constexpr int kResPer = (int)((kResMaxParticles + kResThreads - 1) / kResThreads);  // slots per thread
+constexpr int kEntWords = (kResPer + 3) / 4;  // a thread's slots' entries, 8 bits each
 // Steps on which at most this many particles of a bin changed cell re-sort
 // the bin incrementally; more take the full block sort.
 constexpr uint32_t kResMaxMovers = 32;
 static_assert(kResMaxParticles == (1u << kSlotBits), "slot field of the sort values");
 static_assert(kResMaxCells <= (1u << kSlotBits), "cell field of the sort values");
-static_assert(kResWarps == 32, "the block scan is one warp over the warps' totals");
+static_assert(kResWarps <= 32 && kResThreads % 32 == 0,
+              "the block scan is one warp over the warps' totals");
+static_assert(kResPer <= 32, "a thread's moved slots are one 32-bit mask");
 
 inline __host__ __device__ uint32_t round64(uint32_t n) { return (n + 63u) & ~63u; }
 
@@ -184,13 +190,13 @@ __device__ uint32_t* block_sort(uint32_t* a, uint32_t* b, uint32_t n, uint32_t d
         if (lane == 0) scan[warp] = zeros;
         __syncthreads();
         if (warp == 0) {
-            uint32_t x = scan[lane];
+            uint32_t x = lane < kResWarps ? scan[lane] : 0u;
 #pragma unroll
             for (int d = 1; d < 32; d <<= 1) {
                 const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
                 if (lane >= d) x += y;
             }
-            scan[kResWarps + lane] = x;  // inclusive
+            if (lane < kResWarps) scan[kResWarps + lane] = x;  // inclusive
         }
         __syncthreads();
         const uint32_t total0 = scan[2 * kResWarps - 1];
@@ -233,19 +239,21 @@ __device__ __forceinline__ uint32_t lower_cell(const uint32_t* v, uint32_t n, ui
     return lo;
 }
 
-// Forces on particle i from its 3 x 3 cells, in the reference's order; the
-// neighbours' fields from shared memory.  With culling (the specimen's
+// Forces on particle i, in cell `local` of its specimen's grid, from its
+// 3 x 3 cells, in the reference's order; the neighbours' fields from shared
+// memory.  With culling (the specimen's
 // cells wider than 2 rmax and the particle inside the box by the margin) a
 // column or row of cells farther than r + rmax is skipped: it holds no
 // contact, and its subtotal would be +0.
-__device__ __forceinline__ void res_collide(const KParams& P, uint32_t cellOff, uint32_t i,
-                                            float2 p, float2 v, float w, float r, const Smem& S,
-                                            float2& force, float& moment, float& pr) {
+__device__ __forceinline__ void res_collide(const KParams& P, uint32_t cellOff, uint32_t local,
+                                            uint32_t i, float2 p, float2 v, float w, float r,
+                                            const Smem& S, float2& force, float& moment,
+                                            float& pr) {
     force = make_float2(0.0f, 0.0f);
     moment = 0.0f;
     pr = 0.0f;
-    const int2 gr = grid_pos_fast(P, p);
-    const int gx = gr.x & (int)(P.gx - 1u), gy = gr.y & (int)(P.gy - 1u);
+    // the particle's (wrapped) cell, from its cell index in the specimen's grid
+    const int gx = (int)(local & (P.gx - 1u)), gy = (int)(local >> P.log2gx);
     int y0 = -1, y1 = 1, x0 = -1, x1 = 1;
     if (P.cull && p.x > P.cullMargin && p.x < P.Lx - P.cullMargin && p.y > P.cullMargin &&
         p.y < P.Ly - P.cullMargin) {
@@ -286,6 +294,7 @@ __device__ __forceinline__ void res_collide(const KParams& P, uint32_t cellOff, 
         }
     }
 }
+
 
 __global__ void __launch_bounds__(kResThreads, 1)
 resident_kernel(const KParams* __restrict__ table, const ResBin* __restrict__ bins,
@@ -328,7 +337,9 @@ resident_kernel(const KParams* __restrict__ table, const ResBin* __restrict__ bi
         // the entry of each slot this thread owns (slots tid + k * 1024),
         // 8 bits each
         const uint32_t per = (n + kResThreads - 1u) / kResThreads;
-        uint32_t entPack[2] = {0u, 0u};
+        uint32_t entPack[kEntWords];
+#pragma unroll
+        for (int w = 0; w < kEntWords; ++w) entPack[w] = 0u;
         __syncthreads();
 #pragma unroll
         for (int k = 0; k < kResPer; ++k) {
@@ -386,6 +397,7 @@ resident_kernel(const KParams* __restrict__ table, const ResBin* __restrict__ bi
                         W.stashRad()[dst] = S.radius()[i];
                         W.F()[dst] = make_float2(W.theta(buf)[i], W.mass(buf)[i]);
                         reinterpret_cast<uint32_t*>(W.M())[dst] = W.id(buf)[i];
+                        reinterpret_cast<uint32_t*>(W.Pr())[dst] = key;
                     }
                 }
                 __syncthreads();  // every destination stashed; the old first array read
@@ -403,6 +415,7 @@ resident_kernel(const KParams* __restrict__ table, const ResBin* __restrict__ bi
                     W.theta(buf)[i] = tm.x;
                     W.mass(buf)[i] = tm.y;
                     W.id(buf)[i] = reinterpret_cast<const uint32_t*>(W.M())[i];
+                    W.key()[i] = reinterpret_cast<const uint32_t*>(W.Pr())[i];
                 }
                 // first slot of every cell: one more for every mover that now
                 // comes before the cell, one fewer for every mover that did
@@ -470,6 +483,7 @@ resident_kernel(const KParams* __restrict__ table, const ResBin* __restrict__ bi
                     const uint32_t i = tid + (uint32_t)k * kResThreads;
                     if ((uint32_t)k >= per || i >= n) break;
                     from[i] = sorted[i] & kSlotMask;
+                    W.key()[i] = sorted[i] >> kSlotBits;
                 }
                 __syncthreads();  // the values are read; the state arrays are free
 #pragma unroll 1
@@ -499,8 +513,8 @@ resident_kernel(const KParams* __restrict__ table, const ResBin* __restrict__ bi
                 const KParams& P = table[E.spec];
                 float2 f;
                 float moment, pr;
-                res_collide(P, E.cellOff, i, S.pos()[i], S.vel()[i], S.omega()[i], S.radius()[i], S, f,
-                            moment, pr);
+                res_collide(P, E.cellOff, W.key()[i] - E.cellOff, i, S.pos()[i], S.vel()[i],
+                            S.omega()[i], S.radius()[i], S, f, moment, pr);
                 W.F()[i] = f;
                 W.M()[i] = moment;
                 W.Pr()[i] = pr;
@@ -526,7 +540,7 @@ resident_kernel(const KParams* __restrict__ table, const ResBin* __restrict__ bi
                 const float2 f = W.F()[i];
                 const float moment = W.M()[i];
                 float pr = W.Pr()[i];
-                const uint32_t cellBefore = local_cell(P, s.p);
+                const uint32_t keyBefore = W.key()[i];  // the cell this step sorted by
                 // F/m and M/I as the reference divides them; without contacts
                 // F and M are +0 and the quotients exactly +0 (the step
                 // kernel's shortcut, the same bits)
@@ -548,14 +562,13 @@ resident_kernel(const KParams* __restrict__ table, const ResBin* __restrict__ bi
                 S.omega()[i] = s.w;
                 W.theta(buf)[i] = s.th;
                 if (!(isfinite(s.p.x) && isfinite(s.p.y))) atomicOr(errFlag, 1u);
-                const uint32_t cellAfter = local_cell(P, s.p);
-                W.key()[i] = E.cellOff + cellAfter;
-                if (cellAfter != cellBefore) {
+                const uint32_t keyAfter = E.cellOff + local_cell(P, s.p);
+                W.key()[i] = keyAfter;
+                if (keyAfter != keyBefore) {
                     mover = true;
                     const uint32_t slot = atomicAdd(&sMovers, 1u);
                     if (slot < kResMaxMovers)
-                        S.movers()[slot] = make_uint4(i, E.cellOff + cellBefore,
-                                                      E.cellOff + cellAfter, 0u);
+                        S.movers()[slot] = make_uint4(i, keyBefore, keyAfter, 0u);
                 }
                 if (last) {
                     const uint32_t g = E.gslot + (i - E.slot);
