@@ -265,6 +265,10 @@ __device__ __forceinline__ void res_collide(const KParams& P, uint32_t cellOff, 
         if (Y0 + P.cellH - p.y > reach) y1 = 0;
     }
     const int mx = (int)(P.gx - 1u), my = (int)(P.gy - 1u);
+    // rmax bounds every radius of the batch (INFINITY when unknown): a superset
+    // of the exact test below, cd <= r + rmax in float as in reals
+    const float rr = r + P.rmax;
+    const float reach2 = rr * rr * 1.000002f;
 #pragma unroll 1
     for (int dy = y0; dy <= y1; ++dy) {
         const uint32_t row = cellOff + (uint32_t)((gy + dy) & my) * P.gx;
@@ -275,14 +279,16 @@ __device__ __forceinline__ void res_collide(const KParams& P, uint32_t cellOff, 
             float2 fc = make_float2(0.0f, 0.0f);
 #pragma unroll 1
             for (uint32_t j = a; j < b; ++j) {
-                if (j == i) continue;
                 const float2 pj = S.pos()[j];
                 const float ax = pj.x - p.x, ay = pj.y - p.y;
                 const float d2 = ax * ax + ay * ay;
+                // beyond (r + rmax)^2 (1 + 2e-6) no radius can reach: the
+                // radius is read for the near candidates only
+                if (d2 > reach2) continue;
                 const float rj = S.radius()[j];
                 const float cd = r + rj;
                 // d2 > cd^2 (1 + 2e-6) implies sqrtf(d2) >= cd: no contact
-                if (d2 <= cd * cd * 1.000002f && sqrtf(d2) < cd) {
+                if (j != i && d2 <= cd * cd * 1.000002f && sqrtf(d2) < cd) {
                     const float2 f = pair_force(p, pj, v, S.vel()[j], w, S.omega()[j], r, rj,
                                                 P.pair[0], P.dt, moment, pr);
                     fc.x += f.x;
