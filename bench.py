@@ -703,6 +703,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batched-specimens", type=int, default=4096,
+                    help="specimens of the batched leg (a smaller batch for profiling)")
+    ap.add_argument("--batched-steps", type=int, default=5000,
+                    help="steps of the batched leg's timed call")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-pile", action="store_true")
     ap.add_argument("--sweep", default=DEFAULT_SWEEP,
@@ -923,7 +927,8 @@ def main():
     batched = None
     if rank == 0 and world == 1 and not args.no_batched:
         try:
-            batched = measure_batched(5000, args.warmup)
+            batched = measure_batched(args.batched_steps, args.warmup,
+                                      num=args.batched_specimens)
         except Exception as e:  # reported beside the headline, never instead of it
             batched = {"error": str(e)}
 
