@@ -413,6 +413,11 @@ struct DemContext {
     ResEntry* dResEntries = nullptr;
     uint32_t* resQueue = nullptr;
     void* resWork = nullptr;
+    // DEM_CTX_RESIDENT (single scenes): the cluster launch's scratch, and
+    // whether a cluster of its shape could not be made resident here
+    void* clusterWork = nullptr;
+    size_t clusterWorkBytes = 0;
+    bool clusterUnsupported = false;
     void* adjRec = nullptr;
     size_t adjRecBytes = 0;
     void* adjTmp = nullptr;
@@ -1045,6 +1050,7 @@ extern "C" int dem_destroy(DemContext* c) {
     dev_free(c->dResEntries);
     dev_free(c->resQueue);
     dev_free(c->resWork);
+    dev_free(c->clusterWork);
     dev_free(c->renderOwner);
     dev_free(c->ctlBlock);
     dev_free(c->dTable);
@@ -1427,14 +1433,49 @@ int resident_step(DemContext* c, uint32_t nsteps, cudaStream_t st) {
     return DEM_OK;
 }
 
+// A multi-step call of a single scene created with DEM_CTX_RESIDENT as one
+// cluster launch (dem_resident.cu): every block of the cluster holds the
+// whole scene in shared memory and steps its share of the slots.  Returns
+// kNotResident, having done nothing, for scenes it does not take (more than
+// 8,192 disks or cells, types, attraction, a control particle, profiling) or
+// when no such cluster can be resident on this GPU; the graph path steps
+// those.  The next graph-path step sorts from scratch.
+int cluster_step(DemContext* c, uint32_t nsteps, cudaStream_t st) {
+    if (c->typed || c->ctlOn || c->profiling || c->clusterUnsupported || !has_state_sets(c) ||
+        has_attraction_host(c->P) || !cluster_scene_fits(c->n, c->numCells))
+        return kNotResident;
+    const size_t bytes = cluster_scene_work_bytes(c->n);
+    if (c->clusterWorkBytes < bytes) {
+        dev_free(c->clusterWork);
+        c->clusterWork = nullptr;
+        c->clusterWorkBytes = 0;
+        DEM_TRY_CUDA(dev_alloc(&c->clusterWork, bytes), "cudaMalloc cluster scratch");
+        c->clusterWorkBytes = bytes;
+    }
+    const int a = c->cur;
+    ResIO io{c->dyn[0].pos, c->dyn[a].vel, c->dyn[a].theta, c->dyn[a].omega, c->stat[a].radius,
+             c->stat[a].mass, c->stat[a].id, c->loc, c->pressure, c->acc, c->alpha};
+    const cudaError_t e = launch_cluster_scene(c->P, c->n, c->numCells, c->clusterWork, io,
+                                               nsteps, c->errFlag, st);
+    if (e == cudaErrorNotSupported) {
+        c->clusterUnsupported = true;
+        return kNotResident;
+    }
+    DEM_TRY_CUDA(e, "cluster step");
+    c->keysValid = false;
+    c->haveOrder = false;
+    c->inSortOrder = false;
+    return DEM_OK;
+}
+
 }  // namespace
 
 extern "C" int dem_step(DemContext* c, uint32_t nsteps, void* stream) {
     if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
     if (nsteps == 0 || c->n == 0) return DEM_OK;
     cudaStream_t st = (cudaStream_t)stream;
-    if (c->nspec && (c->flags & DEM_CTX_RESIDENT)) {
-        int rc = resident_step(c, nsteps, st);
+    if (c->flags & DEM_CTX_RESIDENT) {
+        int rc = c->nspec ? resident_step(c, nsteps, st) : cluster_step(c, nsteps, st);
         if (rc != kNotResident) return rc;
     }
     if (!c->keysValid) {

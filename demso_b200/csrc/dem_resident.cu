@@ -27,7 +27,11 @@
 // scratch, which stays in L2.
 #include <algorithm>
 
+#include <cooperative_groups.h>
+
 #include "dem_resident.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace dem {
 namespace {
@@ -163,20 +167,23 @@ __device__ __forceinline__ uint32_t entry_of(const ResEntry* ent, uint32_t count
 // (`differ`).  Lane l of warp w holds elements w * 32 * per + k * 32 + l, so
 // each warp's elements are one contiguous run and its ballots give the
 // ranks.  Returns the array holding the sorted values (a or b).
+template <int THREADS>
 __device__ uint32_t* block_sort(uint32_t* a, uint32_t* b, uint32_t n, uint32_t differ,
                                 uint32_t* scan) {
+    constexpr int kWarps = THREADS / 32;
+    constexpr int kPer = (int)((kResMaxParticles + THREADS - 1) / THREADS);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t per = (n + kResThreads - 1u) / kResThreads;
+    const uint32_t per = (n + THREADS - 1u) / THREADS;
     const uint32_t wbase = (uint32_t)warp * 32u * per;
     const unsigned lt = (1u << lane) - 1u;
 #pragma unroll 1
     for (uint32_t bit = kSlotBits; bit < 2 * kSlotBits; ++bit) {
         if (!((differ >> bit) & 1u)) continue;  // every value agrees here: the pass is the identity
-        uint32_t v[kResPer];
-        unsigned zm[kResPer];
+        uint32_t v[kPer];
+        unsigned zm[kPer];
         uint32_t zeros = 0;
 #pragma unroll
-        for (int k = 0; k < kResPer; ++k) {
+        for (int k = 0; k < kPer; ++k) {
             v[k] = 0u;
             zm[k] = 0u;
             if ((uint32_t)k < per) {
@@ -190,21 +197,21 @@ __device__ uint32_t* block_sort(uint32_t* a, uint32_t* b, uint32_t n, uint32_t d
         if (lane == 0) scan[warp] = zeros;
         __syncthreads();
         if (warp == 0) {
-            uint32_t x = lane < kResWarps ? scan[lane] : 0u;
+            uint32_t x = lane < kWarps ? scan[lane] : 0u;
 #pragma unroll
             for (int d = 1; d < 32; d <<= 1) {
                 const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
                 if (lane >= d) x += y;
             }
-            if (lane < kResWarps) scan[kResWarps + lane] = x;  // inclusive
+            if (lane < kWarps) scan[kWarps + lane] = x;  // inclusive
         }
         __syncthreads();
-        const uint32_t total0 = scan[2 * kResWarps - 1];
-        const uint32_t zBefore = warp ? scan[kResWarps + warp - 1] : 0u;
+        const uint32_t total0 = scan[2 * kWarps - 1];
+        const uint32_t zBefore = warp ? scan[kWarps + warp - 1] : 0u;
         const uint32_t oBefore = min(n, wbase) - zBefore;
         uint32_t zr = 0, orr = 0;
 #pragma unroll
-        for (int k = 0; k < kResPer; ++k) {
+        for (int k = 0; k < kPer; ++k) {
             if ((uint32_t)k < per) {
                 const uint32_t e = wbase + (uint32_t)k * 32u + (uint32_t)lane;
                 const bool ok = e < n;
@@ -226,6 +233,78 @@ __device__ uint32_t* block_sort(uint32_t* a, uint32_t* b, uint32_t n, uint32_t d
         __syncthreads();  // the pass is complete before the next one reads it
     }
     return a;
+}
+
+
+// The movers of the last step, (slot, cell before, cell after) -- at most
+// kResMaxMovers of them -- ranked by one warp (warp 0 calls this) into four
+// sorted arrays of ms (kResMaxMovers words each): their slots; their cells
+// after with their slots, in (cell, slot) order; their cells before.  `src`
+// may be ms itself (the entries are read into registers first); from
+// global memory (fromGlobal) it is read through L2.
+__device__ void rank_movers(const uint4* src, bool fromGlobal, uint32_t nm, uint32_t* ms) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const bool ok = lane < nm;
+    uint4 e = make_uint4(0u, 0u, 0u, 0u);
+    if (ok) e = fromGlobal ? __ldcg(src + lane) : src[lane];
+    __syncwarp();
+    uint32_t rs = 0u, rn = 0u, ro = 0u;
+#pragma unroll 4
+    for (uint32_t q = 0; q < nm; ++q) {
+        const uint32_t x = __shfl_sync(0xffffffffu, e.x, (int)q);
+        const uint32_t y = __shfl_sync(0xffffffffu, e.y, (int)q);
+        const uint32_t z = __shfl_sync(0xffffffffu, e.z, (int)q);
+        rs += x < e.x ? 1u : 0u;
+        rn += (z < e.z || (z == e.z && x < e.x)) ? 1u : 0u;
+        ro += (y < e.y || (y == e.y && x < e.x)) ? 1u : 0u;
+    }
+    if (ok) {
+        ms[rs] = e.x;
+        ms[kResMaxMovers + rn] = e.z;
+        ms[2 * kResMaxMovers + rn] = e.x;
+        ms[3 * kResMaxMovers + ro] = e.y;
+    }
+}
+
+// Entries of the sorted a[0, n) below v.
+__device__ __forceinline__ uint32_t count_below(const uint32_t* a, uint32_t n, uint32_t v) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (a[mid] < v) lo = mid + 1u;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// A slot's place in the new stable order by cell, from the ranked movers
+// (rank_movers) and the old first-particle array: a stayer moves down by
+// the movers before it and up by the movers placed before it; a mover goes
+// after the stayers of lower cells and of its new cell that came before it
+// in the old order, then after the movers placed before it.
+__device__ __forceinline__ uint32_t incremental_dest(const uint32_t* ms, uint32_t nm,
+                                                     const uint32_t* first, uint32_t i,
+                                                     uint32_t key) {
+    const uint32_t* slots = ms;
+    const uint32_t* newCell = ms + kResMaxMovers;
+    const uint32_t* newSlot = ms + 2 * kResMaxMovers;
+    const uint32_t rb = count_below(slots, nm, i);
+    const bool isMover = rb < nm && slots[rb] == i;
+    uint32_t lo = 0, hi = nm;  // movers placed before (key, i)
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (newCell[mid] < key || (newCell[mid] == key && newSlot[mid] < i)) lo = mid + 1u;
+        else hi = mid;
+    }
+    if (!isMover) return i - rb + lo;
+    const uint32_t q = min(max(i, first[key]), first[key + 1u]);
+    return q - count_below(slots, nm, q) + lo;
+}
+
+// Change of cell c's first slot: the movers now below c less those that were.
+__device__ __forceinline__ int first_shift(const uint32_t* ms, uint32_t nm, uint32_t c) {
+    return (int)count_below(ms + kResMaxMovers, nm, c) -
+           (int)count_below(ms + 3 * kResMaxMovers, nm, c);
 }
 
 // First index of the sorted values whose cell is >= c.
@@ -363,38 +442,17 @@ resident_kernel(const KParams* __restrict__ table, const ResBin* __restrict__ bi
                 // move to their places in the stable order by cell, the others
                 // keep their order (the same permutation as the full sort)
                 const uint32_t nm = sMovers;
-                const uint4* __restrict__ mv = S.movers();
                 uint32_t* __restrict__ first = S.first();
+                uint32_t* ms = reinterpret_cast<uint32_t*>(S.movers());
+                if (tid < 32) rank_movers(S.movers(), false, nm, ms);
+                __syncthreads();
                 uint32_t moved = 0u;  // bit k: owned slot k changes
 #pragma unroll 1
                 for (int k = 0; k < kResPer; ++k) {
                     const uint32_t i = tid + (uint32_t)k * kResThreads;
                     if ((uint32_t)k >= per || i >= n) break;
                     const uint32_t key = W.key()[i];  // the cell after the last integrate
-                    // movers before slot i; movers before (key, i) in the
-                    // new order; whether slot i is one
-                    uint32_t rb = 0u, ib = 0u;
-                    bool isMover = false;
-#pragma unroll 1
-                    for (uint32_t m = 0; m < nm; ++m) {
-                        const uint4 e = mv[m];
-                        rb += e.x < i ? 1u : 0u;
-                        ib += (e.z < key || (e.z == key && e.x < i)) ? 1u : 0u;
-                        isMover |= e.x == i;
-                    }
-                    uint32_t dst;
-                    if (!isMover) {
-                        // a stayer: the stayers before it, the movers placed before it
-                        dst = i - rb + ib;
-                    } else {
-                        // a mover: the stayers of lower cells and of its new cell
-                        // before it in the old order, then the movers placed before it
-                        const uint32_t q = min(max(i, first[key]), first[key + 1u]);
-                        uint32_t rq = 0u;
-#pragma unroll 1
-                        for (uint32_t m = 0; m < nm; ++m) rq += mv[m].x < q ? 1u : 0u;
-                        dst = q - rq + ib;
-                    }
+                    const uint32_t dst = incremental_dest(ms, nm, first, i, key);
                     if (dst != i) {
                         moved |= 1u << k;
                         W.stashPos()[dst] = S.pos()[i];
@@ -426,15 +484,8 @@ resident_kernel(const KParams* __restrict__ table, const ResBin* __restrict__ bi
                 // first slot of every cell: one more for every mover that now
                 // comes before the cell, one fewer for every mover that did
 #pragma unroll 1
-                for (uint32_t c = tid; c <= bin.cells; c += kResThreads) {
-                    int d = 0;
-#pragma unroll 1
-                    for (uint32_t m = 0; m < nm; ++m) {
-                        const uint4 e = mv[m];
-                        d += (e.z < c ? 1 : 0) - (e.y < c ? 1 : 0);
-                    }
-                    first[c] = (uint32_t)((int)first[c] + d);
-                }
+                for (uint32_t c = tid; c <= bin.cells; c += kResThreads)
+                    first[c] = (uint32_t)((int)first[c] + first_shift(ms, nm, c));
                 __syncthreads();
                 if (tid == 0) sMovers = 0u;
             } else if (needSort) {
@@ -477,7 +528,8 @@ resident_kernel(const KParams* __restrict__ table, const ResBin* __restrict__ bi
                 // the cell bits on which the values differ (the passes use
                 // other scan words)
                 const uint32_t differ = S.scan()[2 * kResWarps] & ~S.scan()[2 * kResWarps + 1];
-                const uint32_t* sorted = block_sort(S.sortA(), S.sortB(), n, differ, S.scan());
+                const uint32_t* sorted =
+                    block_sort<kResThreads>(S.sortA(), S.sortB(), n, differ, S.scan());
                 // first particle of every cell of the bin (bin.cells + 1
                 // entries); each new slot's old slot to the scratch
 #pragma unroll 1
@@ -606,6 +658,312 @@ resident_kernel(const KParams* __restrict__ table, const ResBin* __restrict__ bi
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// One scene across a thread-block cluster (DEM_CTX_RESIDENT on a single
+// scene of at most kResMaxParticles disks and kResMaxCells cells): the
+// cluster's kClusterCtas blocks, one per multiprocessor, each hold a full
+// copy of the scene's positions, velocities, spins and radii in shared
+// memory, and each steps its own share of the slots.  A step is
+//   sort      only after a step in which a disk changed cell: every block
+//             runs the same sort (incremental or full, as above) on its own
+//             copy, which gives the same permutation in every block; block 0
+//             also moves the angles, masses, ids and cells, which live in
+//             global memory;
+//   collide   the block's slots against its own copy;
+//   integrate the block's slots, held in registers;
+//   broadcast after a cluster barrier (every copy read), each block writes
+//             its slots' new positions, velocities and spins into every
+//             block's copy through distributed shared memory; a second
+//             cluster barrier makes them visible.
+// Every block takes the same cluster barriers in the same order whatever
+// its data: the sort decision reads a counter after a barrier, and no sort
+// path contains a cluster barrier.  Global memory another block wrote is
+// read through L2 (__ldcg).
+
+constexpr int kClusterCtas = 8;  // portable cluster size
+
+// Global scratch of one cluster: angles, masses, ids (two sets), the cell of
+// every slot, the incremental sort's stash of those four, two mover counters
+// and lists, and per block the full sort's stash and source slots.
+struct CWork {
+    char* base;
+    uint32_t nb;
+    __device__ __forceinline__ float* theta(int k) const {
+        return reinterpret_cast<float*>(base + (12ull * k) * nb);
+    }
+    __device__ __forceinline__ float* mass(int k) const {
+        return reinterpret_cast<float*>(base + (4ull + 12ull * k) * nb);
+    }
+    __device__ __forceinline__ uint32_t* id(int k) const {
+        return reinterpret_cast<uint32_t*>(base + (8ull + 12ull * k) * nb);
+    }
+    __device__ __forceinline__ uint32_t* key() const {
+        return reinterpret_cast<uint32_t*>(base + 24ull * nb);
+    }
+    __device__ __forceinline__ float2* stashTM() const {
+        return reinterpret_cast<float2*>(base + 28ull * nb);
+    }
+    __device__ __forceinline__ uint32_t* stashId() const {
+        return reinterpret_cast<uint32_t*>(base + 36ull * nb);
+    }
+    __device__ __forceinline__ uint32_t* stashKey() const {
+        return reinterpret_cast<uint32_t*>(base + 40ull * nb);
+    }
+    __device__ __forceinline__ char* block(uint32_t r) const {
+        return base + (44ull + 28ull * r) * nb;
+    }
+    __device__ __forceinline__ float2* stashPos(uint32_t r) const {
+        return reinterpret_cast<float2*>(block(r));
+    }
+    __device__ __forceinline__ float2* stashVel(uint32_t r) const {
+        return reinterpret_cast<float2*>(block(r) + 8ull * nb);
+    }
+    __device__ __forceinline__ float* stashOm(uint32_t r) const {
+        return reinterpret_cast<float*>(block(r) + 16ull * nb);
+    }
+    __device__ __forceinline__ float* stashRad(uint32_t r) const {
+        return reinterpret_cast<float*>(block(r) + 20ull * nb);
+    }
+    __device__ __forceinline__ uint32_t* from(uint32_t r) const {
+        return reinterpret_cast<uint32_t*>(block(r) + 24ull * nb);
+    }
+    __device__ __forceinline__ uint32_t* counter() const {
+        return reinterpret_cast<uint32_t*>(base + (44ull + 28ull * kClusterCtas) * nb);
+    }
+    __device__ __forceinline__ uint4* movers(int k) const {
+        return reinterpret_cast<uint4*>(base + (44ull + 28ull * kClusterCtas) * nb + 256u) +
+               k * kResMaxMovers;
+    }
+};
+
+__host__ __device__ inline size_t cluster_work_bytes(uint32_t n) {
+    return (44ull + 28ull * kClusterCtas) * round64(n) + 256u + 2u * 16u * kResMaxMovers;
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, 1)
+cluster_kernel(const __grid_constant__ KParams P, ResIO io, uint32_t n, uint32_t cells,
+               char* workBase, uint32_t nsteps, uint32_t* __restrict__ errFlag) {
+    constexpr int kPer = (int)((kResMaxParticles + THREADS - 1) / THREADS);
+    static_assert(kPer <= 32, "a thread's moved slots are one 32-bit mask");
+    cg::cluster_group cl = cg::this_cluster();
+    const uint32_t rank = cl.block_rank();
+    const uint32_t tid = threadIdx.x;
+    const Smem S{round64(n), round64(cells + 1)};
+    const CWork W{workBase, round64(n)};
+    // this thread's slot
+    const uint32_t share = (n + kClusterCtas - 1u) / kClusterCtas;
+    const uint32_t own = rank * share + tid;
+    const bool mine = tid < share && own < n;
+    const uint32_t per = (n + THREADS - 1u) / THREADS;  // slots of the copy per thread
+#pragma unroll 1
+    for (uint32_t i = tid; i < n; i += THREADS) {
+        S.pos()[i] = io.pos[i];
+        S.vel()[i] = io.vel[i];
+        S.omega()[i] = io.omega[i];
+        S.radius()[i] = io.radius[i];
+        if (rank == 0) {
+            W.theta(0)[i] = io.theta[i];
+            W.mass(0)[i] = io.mass[i];
+            W.id(0)[i] = io.id[i];
+        }
+    }
+    if (rank == 0 && tid < 2) W.counter()[tid] = 0u;
+    int buf = 0;
+    bool needSort = true, fullSort = true;
+    cl.sync();
+#pragma unroll 1
+    for (uint32_t step = 0; step < nsteps; ++step) {
+        const int par = (int)(step & 1u);  // this step's movers: counter / list par
+        if (needSort) {
+            const uint32_t nm = fullSort ? 0xffffffffu : __ldcg(W.counter() + (par ^ 1));
+            const uint4* __restrict__ mv = W.movers(par ^ 1);
+            uint32_t* __restrict__ first = S.first();
+            if (nm <= kResMaxMovers) {
+                // ---- incremental sort of this block's copy (as in
+                // resident_kernel, over every slot of the copy)
+                uint32_t* ms = reinterpret_cast<uint32_t*>(S.movers());
+                if (tid < 32) rank_movers(mv, true, nm, ms);
+                __syncthreads();
+                uint32_t moved = 0u;
+#pragma unroll 1
+                for (int k = 0; k < kPer; ++k) {
+                    const uint32_t i = tid + (uint32_t)k * THREADS;
+                    if ((uint32_t)k >= per || i >= n) break;
+                    // the slot's cell from the copy's position (the cell array
+                    // in global memory is rewritten by block 0 meanwhile)
+                    const uint32_t key = local_cell(P, S.pos()[i]);
+                    const uint32_t dst = incremental_dest(ms, nm, first, i, key);
+                    if (dst != i) {
+                        moved |= 1u << k;
+                        W.stashPos(rank)[dst] = S.pos()[i];
+                        W.stashVel(rank)[dst] = S.vel()[i];
+                        W.stashOm(rank)[dst] = S.omega()[i];
+                        W.stashRad(rank)[dst] = S.radius()[i];
+                        if (rank == 0) {
+                            W.stashTM()[dst] = make_float2(__ldcg(W.theta(buf) + i),
+                                                           __ldcg(W.mass(buf) + i));
+                            W.stashId()[dst] = __ldcg(W.id(buf) + i);
+                            W.stashKey()[dst] = key;
+                        }
+                    }
+                }
+                __syncthreads();
+#pragma unroll 1
+                for (int k = 0; k < kPer; ++k) {
+                    if (!((moved >> k) & 1u)) continue;
+                    const uint32_t i = tid + (uint32_t)k * THREADS;
+                    S.pos()[i] = W.stashPos(rank)[i];
+                    S.vel()[i] = W.stashVel(rank)[i];
+                    S.omega()[i] = W.stashOm(rank)[i];
+                    S.radius()[i] = W.stashRad(rank)[i];
+                    if (rank == 0) {
+                        const float2 tm = W.stashTM()[i];
+                        W.theta(buf)[i] = tm.x;
+                        W.mass(buf)[i] = tm.y;
+                        W.id(buf)[i] = W.stashId()[i];
+                        W.key()[i] = W.stashKey()[i];
+                    }
+                }
+#pragma unroll 1
+                for (uint32_t c = tid; c <= cells; c += THREADS)
+                    first[c] = (uint32_t)((int)first[c] + first_shift(ms, nm, c));
+                __syncthreads();
+            } else {
+                // ---- full sort of this block's copy
+#pragma unroll 1
+                for (uint32_t i = tid; i < n; i += THREADS) {
+                    W.stashPos(rank)[i] = S.pos()[i];
+                    W.stashVel(rank)[i] = S.vel()[i];
+                    W.stashOm(rank)[i] = S.omega()[i];
+                    W.stashRad(rank)[i] = S.radius()[i];
+                }
+                if (tid == 0) {
+                    S.scan()[2 * (THREADS / 32)] = 0u;
+                    S.scan()[2 * (THREADS / 32) + 1] = 0xffffffffu;
+                }
+                __syncthreads();
+                uint32_t orv = 0u, andv = 0xffffffffu;
+#pragma unroll 1
+                for (uint32_t i = tid; i < n; i += THREADS) {
+                    const uint32_t v = (local_cell(P, W.stashPos(rank)[i]) << kSlotBits) | i;
+                    S.sortA()[i] = v;
+                    orv |= v;
+                    andv &= v;
+                }
+                orv = __reduce_or_sync(0xffffffffu, orv);
+                andv = __reduce_and_sync(0xffffffffu, andv);
+                if ((tid & 31) == 0) {
+                    atomicOr(&S.scan()[2 * (THREADS / 32)], orv);
+                    atomicAnd(&S.scan()[2 * (THREADS / 32) + 1], andv);
+                }
+                __syncthreads();
+                const uint32_t differ =
+                    S.scan()[2 * (THREADS / 32)] & ~S.scan()[2 * (THREADS / 32) + 1];
+                const uint32_t* sorted =
+                    block_sort<THREADS>(S.sortA(), S.sortB(), n, differ, S.scan());
+#pragma unroll 1
+                for (uint32_t c = tid; c <= cells; c += THREADS) first[c] = lower_cell(sorted, n, c);
+#pragma unroll 1
+                for (uint32_t i = tid; i < n; i += THREADS) {
+                    W.from(rank)[i] = sorted[i] & kSlotMask;
+                    if (rank == 0) W.key()[i] = sorted[i] >> kSlotBits;
+                }
+                __syncthreads();  // the values are read; the copy's arrays are free
+#pragma unroll 1
+                for (uint32_t i = tid; i < n; i += THREADS) {
+                    const uint32_t f = W.from(rank)[i];
+                    S.pos()[i] = W.stashPos(rank)[f];
+                    S.vel()[i] = W.stashVel(rank)[f];
+                    S.omega()[i] = W.stashOm(rank)[f];
+                    S.radius()[i] = W.stashRad(rank)[f];
+                    if (rank == 0) {
+                        W.theta(buf ^ 1)[i] = __ldcg(W.theta(buf) + f);
+                        W.mass(buf ^ 1)[i] = __ldcg(W.mass(buf) + f);
+                        W.id(buf ^ 1)[i] = __ldcg(W.id(buf) + f);
+                    }
+                }
+                buf ^= 1;
+                __syncthreads();
+            }
+            fullSort = false;
+        }
+        cl.sync();  // every copy sorted; block 0's angles, masses, ids and cells visible
+        // the previous step's mover count is consumed: it counts this step's
+        // successor's movers next
+        if (rank == 0 && tid == 0) W.counter()[par ^ 1] = 0u;
+        const bool last = step + 1u == nsteps;
+        Dyn s;
+        bool mover = false;
+        if (mine) {
+            const uint32_t keyBefore = __ldcg(W.key() + own);
+            float2 f;
+            float moment, pr;
+            s.p = S.pos()[own];
+            s.v = S.vel()[own];
+            s.w = S.omega()[own];
+            const float r = S.radius()[own];
+            res_collide(P, 0u, keyBefore, own, s.p, s.v, s.w, r, S, f, moment, pr);
+            s.th = __ldcg(W.theta(buf) + own);
+            const float m = __ldcg(W.mass(buf) + own);
+            const bool quiet = f.x == 0.0f && f.y == 0.0f && moment == 0.0f && m > 0.0f &&
+                               m < INFINITY;
+            const float two_mrr = 2.0f * m * r * r;
+            float2 a;
+            float al;
+            if (quiet && two_mrr >= 1e-30f && two_mrr <= 1e30f) {
+                a = make_float2(0.0f, 0.0f);
+                al = 0.0f;
+            } else {
+                a = make_float2(f.x / m, f.y / m);
+                al = moment / inertia_of(m, r);
+            }
+            integrate_one(P, s, a, al, r, m, 0u, pr);
+            W.theta(buf)[own] = s.th;
+            if (!(isfinite(s.p.x) && isfinite(s.p.y))) atomicOr(errFlag, 1u);
+            const uint32_t keyAfter = local_cell(P, s.p);
+            W.key()[own] = keyAfter;
+            if (keyAfter != keyBefore) {
+                mover = true;
+                const uint32_t slot = atomicAdd(W.counter() + par, 1u);
+                if (slot < kResMaxMovers)
+                    W.movers(par)[slot] = make_uint4(own, keyBefore, keyAfter, 0u);
+            }
+            if (last) {
+                if (io.pressure) io.pressure[own] = pr;
+                if (io.acc) io.acc[own] = a;
+                if (io.alpha) io.alpha[own] = al;
+            }
+        }
+        (void)mover;
+        cl.sync();  // every block has read its copy: the copies may be overwritten
+        if (mine) {
+#pragma unroll 1
+            for (uint32_t r = 0; r < (uint32_t)kClusterCtas; ++r) {
+                cl.map_shared_rank(S.pos(), r)[own] = s.p;
+                cl.map_shared_rank(S.vel(), r)[own] = s.v;
+                cl.map_shared_rank(S.omega(), r)[own] = s.w;
+            }
+        }
+        cl.sync();  // every copy holds the new state; the mover count is final
+        needSort = __ldcg(W.counter() + par) != 0u;
+    }
+    // this block's slots back into the scene, in the order of the last sort
+    if (mine) {
+        io.pos[own] = S.pos()[own];
+        io.vel[own] = S.vel()[own];
+        io.omega[own] = S.omega()[own];
+        io.radius[own] = S.radius()[own];
+        io.theta[own] = __ldcg(W.theta(buf) + own);
+        io.mass[own] = __ldcg(W.mass(buf) + own);
+        const uint32_t id = __ldcg(W.id(buf) + own);
+        io.id[own] = id;
+        if (id < n) io.loc[id] = own;
+    }
+    cl.sync();  // no block leaves while another may still address its shared memory
+}
+
 }  // namespace
 
 bool resident_plan(const std::vector<uint32_t>& partOff, const std::vector<uint32_t>& cells,
@@ -685,6 +1043,46 @@ cudaError_t launch_resident(const KParams* table, const ResBin* bins, uint32_t n
                                                        maxC, static_cast<char*>(work), io, nTotal,
                                                        nsteps, errFlag);
     return cudaGetLastError();
+}
+
+
+size_t cluster_scene_work_bytes(uint32_t n) { return cluster_work_bytes(n); }
+
+bool cluster_scene_fits(uint32_t n, uint32_t cells) {
+    return n >= 1u && n <= kResMaxParticles && cells <= kResMaxCells;
+}
+
+cudaError_t launch_cluster_scene(const KParams& P, uint32_t n, uint32_t cells, void* work,
+                                 ResIO io, uint32_t nsteps, uint32_t* errFlag, cudaStream_t st) {
+    if (n == 0 || nsteps == 0) return cudaSuccess;
+    if (!cluster_scene_fits(n, cells)) return cudaErrorInvalidValue;
+    const size_t smem = smem_bytes(n, cells);
+    const uint32_t share = (n + kClusterCtas - 1u) / kClusterCtas;
+    auto launch = [&](auto kernel, int threads) -> cudaError_t {
+        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(kClusterCtas, 1, 1);
+        cfg.blockDim = dim3((unsigned)threads, 1, 1);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = kClusterCtas;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        e = cudaOccupancyMaxActiveClusters(&clusters, kernel, &cfg);
+        if (e != cudaSuccess) return e;
+        if (clusters < 1) return cudaErrorNotSupported;
+        return cudaLaunchKernelEx(&cfg, kernel, P, io, n, cells, static_cast<char*>(work),
+                                  nsteps, errFlag);
+    };
+    if (share <= 512u) return launch(cluster_kernel<512>, 512);
+    return launch(cluster_kernel<1024>, 1024);
 }
 
 }  // namespace dem

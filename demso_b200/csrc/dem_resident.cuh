@@ -70,4 +70,16 @@ cudaError_t launch_resident(const KParams* table, const ResBin* bins, uint32_t n
                             uint32_t* queue, void* work, int blocks, ResIO io, uint32_t nTotal,
                             uint32_t nsteps, uint32_t* errFlag, cudaStream_t st);
 
+
+// One scene stepped by a thread-block cluster (every block a full copy of
+// the scene in its shared memory, its own share of the slots stepped, the
+// new state broadcast through distributed shared memory).  Fits scenes of at
+// most kResMaxParticles disks and kResMaxCells cells; `work` is
+// cluster_scene_work_bytes(n) bytes of device memory.  Returns
+// cudaErrorNotSupported when no cluster of this shape can be resident.
+bool cluster_scene_fits(uint32_t n, uint32_t cells);
+size_t cluster_scene_work_bytes(uint32_t n);
+cudaError_t launch_cluster_scene(const KParams& P, uint32_t n, uint32_t cells, void* work,
+                                 ResIO io, uint32_t nsteps, uint32_t* errFlag, cudaStream_t st);
+
 }  // namespace dem

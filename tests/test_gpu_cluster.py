@@ -1,0 +1,84 @@
+"""Single scenes stepped by a thread-block cluster (DEM_CTX_RESIDENT on a
+context of at most 8,192 disks and cells): every block holds the whole scene
+in shared memory, steps its share of the slots and broadcasts the new state
+to the other blocks through distributed shared memory.  The state equals
+the graph path's bit for bit -- positions, velocities, angles, spins, the
+static fields in the same order, loc, and the last step's pressure, acc and
+alpha -- on piles, gases that re-sort on most steps or every step, tiny
+wrapping grids, both block sizes, unsorted starts, consecutive calls, and
+scenes it declines."""
+import numpy as np
+import pytest
+
+from demso_b200 import scenes
+from helpers import same
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ["pos", "vel", "theta", "omega", "radius", "mass", "id", "loc", "pressure", "acc",
+          "alpha"]
+
+
+def _torch(a):
+    import torch
+    a = np.ascontiguousarray(a)
+    return torch.from_numpy(a.view(np.int32) if a.dtype == np.uint32 else a.copy())
+
+
+def run(sc, calls, resident, shuffle_seed=None):
+    import torch
+    import demso_b200 as D
+    flags = D.CTX_PRESSURE | D.CTX_ACCEL | (D.CTX_RESIDENT if resident else 0)
+    sim = D.Simulation(sc.sys, capacity=sc.n, flags=flags)
+    st = sc.state()
+    if shuffle_seed is not None:
+        order = np.random.default_rng(shuffle_seed).permutation(sc.n)
+        st = {k: (None if v is None else np.asarray(v)[order]) for k, v in st.items()}
+    sim.set_state(_torch(st["pos"]), _torch(st["vel"]), _torch(st["theta"]), _torch(st["omega"]),
+                  _torch(st["radius"]), _torch(st["mass"]), _torch(st["id"]))
+    for k in calls:
+        sim.step(k)
+    torch.cuda.synchronize()
+    out = {k: (None if v is None else (v.numpy().view(np.uint32) if v.dtype == torch.int32
+                                       else v.numpy())) for k, v in sim.get_state("cpu").items()}
+    sim.check()
+    sim.close()
+    return out
+
+
+def assert_same(sc, calls, **kw):
+    a = run(sc, calls, True, **kw)
+    b = run(sc, calls, False, **kw)
+    for k in FIELDS:
+        assert same(a[k], b[k]), k
+
+
+def test_cluster_settling_pile():
+    """The 4,096-disk settling pile (64 x 64 cells), 400 steps."""
+    assert_same(scenes.settling_pile(), [400])
+
+
+@pytest.mark.parametrize("n,vel,steps", [(3000, 1.0, 120), (1500, 4.0, 60), (7000, 0.5, 60)])
+def test_cluster_gases(n, vel, steps):
+    """Gases whose disks change cell on most steps (incremental re-sorts) or
+    on every step in numbers (full sorts); 7,000 disks take the 1,024-thread
+    blocks."""
+    assert_same(scenes.agitated_gas(n=n, seed=7 + n, vel_std=vel, omega_std=100.0), [steps])
+
+
+def test_cluster_tiny_wrapping_grid():
+    """90 disks on a 2 x 2 grid: no culling, cells visited more than once."""
+    assert_same(scenes.agitated_gas(n=90, seed=55, grid=(2, 2)), [40])
+
+
+def test_cluster_unsorted_start_and_consecutive_calls():
+    sc = scenes.agitated_gas(n=2500, seed=31, vel_std=0.8)
+    ref = run(sc, [33], False, shuffle_seed=4)
+    out = run(sc, [1, 12, 20], True, shuffle_seed=4)
+    for k in FIELDS:
+        assert same(out[k], ref[k]), k
+
+
+def test_cluster_declines_a_larger_scene():
+    """More than 8,192 disks: the graph path steps the scene (same results)."""
+    assert_same(scenes.agitated_gas(n=9000, seed=81), [10])
