@@ -442,33 +442,46 @@ def measure_adjoint(n: int = 16384, steps: int = 2000, every: int = 100):
 # ------------------------------------------------------------------ config 0
 def measure_settling_pile(steps: int = 20000):
     """The plain 2D settling pile (4,096 disks, 20,000 steps): wall time of
-    the whole run on the GPU (settling_pile_cpu adds the host build's)."""
+    the whole run on the GPU as one dem_step call, for the context stepped
+    by a thread-block cluster (DEM_CTX_RESIDENT) and on the graph path; the
+    faster gives gpu_seconds (settling_pile_cpu adds the host build's)."""
     import torch
     import demso_b200 as D
     from demso_b200 import scenes
     sc = scenes.settling_pile()
-    sim = D.Simulation(sc.sys, capacity=sc.n, flags=D.CTX_PRESSURE)
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int32) if a.dtype == np.uint32
                                    else np.ascontiguousarray(a))
     st = sc.state()
-    sim.set_state(t(st["pos"]), t(st["vel"]), t(st["theta"]), t(st["omega"]), t(st["radius"]),
-                  t(st["mass"]), t(st["id"]))
-    sim.step(10)
-    sim.set_state(t(st["pos"]), t(st["vel"]), t(st["theta"]), t(st["omega"]), t(st["radius"]),
-                  t(st["mass"]), t(st["id"]))
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    sim.step(steps)
-    e1.record()
-    torch.cuda.synchronize()
-    sim.check()
-    gpu_s = e0.elapsed_time(e1) * 1e-3
-    sim.close()
+
+    def run(flags):
+        sim = D.Simulation(sc.sys, capacity=sc.n, flags=flags)
+        sim.set_state(t(st["pos"]), t(st["vel"]), t(st["theta"]), t(st["omega"]), t(st["radius"]),
+                      t(st["mass"]), t(st["id"]))
+        sim.step(10)
+        sim.set_state(t(st["pos"]), t(st["vel"]), t(st["theta"]), t(st["omega"]), t(st["radius"]),
+                      t(st["mass"]), t(st["id"]))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sim.step(steps)
+        e1.record()
+        torch.cuda.synchronize()
+        sim.check()
+        sim.close()
+        return e0.elapsed_time(e1) * 1e-3
+
+    cluster_s = run(D.CTX_PRESSURE | D.CTX_RESIDENT)
+    graph_s = run(D.CTX_PRESSURE)
+    gpu_s = min(cluster_s, graph_s)
     out = {"workload": "plain 2D settling pile: 4096 disks, radii U[0.9, 1.1] mm, 64x64 "
                        "jittered lattice in a 0.2 x 0.2 m box, dt 2e-6 s, %d steps" % steps,
            "gpu_seconds": gpu_s, "gpu_steps_per_s": steps / gpu_s,
-           "gpu_particle_steps_per_s": sc.n * steps / gpu_s}
+           "gpu_particle_steps_per_s": sc.n * steps / gpu_s,
+           "path": "cluster" if cluster_s <= graph_s else "graph",
+           "cluster_seconds": cluster_s, "graph_path_seconds": graph_s,
+           "cluster_form": "one launch of a cluster of 8 blocks, each holding the scene in "
+                           "shared memory and stepping an eighth of the disks",
+           "graph_path_form": "one graph launch of the device-side step loop"}
     return out
 
 

@@ -681,7 +681,7 @@ resident_kernel(const KParams* __restrict__ table, const ResBin* __restrict__ bi
 // path contains a cluster barrier.  Global memory another block wrote is
 // read through L2 (__ldcg).
 
-constexpr int kClusterCtas = 8;  // portable cluster size
+constexpr int kClusterCtas = 8;  // blocks of a cluster (the portable size; 16 measured slower)
 
 // Global scratch of one cluster: angles, masses, ids (two sets), the cell of
 // every slot, the incremental sort's stash of those four, two mover counters
@@ -753,7 +753,8 @@ cluster_kernel(const __grid_constant__ KParams P, ResIO io, uint32_t n, uint32_t
     const Smem S{round64(n), round64(cells + 1)};
     const CWork W{workBase, round64(n)};
     // this thread's slot
-    const uint32_t share = (n + kClusterCtas - 1u) / kClusterCtas;
+    const uint32_t ctas = cl.num_blocks();
+    const uint32_t share = (n + ctas - 1u) / ctas;
     const uint32_t own = rank * share + tid;
     const bool mine = tid < share && own < n;
     const uint32_t per = (n + THREADS - 1u) / THREADS;  // slots of the copy per thread
@@ -940,7 +941,7 @@ cluster_kernel(const __grid_constant__ KParams P, ResIO io, uint32_t n, uint32_t
         cl.sync();  // every block has read its copy: the copies may be overwritten
         if (mine) {
 #pragma unroll 1
-            for (uint32_t r = 0; r < (uint32_t)kClusterCtas; ++r) {
+            for (uint32_t r = 0; r < ctas; ++r) {
                 cl.map_shared_rank(S.pos(), r)[own] = s.p;
                 cl.map_shared_rank(S.vel(), r)[own] = s.v;
                 cl.map_shared_rank(S.omega(), r)[own] = s.w;
@@ -1057,32 +1058,36 @@ cudaError_t launch_cluster_scene(const KParams& P, uint32_t n, uint32_t cells, v
     if (n == 0 || nsteps == 0) return cudaSuccess;
     if (!cluster_scene_fits(n, cells)) return cudaErrorInvalidValue;
     const size_t smem = smem_bytes(n, cells);
-    const uint32_t share = (n + kClusterCtas - 1u) / kClusterCtas;
-    auto launch = [&](auto kernel, int threads) -> cudaError_t {
+    // a launch of `ctas` blocks of `threads`, or cudaErrorNotSupported when no
+    // such cluster can be resident
+    auto launch = [&](auto kernel, int threads, int ctas) -> cudaError_t {
         cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return e;
         cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(kClusterCtas, 1, 1);
+        cfg.gridDim = dim3((unsigned)ctas, 1, 1);
         cfg.blockDim = dim3((unsigned)threads, 1, 1);
         cfg.dynamicSmemBytes = smem;
         cfg.stream = st;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = kClusterCtas;
+        attr[0].val.clusterDim.x = (unsigned)ctas;
         attr[0].val.clusterDim.y = 1;
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         int clusters = 0;
         e = cudaOccupancyMaxActiveClusters(&clusters, kernel, &cfg);
-        if (e != cudaSuccess) return e;
-        if (clusters < 1) return cudaErrorNotSupported;
+        if (e != cudaSuccess || clusters < 1) {
+            (void)cudaGetLastError();  // the query's error is not the caller's
+            return cudaErrorNotSupported;
+        }
         return cudaLaunchKernelEx(&cfg, kernel, P, io, n, cells, static_cast<char*>(work),
                                   nsteps, errFlag);
     };
-    if (share <= 512u) return launch(cluster_kernel<512>, 512);
-    return launch(cluster_kernel<1024>, 1024);
+    const uint32_t share = (n + (uint32_t)kClusterCtas - 1u) / (uint32_t)kClusterCtas;
+    return share <= 512u ? launch(cluster_kernel<512>, 512, kClusterCtas)
+                         : launch(cluster_kernel<1024>, 1024, kClusterCtas);
 }
 
 }  // namespace dem

@@ -180,9 +180,11 @@ typedef struct DemContext DemContext;
                                  (dem_get_step_variant) */
 #define DEM_CTX_CALLER_STATE 16u /* allocate no particle state: the caller's buffers
                                     are handed over by dem_adopt_state */
-#define DEM_CTX_RESIDENT 32u  /* batches: run each dem_step call as one persistent
-                                 launch in which every specimen is stepped inside one
-                                 multiprocessor's shared memory (see dem_batch_create) */
+#define DEM_CTX_RESIDENT 32u  /* run each dem_step call as one launch that keeps the
+                                 particles in shared memory: batches as bins of
+                                 specimens, one per multiprocessor (see
+                                 dem_batch_create); single scenes of up to 8,192 disks
+                                 as one thread-block cluster (see dem_step) */
 
 int dem_create(const DemSystem* sys, uint32_t capacity, uint32_t flags, DemContext** out);
 int dem_destroy(DemContext* ctx);
@@ -302,7 +304,17 @@ int dem_state_view(DemContext* ctx, DemStateSet* out, int* setIndex);
  * launch shapes in turn, each timed by CUDA events on `stream`; the step
  * that completes the 24th waits for `stream` once and keeps the shape with
  * the smallest median time.  Every shape computes the same bits, so the
- * trajectory does not depend on the choice. */
+ * trajectory does not depend on the choice.
+ * A single scene created with DEM_CTX_RESIDENT, of at most 8,192 disks and
+ * 8,192 cells, one material, no attraction and no control particle, steps
+ * each call as ONE launch of a thread-block cluster of 8 blocks: every block
+ * keeps the whole scene's positions, velocities, spins and radii in its
+ * shared memory, steps an eighth of the disks and writes their new state
+ * into every block's copy through distributed shared memory.  The bits are
+ * the graph path's.  Its first call allocates the cluster's scratch (about
+ * 270 B per disk); the next graph-path step sorts from scratch.  Other
+ * scenes, calls while profiling, and GPUs that cannot hold such a cluster
+ * take the graph path. */
 int dem_step(DemContext* ctx, uint32_t nsteps, void* stream);
 
 /* Launch shapes of the step kernel (threads per block x blocks per SM its
