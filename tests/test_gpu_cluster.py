@@ -35,7 +35,8 @@ def run(sc, calls, resident, shuffle_seed=None):
         order = np.random.default_rng(shuffle_seed).permutation(sc.n)
         st = {k: (None if v is None else np.asarray(v)[order]) for k, v in st.items()}
     sim.set_state(_torch(st["pos"]), _torch(st["vel"]), _torch(st["theta"]), _torch(st["omega"]),
-                  _torch(st["radius"]), _torch(st["mass"]), _torch(st["id"]))
+                  _torch(st["radius"]), _torch(st["mass"]), _torch(st["id"]),
+                  None if st.get("type") is None else _torch(st["type"]))
     for k in calls:
         sim.step(k)
     torch.cuda.synchronize()
@@ -82,3 +83,15 @@ def test_cluster_unsorted_start_and_consecutive_calls():
 def test_cluster_declines_a_larger_scene():
     """More than 8,192 disks: the graph path steps the scene (same results)."""
     assert_same(scenes.agitated_gas(n=9000, seed=81), [10])
+
+
+@pytest.mark.parametrize("n", [1, 2, 5, 33])
+def test_cluster_tiny_scenes(n):
+    """A handful of disks: most blocks of the cluster own no slot."""
+    assert_same(scenes.agitated_gas(n=n, seed=100 + n, vel_std=1.0), [25])
+
+
+def test_cluster_declines_types_and_attraction():
+    """Several materials, or attraction: the graph path steps the scene."""
+    assert_same(scenes.agitated_gas(n=600, seed=61, n_mat=3), [20])
+    assert_same(scenes.agitated_gas(n=600, seed=62, attraction=0.05), [20])
