@@ -1470,6 +1470,10 @@ int cluster_step(DemContext* c, uint32_t nsteps, cudaStream_t st) {
 
 }  // namespace
 
+namespace {
+int step_graph_path(DemContext* c, uint32_t nsteps, cudaStream_t st);
+}  // namespace
+
 extern "C" int dem_step(DemContext* c, uint32_t nsteps, void* stream) {
     if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
     if (nsteps == 0 || c->n == 0) return DEM_OK;
@@ -1478,6 +1482,14 @@ extern "C" int dem_step(DemContext* c, uint32_t nsteps, void* stream) {
         int rc = c->nspec ? resident_step(c, nsteps, st) : cluster_step(c, nsteps, st);
         if (rc != kNotResident) return rc;
     }
+    return step_graph_path(c, nsteps, st);
+}
+
+namespace {
+// dem_step on the graph path: the sort and step graphs, or the device-side
+// step loop for pairs of steps (also the steps of dem_step_followed, whose
+// per-step rows are gathered from this path's buffers).
+int step_graph_path(DemContext* c, uint32_t nsteps, cudaStream_t st) {
     if (!c->keysValid) {
         if (c->nspec)
             DEM_TRY_CUDA(launch_calc_hash_batched(c->dTable, c->spec, c->dyn[0].pos, c->keys, c->n,
@@ -1551,6 +1563,7 @@ extern "C" int dem_step(DemContext* c, uint32_t nsteps, void* stream) {
     }
     return DEM_OK;
 }
+}  // namespace
 
 extern "C" int dem_set_step_variant(DemContext* c, int32_t variant) {
     if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
@@ -1755,7 +1768,8 @@ extern "C" int dem_step_followed(DemContext* c, uint32_t nsteps, const uint32_t*
                 DEM_TRY_CUDA(cudaGraphLaunch(c->followGraph[p], st), "graph launch");
                 j += 2 * pairs;
             } else {
-                int rc = dem_step(c, 1, stream);
+                // the graph path: the rows are gathered from its buffers
+                int rc = step_graph_path(c, 1, st);
                 if (rc) return rc;
                 DEM_TRY_CUDA(enqueue_followed_ring(c, c->cur ^ 1, nullptr, j, st), "followed gather");
                 ++j;

@@ -95,3 +95,37 @@ def test_cluster_declines_types_and_attraction():
     """Several materials, or attraction: the graph path steps the scene."""
     assert_same(scenes.agitated_gas(n=600, seed=61, n_mat=3), [20])
     assert_same(scenes.agitated_gas(n=600, seed=62, attraction=0.05), [20])
+
+
+def test_followed_rows_on_a_resident_context():
+    """dem_step_followed steps a resident context on the graph path (its rows
+    come from that path's buffers), then dem_step takes the cluster again:
+    rows and state equal a plain context's."""
+    import torch
+    import demso_b200 as D
+    sc = scenes.agitated_gas(n=1800, seed=44, vel_std=0.7)
+    ids = np.array([0, 17, 900, 1799], dtype=np.uint32)
+
+    def go(flags):
+        sim = D.Simulation(sc.sys, capacity=sc.n, flags=flags)
+        st = sc.state()
+        sim.set_state(_torch(st["pos"]), _torch(st["vel"]), _torch(st["theta"]),
+                      _torch(st["omega"]), _torch(st["radius"]), _torch(st["mass"]),
+                      _torch(st["id"]))
+        sim.step(7)
+        rows = sim.step_followed(15, ids)
+        sim.step(9)
+        torch.cuda.synchronize()
+        out = {k: (None if v is None else (v.numpy().view(np.uint32) if v.dtype == torch.int32
+                                           else v.numpy()))
+               for k, v in sim.get_state("cpu").items()}
+        sim.check()
+        sim.close()
+        return rows, out
+
+    base = D.CTX_PRESSURE | D.CTX_ACCEL
+    rows_a, a = go(base | D.CTX_RESIDENT)
+    rows_b, b = go(base)
+    assert np.array_equal(rows_a.view(np.uint32), rows_b.view(np.uint32))
+    for k in FIELDS:
+        assert same(a[k], b[k]), k
