@@ -407,7 +407,8 @@ int dem_get_followed_async(DemContext* ctx, const uint32_t* ids, uint32_t count,
  * (cudaFree/cudaMalloc, which can wait for the device) and captures the
  * step loop's graphs again; a call no larger than an earlier one allocates
  * nothing.  Callers whose id count varies can make one call with the largest
- * count first. */
+ * count first.  A context created with DEM_CTX_RESIDENT steps these calls on
+ * the graph path (same bits). */
 int dem_step_followed(DemContext* ctx, uint32_t nsteps, const uint32_t* ids, uint32_t count,
                       float* rows, void* stream);
 
