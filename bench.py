@@ -250,8 +250,9 @@ def measure_batched(steps: int, warmup: int, num: int = 4096, loop_sample: int =
     disks, own boxes/parameters; 5,000 steps issued as one dem_step call) in
     its two forms -- one persistent launch of the resident step, and one
     graph launch of the device-side step loop -- against looping the plain
-    single-scene step over an evenly spaced sample of the same specimens.
-    `value` is the faster form."""
+    single-scene step over an evenly spaced sample of the same specimens, in
+    the faster of its two forms (graph path, cluster launch).  `value` is
+    the faster batched form."""
     import torch
     import demso_b200 as D
     from demso_b200 import scenes
@@ -315,7 +316,28 @@ def measure_batched(steps: int, warmup: int, num: int = 4096, loop_sample: int =
     e1.record()
     torch.cuda.synchronize()
     sample_n = sum(sc.n for sc in sample)
-    looped = sample_n * lsteps / (e0.elapsed_time(e1) * 1e-3)
+    looped_graph = sample_n * lsteps / (e0.elapsed_time(e1) * 1e-3)
+    # the same, each specimen's context stepped as one thread-block cluster
+    # launch (DEM_CTX_RESIDENT on a single scene of at most 8,192 disks)
+    csims = []
+    for sc in sample:
+        sim = D.Simulation(sc.sys, capacity=sc.n, flags=D.CTX_PRESSURE | D.CTX_RESIDENT)
+        sim.set_state(t(sc.pos), t(sc.vel), t(sc.theta), t(sc.omega), t(sc.radius), t(sc.mass),
+                      t(sc.id))
+        sim.step(3)
+        csims.append(sim)
+    torch.cuda.synchronize()
+    e0.record()
+    for sim in csims:
+        sim.step(lsteps)
+    e1.record()
+    torch.cuda.synchronize()
+    for sim in csims:
+        sim.check()
+        sim.close()
+    looped_cluster = sample_n * lsteps / (e0.elapsed_time(e1) * 1e-3)
+    # the looped plain step in its faster form is the baseline of the ratios
+    looped = max(looped_graph, looped_cluster)
     # the weaker form measured before: single-step calls interleaved across
     # the contexts (two graph launches per specimen-step)
     isteps = 20
@@ -341,12 +363,14 @@ def measure_batched(steps: int, warmup: int, num: int = 4096, loop_sample: int =
                            "step_kernel_shape": [shape["threads"], shape["blocks_per_sm"]],
                            "form": "the %d steps as one graph launch of the device-side step "
                                    "loop, %d kernels per step" % (steps, kernels)},
+            "looped_plain_forms": {"graph_path": looped_graph, "cluster": looped_cluster},
             "looped_plain_interleaved_single_steps": interleaved,
             "ratio_vs_interleaved": batched / interleaved,
             "unit": UNIT, "specimens": num, "particles": total, "steps": steps,
             "looped_sample": "%d of the %d specimens (every %d-th), each its own context "
-                             "stepping %d steps as one dem_step call (device-side step "
-                             "loop), one specimen after another"
+                             "stepping %d steps as one dem_step call, one specimen after "
+                             "another; the faster of the graph path (device-side step "
+                             "loop) and the cluster launch"
                              % (len(sample), num, max(1, num // loop_sample), lsteps),
             "workload": "batched: specimens with counts log-uniform in [256, 8192], square "
                         "walled boxes at area fraction 0.5, radii U[0.9, 1.1] mm, kn "
