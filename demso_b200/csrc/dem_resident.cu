@@ -773,10 +773,14 @@ cluster_kernel(const __grid_constant__ KParams P, ResIO io, uint32_t n, uint32_t
     if (rank == 0 && tid < 2) W.counter()[tid] = 0u;
     int buf = 0;
     bool needSort = true, fullSort = true;
+    // the own slot's cell, angle and mass, kept in registers between sorts
+    uint32_t myKey = 0u;
+    float myTh = 0.0f, myM = 0.0f;
     cl.sync();
 #pragma unroll 1
     for (uint32_t step = 0; step < nsteps; ++step) {
         const int par = (int)(step & 1u);  // this step's movers: counter / list par
+        const bool sorting = needSort;
         if (needSort) {
             const uint32_t nm = fullSort ? 0xffffffffu : __ldcg(W.counter() + (par ^ 1));
             const uint4* __restrict__ mv = W.movers(par ^ 1);
@@ -894,11 +898,17 @@ cluster_kernel(const __grid_constant__ KParams P, ResIO io, uint32_t n, uint32_t
         // the previous step's mover count is consumed: it counts this step's
         // successor's movers next
         if (rank == 0 && tid == 0) W.counter()[par ^ 1] = 0u;
+        if (sorting && mine) {
+            // the slot now holds another disk: its cell from the copy, its
+            // angle and mass from block 0's permutation
+            myKey = local_cell(P, S.pos()[own]);
+            myTh = __ldcg(W.theta(buf) + own);
+            myM = __ldcg(W.mass(buf) + own);
+        }
         const bool last = step + 1u == nsteps;
         Dyn s;
-        bool mover = false;
         if (mine) {
-            const uint32_t keyBefore = __ldcg(W.key() + own);
+            const uint32_t keyBefore = myKey;
             float2 f;
             float moment, pr;
             s.p = S.pos()[own];
@@ -906,8 +916,8 @@ cluster_kernel(const __grid_constant__ KParams P, ResIO io, uint32_t n, uint32_t
             s.w = S.omega()[own];
             const float r = S.radius()[own];
             res_collide(P, 0u, keyBefore, own, s.p, s.v, s.w, r, S, f, moment, pr);
-            s.th = __ldcg(W.theta(buf) + own);
-            const float m = __ldcg(W.mass(buf) + own);
+            s.th = myTh;
+            const float m = myM;
             const bool quiet = f.x == 0.0f && f.y == 0.0f && moment == 0.0f && m > 0.0f &&
                                m < INFINITY;
             const float two_mrr = 2.0f * m * r * r;
@@ -921,12 +931,12 @@ cluster_kernel(const __grid_constant__ KParams P, ResIO io, uint32_t n, uint32_t
                 al = moment / inertia_of(m, r);
             }
             integrate_one(P, s, a, al, r, m, 0u, pr);
-            W.theta(buf)[own] = s.th;
+            myTh = s.th;
+            W.theta(buf)[own] = s.th;  // for block 0's permutation at the next sort
             if (!(isfinite(s.p.x) && isfinite(s.p.y))) atomicOr(errFlag, 1u);
             const uint32_t keyAfter = local_cell(P, s.p);
-            W.key()[own] = keyAfter;
+            myKey = keyAfter;
             if (keyAfter != keyBefore) {
-                mover = true;
                 const uint32_t slot = atomicAdd(W.counter() + par, 1u);
                 if (slot < kResMaxMovers)
                     W.movers(par)[slot] = make_uint4(own, keyBefore, keyAfter, 0u);
@@ -937,8 +947,9 @@ cluster_kernel(const __grid_constant__ KParams P, ResIO io, uint32_t n, uint32_t
                 if (io.alpha) io.alpha[own] = al;
             }
         }
-        (void)mover;
-        cl.sync();  // every block has read its copy: the copies may be overwritten
+        // every block has read its copy (each value read was used above), so
+        // the copies may be overwritten: an arrive without release semantics
+        asm volatile("barrier.cluster.arrive.relaxed;\n\tbarrier.cluster.wait;" ::: "memory");
         if (mine) {
 #pragma unroll 1
             for (uint32_t r = 0; r < ctas; ++r) {
@@ -956,8 +967,8 @@ cluster_kernel(const __grid_constant__ KParams P, ResIO io, uint32_t n, uint32_t
         io.vel[own] = S.vel()[own];
         io.omega[own] = S.omega()[own];
         io.radius[own] = S.radius()[own];
-        io.theta[own] = __ldcg(W.theta(buf) + own);
-        io.mass[own] = __ldcg(W.mass(buf) + own);
+        io.theta[own] = myTh;
+        io.mass[own] = myM;
         const uint32_t id = __ldcg(W.id(buf) + own);
         io.id[own] = id;
         if (id < n) io.loc[id] = own;
