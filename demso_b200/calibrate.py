@@ -328,27 +328,34 @@ class Calibration:
 def looped_window_seconds(specimens, steps: int, sample: int = 16) -> float:
     """Seconds for one window of `steps` steps of every specimen with the
     plain single-scene step looped over the specimens, extrapolated from an
-    evenly spaced sample."""
+    evenly spaced sample, in the faster of its two forms: the graph path and
+    the cluster launch (CTX_RESIDENT, for specimens of up to 8,192 disks)."""
     import torch
+    from . import CTX_RESIDENT
     picks = specimens[:: max(1, len(specimens) // sample)][:sample]
-    sims = []
-    for sc in picks:
-        sim = Simulation(sc.sys, capacity=sc.n, flags=CTX_PRESSURE)
-        t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int32)
-                                       if a.dtype == np.uint32 else np.ascontiguousarray(a))
-        sim.set_state(t(sc.pos), t(sc.vel), t(sc.theta), t(sc.omega), t(sc.radius), t(sc.mass),
-                      t(sc.id))
-        sim.step(3)
-        sims.append(sim)
-    torch.cuda.synchronize()
     k = max(3, min(steps, 200))
-    t0 = time.perf_counter()
-    for sim in sims:
-        sim.step(k)
-    torch.cuda.synchronize()
-    dt = time.perf_counter() - t0
-    for sim in sims:
-        sim.close()
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int32)
+                                   if a.dtype == np.uint32 else np.ascontiguousarray(a))
+
+    def timed(flags):
+        sims = []
+        for sc in picks:
+            sim = Simulation(sc.sys, capacity=sc.n, flags=flags)
+            sim.set_state(t(sc.pos), t(sc.vel), t(sc.theta), t(sc.omega), t(sc.radius),
+                          t(sc.mass), t(sc.id))
+            sim.step(3)
+            sims.append(sim)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for sim in sims:
+            sim.step(k)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        for sim in sims:
+            sim.close()
+        return dt
+
+    dt = min(timed(CTX_PRESSURE), timed(CTX_PRESSURE | CTX_RESIDENT))
     per_particle_step = dt / (k * sum(sc.n for sc in picks))
     per_step_launch = dt / (k * len(picks))
     # launch-bound at these sizes: scale by specimen count and steps
