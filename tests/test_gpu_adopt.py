@@ -211,16 +211,19 @@ def test_bad_sets_are_refused_before_any_launch():
     sim.close()
 
 
-def test_a_batch_steps_in_adopted_sets():
-    """The batched form in caller buffers: the concatenated specimens in
-    the first set, every specimen bit for bit the oracle's run alone."""
+@pytest.mark.parametrize("resident", [False, True])
+def test_a_batch_steps_in_adopted_sets(resident):
+    """The batched form in caller buffers, on the graph path or the resident
+    launch: the concatenated specimens in the first set, every specimen bit
+    for bit the oracle's run alone."""
     import torch
     import demso_b200 as D
     specimens = [scenes.agitated_gas(n=700, seed=84), scenes.settling_pile(side=20, box=0.05,
                                                                             seed=85, vel_std=0.3),
                  scenes.agitated_gas(n=400, seed=86, grid="ref", vel_std=1.0)]
     steps = 30
-    b = D.Batch([(sc.sys, sc.n) for sc in specimens], flags=D.CTX_CALLER_STATE)
+    b = D.Batch([(sc.sys, sc.n) for sc in specimens],
+                flags=D.CTX_CALLER_STATE | (D.CTX_RESIDENT if resident else 0))
     st = scenes.concat_specimens(specimens)
     first, second = _sets(st, False)
     b.adopt_state(first, second, b.capacity)

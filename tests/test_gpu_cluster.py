@@ -129,3 +129,32 @@ def test_followed_rows_on_a_resident_context():
     assert np.array_equal(rows_a.view(np.uint32), rows_b.view(np.uint32))
     for k in FIELDS:
         assert same(a[k], b[k]), k
+
+
+@pytest.mark.parametrize("caller_state", [False, True])
+def test_cluster_steps_in_adopted_sets(caller_state):
+    """The cluster reads and writes the caller's two ping-pong sets
+    (dem_adopt_state), with or without a context state of its own; the view
+    then shows the graph path's state."""
+    import torch
+    import demso_b200 as D
+    from helpers import gpu_run
+    from test_gpu_adopt import FIELDS as ADOPT_FIELDS, _sets, _view_np
+    sc = scenes.agitated_gas(n=2200, seed=57, vel_std=0.8)
+    chunks = [1, 9, 30]
+    ref = gpu_run(sc.sys, sc.state(), sum(chunks), chunks=chunks)
+    flags = D.CTX_PRESSURE | D.CTX_ACCEL | D.CTX_RESIDENT | (D.CTX_CALLER_STATE if caller_state
+                                                            else 0)
+    sim = D.Simulation(sc.sys, capacity=sc.n, flags=flags)
+    first, second = _sets(sc.state(), False)
+    sim.adopt_state(first, second, sc.n)
+    for c in chunks:
+        sim.step(c)
+    torch.cuda.synchronize()
+    sim.check()
+    got = _view_np(sim.state_view())
+    sim.close()
+    for k in ADOPT_FIELDS:
+        if k == "type":
+            continue
+        assert same(got[k], ref[k]), k
