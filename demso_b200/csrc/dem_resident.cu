@@ -25,6 +25,11 @@
 // shared memory (24 B per particle); angles, masses and ids are read and
 // written only by the particle's own thread and live in the block's global
 // scratch, which stays in L2.
+//
+// The same file steps a single scene of up to kResMaxParticles disks as one
+// thread-block cluster (cluster_kernel, below): every block holds the whole
+// scene, steps its share of the slots and broadcasts their new state to the
+// other blocks through distributed shared memory.
 #include <algorithm>
 
 #include <cooperative_groups.h>
@@ -668,10 +673,11 @@ resident_kernel(const KParams* __restrict__ table, const ResBin* __restrict__ bi
 //   sort      only after a step in which a disk changed cell: every block
 //             runs the same sort (incremental or full, as above) on its own
 //             copy, which gives the same permutation in every block; block 0
-//             also moves the angles, masses, ids and cells, which live in
-//             global memory;
+//             also moves the angles, masses and ids, which live in global
+//             memory;
 //   collide   the block's slots against its own copy;
-//   integrate the block's slots, held in registers;
+//   integrate the block's slots, held in registers (a thread keeps its
+//             slot's cell, angle and mass in registers between sorts);
 //   broadcast after a cluster barrier (every copy read), each block writes
 //             its slots' new positions, velocities and spins into every
 //             block's copy through distributed shared memory; a second
