@@ -158,3 +158,48 @@ def test_cluster_steps_in_adopted_sets(caller_state):
         if k == "type":
             continue
         assert same(got[k], ref[k]), k
+
+
+def test_nan_is_reported_on_the_resident_paths():
+    """A NaN position: the cluster launch and the resident batch set the
+    error word (dem_check: DEM_ERR_OOB) and carry the NaN exactly as the
+    graph path does."""
+    import torch
+    import demso_b200 as D
+    sc = scenes.agitated_gas(n=1000, seed=2)
+    sc.pos[10] = [np.nan, 0.01]
+
+    def state_after(flags):
+        sim = D.Simulation(sc.sys, capacity=sc.n, flags=D.CTX_PRESSURE | D.CTX_ACCEL | flags)
+        st = sc.state()
+        sim.set_state(_torch(st["pos"]), _torch(st["vel"]), _torch(st["theta"]),
+                      _torch(st["omega"]), _torch(st["radius"]), _torch(st["mass"]),
+                      _torch(st["id"]))
+        sim.step(6)
+        torch.cuda.synchronize()
+        out = {k: (None if v is None else (v.numpy().view(np.uint32) if v.dtype == torch.int32
+                                           else v.numpy()))
+               for k, v in sim.get_state("cpu").items()}
+        with pytest.raises(D.DemError) as err:
+            sim.check()
+        sim.close()
+        return out, err.value.code
+
+    a, code_a = state_after(0)
+    b, code_b = state_after(D.CTX_RESIDENT)
+    assert code_a == code_b == 3
+    for k in FIELDS:
+        assert same(a[k], b[k]), k
+
+    specimens = [sc, scenes.agitated_gas(n=500, seed=3)]
+    bt = D.Batch([(s.sys, s.n) for s in specimens],
+                 flags=D.CTX_PRESSURE | D.CTX_ACCEL | D.CTX_RESIDENT)
+    st = scenes.concat_specimens(specimens)
+    bt.set_state(_torch(st["pos"]), _torch(st["vel"]), _torch(st["theta"]),
+                 _torch(st["omega"]), _torch(st["radius"]), _torch(st["mass"]), _torch(st["id"]))
+    bt.step(6)
+    torch.cuda.synchronize()
+    with pytest.raises(D.DemError) as err:
+        bt.check()
+    assert err.value.code == 3
+    bt.close()
