@@ -709,8 +709,9 @@ def main_slabs(args, world, rank, local, dist):
                                                    stepper.sys.gy),
                                n_particles=total,
                                parallelism="slab decomposition over %d ranks: halo windows of "
-                                           "%d rows, bands exchanged every %d steps over NCCL"
-                                           % (world, slab.halo, args.period),
+                                           "%d rows, bands exchanged every %d steps over %s"
+                                           % (world, slab.halo, args.period,
+                                              "NCCL" if args.comm_backend == "nccl" else "gloo"),
                                slab_rows=bounds, window_capacity=cap),
                 "timed_repeats": {"count": int(len(reps)), "statistic": "median",
                                   "timed_s": float(np.sum(reps)) * 1e-3},
