@@ -759,7 +759,7 @@ def main():
     ap.add_argument("--direct", action="store_true",
                     help="launch each kernel directly instead of through CUDA graphs "
                          "(for per-kernel profilers; one host read-back per step)")
-    ap.add_argument("--period", type=int, default=25,
+    ap.add_argument("--period", type=int, default=40,
                     help="N > 1: steps between the slabs' band exchanges")
     ap.add_argument("--comm-backend", default="nccl", choices=["nccl", "gloo"],
                     help="N > 1: process-group backend; gloo moves the bands through host "

@@ -300,7 +300,7 @@ class ContextStepper:
     module docstring) so that the context's graphs survive rebuilds; a window
     that outgrows the count gets a new context with room to spare."""
 
-    SPARE = 0.05  # capacity above the first window's particle count
+    SPARE = 0.01  # capacity above the first window's particle count
 
     def __init__(self, sys, rmax: float, flags=None, device="cuda"):
         import torch
