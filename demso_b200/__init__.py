@@ -182,14 +182,22 @@ def integrateSystem(sys: System, pos, vel, acc, theta, omega, alpha, type_, radi
 class Simulation:
     """Library-owned state and the fused, graph-captured step (dem_step)."""
 
-    def __init__(self, sys: System, capacity: int, flags: int = CTX_PRESSURE, _handle=None):
+    def __init__(self, sys: System, capacity: int, flags: int = CTX_PRESSURE, _handle=None,
+                 rows=None):
+        """`rows` = (first, count): a context over those cell rows of the
+        grid only (dem_create_rows); None for the whole grid."""
         import ctypes as C
         self.sys = sys
         self.capacity = int(capacity)
         self.flags = flags
+        self.rows = None if rows is None else (int(rows[0]), int(rows[1]))
         if _handle is None:
             self._h = C.c_void_p()
-            check(load().dem_create(sys.to_c(0), self.capacity, flags, C.byref(self._h)))
+            if self.rows is None:
+                check(load().dem_create(sys.to_c(0), self.capacity, flags, C.byref(self._h)))
+            else:
+                check(load().dem_create_rows(sys.to_c(0), self.capacity, flags, self.rows[0],
+                                             self.rows[1], C.byref(self._h)))
         else:
             self._h = _handle
         self.n = 0

@@ -101,6 +101,7 @@ SIGNATURES = [
     ("dem_collide", C.c_int, [_SYS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _U, _U, _P, _P]),
     ("dem_integrate_system", C.c_int, [_SYS, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _U, _P]),
     ("dem_create", C.c_int, [_SYS, _U, _U, C.POINTER(_P)]),
+    ("dem_create_rows", C.c_int, [_SYS, _U, _U, _U, _U, C.POINTER(_P)]),
     ("dem_batch_create", C.c_int, [_SYS, _U, _U, C.POINTER(_P)]),
     ("dem_batch_specimen", C.c_int, [_P, _U, C.POINTER(_U), C.POINTER(_U)]),
     ("dem_batch_set_systems", C.c_int, [_P, _P, _U, _P]),

@@ -306,6 +306,9 @@ struct DemContext {
     DemSystem sys;
     KParams P;
     uint32_t capacity = 0, n = 0, flags = 0, numCells = 0, keyBits = 0;
+    // Row window (dem_create_rows): the context's cells are the scene's rows
+    // rowFirst .. rowFirst + rows - 1; rows 0 for the whole grid.
+    uint32_t rowFirst = 0, rows = 0;
     int device = 0;
     bool typed = false;
     // The current state (order of the last sort): positions in dyn[0].pos,
@@ -440,6 +443,17 @@ struct DemContext {
 };
 
 namespace {
+
+// Kernel parameters of a single-scene context over `n` particles: the
+// scene's, with a row window's row count and first row.
+KParams scene_kparams(const DemContext* c, uint32_t n) {
+    KParams P = make_kparams(&c->sys, n);
+    if (c->rows) {
+        P.gy = c->rows;
+        P.rowOff = (int32_t)c->rowFirst;
+    }
+    return P;
+}
 
 // rounds of the autotuner: every variant once per round, the first round
 // (cold instruction caches, first graph launches) not counted
@@ -844,15 +858,36 @@ extern "C" int dem_create(const DemSystem* sys, uint32_t capacity, uint32_t flag
     *out = nullptr;
     int rc = validate(sys);
     if (rc) return rc;
+    return dem_create_rows(sys, capacity, flags, 0, sys->gridSize[1], out);
+}
+
+extern "C" int dem_create_rows(const DemSystem* sys, uint32_t capacity, uint32_t flags,
+                               uint32_t rowFirst, uint32_t rowCount, DemContext** out) {
+    if (!out) return fail(DEM_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    int rc = validate(sys);
+    if (rc) return rc;
     if (capacity == 0) return fail(DEM_ERR_INVALID_ARG, "capacity must be > 0");
     if (capacity >= (1u << 30)) return fail(DEM_ERR_INVALID_ARG, "capacity must be < 2^30");
+    const uint32_t gy = sys->gridSize[1];
+    if (!is_pow2(rowCount) || rowCount > gy)
+        return fail(DEM_ERR_INVALID_ARG, "rowCount %u: a power of two, at most the grid's %u rows",
+                    rowCount, gy);
+    if (rowFirst >= gy)
+        return fail(DEM_ERR_INVALID_ARG, "rowFirst %u outside the grid's %u rows", rowFirst, gy);
     DemContext* c = new (std::nothrow) DemContext();
     if (!c) return fail(DEM_ERR_NO_MEMORY, "host allocation failed");
     c->sys = *sys;
     c->flags = flags;
     c->typed = sys->numMaterials > 1;
-    c->P = make_kparams(sys, 0);
-    return init_context(c, capacity, sys->gridSize[0] * sys->gridSize[1], out);
+    // the whole grid is no window: rows 0 keeps every kernel parameter the
+    // scene's own
+    if (rowFirst != 0 || rowCount != gy) {
+        c->rowFirst = rowFirst;
+        c->rows = rowCount;
+    }
+    c->P = scene_kparams(c, 0);
+    return init_context(c, capacity, sys->gridSize[0] * rowCount, out);
 }
 
 extern "C" int dem_batch_create(const DemSystem* specs, uint32_t numSpecimens, uint32_t flags,
@@ -1072,7 +1107,7 @@ extern "C" int dem_set_system(DemContext* c, const DemSystem* sys) {
     if ((sys->numMaterials > 1) != c->typed)
         return fail(DEM_ERR_INVALID_ARG, "single/multi-material layout is fixed at dem_create");
     c->sys = *sys;
-    c->P = make_kparams(sys, c->n);
+    c->P = scene_kparams(c, c->n);
     set_rmax(c->P, c->rmax);
     drop_graphs(c);
     // keys depend on the box size; recompute them and sort from scratch
@@ -1165,7 +1200,7 @@ int accept_state(DemContext* c, uint32_t n, cudaStream_t st) {
                                 cudaMemcpyHostToDevice),
                      "specimen table");
     } else {
-        c->P = make_kparams(&c->sys, n);
+        c->P = scene_kparams(c, n);
         set_rmax(c->P, c->rmax);
     }
     drop_graphs(c);
@@ -1441,7 +1476,8 @@ int resident_step(DemContext* c, uint32_t nsteps, cudaStream_t st) {
 // when no such cluster can be resident on this GPU; the graph path steps
 // those.  The next graph-path step sorts from scratch.
 int cluster_step(DemContext* c, uint32_t nsteps, cudaStream_t st) {
-    if (c->typed || c->ctlOn || c->profiling || c->clusterUnsupported || !has_state_sets(c) ||
+    if (c->typed || c->ctlOn || c->profiling || c->clusterUnsupported || c->rows ||
+        !has_state_sets(c) ||
         has_attraction_host(c->P) || !cluster_scene_fits(c->n, c->numCells))
         return kNotResident;
     const size_t bytes = cluster_scene_work_bytes(c->n);
@@ -1610,10 +1646,14 @@ extern "C" int dem_row_slots(DemContext* c, uint32_t rowLo, uint32_t rowHi, uint
     if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
     if (c->nspec) return fail(DEM_ERR_INVALID_ARG, "dem_row_slots takes a single scene");
     if (!first || !count) return fail(DEM_ERR_INVALID_ARG, "dem_row_slots: NULL output");
-    const uint32_t gx = c->sys.gridSize[0], gy = c->sys.gridSize[1];
-    if (rowLo > rowHi || rowHi > gy)
-        return fail(DEM_ERR_INVALID_ARG, "rows [%u, %u) outside the grid's %u rows", rowLo, rowHi,
-                    gy);
+    // the scene's rows; a row window holds rows [rowFirst, rowFirst + rows)
+    const uint32_t gx = c->sys.gridSize[0];
+    const uint32_t lo0 = c->rowFirst, hi0 = c->rowFirst + (c->rows ? c->rows : c->sys.gridSize[1]);
+    if (rowLo > rowHi || rowLo < lo0 || rowHi > hi0)
+        return fail(DEM_ERR_INVALID_ARG, "rows [%u, %u) outside the context's rows [%u, %u)",
+                    rowLo, rowHi, lo0, hi0);
+    rowLo -= lo0;
+    rowHi -= lo0;
     if (!c->inSortOrder)
         return fail(DEM_ERR_INVALID_ARG, "the state is not in the order of a sort: step first");
     cudaStream_t st = (cudaStream_t)stream;
@@ -2041,6 +2081,7 @@ int adj_check_context(DemContext* c) {
     if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
     if (c->typed) return fail(DEM_ERR_INVALID_ARG, "the adjoint takes a single material");
     if (c->ctlOn) return fail(DEM_ERR_INVALID_ARG, "the adjoint has no control particle");
+    if (c->rows) return fail(DEM_ERR_INVALID_ARG, "the adjoint takes a context over the whole grid");
     if (!(c->flags & DEM_CTX_ACCEL)) return fail(DEM_ERR_INVALID_ARG, "create the context with DEM_CTX_ACCEL");
     const uint32_t ns = c->nspec ? c->nspec : 1u;
     for (uint32_t s = 0; s < ns; ++s) {

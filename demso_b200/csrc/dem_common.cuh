@@ -53,6 +53,11 @@ struct KParams {
     uint32_t cellOff;
     uint32_t log2gx;
     uint32_t cull;
+    // Row window: the context's cell rows are the scene's rows rowOff,
+    // rowOff + 1, ... (gy of them, wrapping); gyf, Ly, cellH and invLy stay
+    // the whole scene's, so positions give the scene's rows bit for bit.
+    // 0 for a context over the whole grid and for every batch.
+    int32_t rowOff;
 };
 
 // particles_kernel.cuh:36-41, evaluated on the host when KParams is built.
@@ -94,11 +99,19 @@ __device__ __forceinline__ int2 grid_pos_fast(const KParams& P, float2 p) {
                      grid_axis_fast(p.y, P.gyf, P.Ly, P.invLy));
 }
 
-// particles_kernel.cuh:124-130: power-of-two wrap, row-major cell index.
-__device__ __forceinline__ uint32_t grid_hash(const KParams& P, int x, int y) {
+// particles_kernel.cuh:124-130: power-of-two wrap, row-major cell index, for
+// a cell given in the context's own rows (a key's decoded row and its
+// neighbours).
+__device__ __forceinline__ uint32_t cell_index(const KParams& P, int x, int y) {
     x &= (int)(P.gx - 1u);
     y &= (int)(P.gy - 1u);
     return P.cellOff + (uint32_t)y * P.gx + (uint32_t)x;
+}
+
+// The same for a cell given in the scene's rows (grid_pos of a position): a
+// row window first moves the row to its own numbering.
+__device__ __forceinline__ uint32_t grid_hash(const KParams& P, int x, int y) {
+    return cell_index(P, x, y - P.rowOff);
 }
 
 // `pressure += length(force) / (4*M_PI*r*r)` -- the reference does this sum in

@@ -185,6 +185,8 @@ __device__ __forceinline__ void candidate(const KParams& P, uint32_t j, float2 p
 //    least 3 cells per axis and cells wider than 2 rmax (then the three
 //    columns/rows are distinct cells and a wrapped neighbour is out of
 //    reach) and a particle inside the box by more than the margin.
+// `g` is the particle's cell in the context's rows (for a row window, the
+// scene's row minus rowOff).
 template <bool TYPED, bool ATTRACT, bool CULL, typename Cells>
 __device__ __forceinline__ void collide_one(const KParams& P, uint32_t i, int2 g, float2 p,
                                             float2 v, float w, float r, uint32_t mat,
@@ -203,7 +205,8 @@ __device__ __forceinline__ void collide_one(const KParams& P, uint32_t i, int2 g
     if (CULL && p.x > P.cullMargin && p.x < P.Lx - P.cullMargin && p.y > P.cullMargin &&
         p.y < P.Ly - P.cullMargin) {
         const float reach = (r + P.rmax) * 1.0001f + P.cullMargin;
-        const float X0 = (float)g.x * P.cellW, Y0 = (float)g.y * P.cellH;
+        // the cell's lower corner; a row window's rows are the scene's from rowOff
+        const float X0 = (float)g.x * P.cellW, Y0 = (float)(g.y + P.rowOff) * P.cellH;
         if (p.x - X0 > reach) x0 = 0;
         if (X0 + P.cellW - p.x > reach) x1 = 0;
         if (p.y - Y0 > reach) y0 = 0;
@@ -215,7 +218,7 @@ __device__ __forceinline__ void collide_one(const KParams& P, uint32_t i, int2 g
     for (int dy = y0; dy <= y1; ++dy) {
 #pragma unroll 1
         for (int dx = x0; dx <= x1; ++dx) {
-            const uint2 se = cells.get(grid_hash(P, g.x + dx, g.y + dy));
+            const uint2 se = cells.get(cell_index(P, g.x + dx, g.y + dy));
             float2 fc = make_float2(0.0f, 0.0f);
             // empty cells have start >= end (start 0xFFFFFFFF): no iterations
             const uint32_t count = se.y > se.x ? se.y - se.x : 0u;
@@ -292,7 +295,7 @@ __device__ __forceinline__ bool collide_rows(const KParams& P, uint32_t i, int2 
     if (p.x > P.cullMargin && p.x < P.Lx - P.cullMargin && p.y > P.cullMargin &&
         p.y < P.Ly - P.cullMargin) {
         const float reach = (r + P.rmax) * 1.0001f + P.cullMargin;
-        const float X0 = (float)g.x * P.cellW, Y0 = (float)g.y * P.cellH;
+        const float X0 = (float)g.x * P.cellW, Y0 = (float)(g.y + P.rowOff) * P.cellH;
         if (p.x - X0 > reach) x0 = 0;
         if (X0 + P.cellW - p.x > reach) x1 = 0;
         if (p.y - Y0 > reach) y0 = 0;
@@ -396,7 +399,9 @@ collide_kernel(KParams P, const float2* __restrict__ pos, const float2* __restri
     const uint32_t mat = TYPED ? type[i] : 0u;
     float2 f;
     float moment, pr;
-    collide_one<TYPED, ATTRACT, false>(P, i, grid_pos(P, p), p, v, w, r, mat, pos, vel, omega,
+    int2 g = grid_pos(P, p);
+    g.y -= P.rowOff;  // collide_one takes the cell in the context's rows
+    collide_one<TYPED, ATTRACT, false>(P, i, g, p, v, w, r, mat, pos, vel, omega,
                                        radius, type, nullptr, SplitCells{cellStart, cellEnd}, f,
                                        moment, pr);
     const float m = mass[i];

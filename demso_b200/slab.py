@@ -312,6 +312,7 @@ class ContextStepper:
         self.typed = len(sys.materials) > 1
         self.sim = None
         self.capacity = 0
+        self.rows = (0, sys.gy)  # the context's cell rows (first, count)
         self.gid = None     # global id of every window-local id (-1: parked)
         self.m = 0          # real particles of the window
         self._park = None
@@ -330,17 +331,45 @@ class ContextStepper:
             t[k] = torch.from_numpy(a).to(self.device)
         return t
 
-    def _free_rows(self, window):
-        """Rows two or more rows away from the window."""
+    def _context_rows(self, window, parked: int):
+        """(first, count) cell rows for a window's context: the window's rows,
+        a row clear of them on either side and rows for `parked` parked
+        particles, rounded up to a power of two (dem_create_rows); the whole
+        grid when that reaches it.  A window of a tall scene then sorts and
+        scans its own cells only."""
         wlo, whi = window
-        return [y for y in range(self.sys.gy) if y < wlo - 1 or y >= whi + 1]
+        gx, gy = self.sys.gx, self.sys.gy
+        need = (whi - wlo) + 2 + -(-int(parked) // gx)
+        count = 1
+        while count < need:
+            count <<= 1
+        return (0, gy) if count >= gy else (wlo, count)
+
+    def _free_rows(self, window, rows=None):
+        """Scene rows for parked particles: rows whose cell row in the
+        context (rows = (first, count); (R - wlo) mod count relative to the
+        window) is at least one row clear of the window's on either side,
+        each cell row once.  They are two or more rows from the window in the
+        scene too, so no window particle ever visits their cells."""
+        rows = rows or self.rows
+        key = (tuple(window), tuple(rows))
+        cache = self.__dict__.setdefault("_free_cache", {})
+        if key not in cache:
+            wlo, whi = window
+            count, m = rows[1], whi - wlo
+            y = np.arange(self.sys.gy, dtype=np.int64)
+            lr = (y - wlo) % count
+            ok = (lr >= m + 1) & (lr < count - 1)
+            # the first scene row of each cell row
+            _, first = np.unique(lr[ok], return_index=True)
+            cache[key] = np.sort(y[ok][first]).tolist()
+        return cache[key]
 
     def _parked(self, count: int, window) -> dict:
-        """`count` parked particles in cells of rows two or more rows away
-        from the window, one per cell (built once per window and count
-        bound, then sliced)."""
+        """`count` parked particles in the cells of the free rows, one per
+        cell (built once per window and count bound, then sliced)."""
         import torch
-        key = window
+        key = (window, self.rows)
         if self._park is None or self._park[0] != key or self._park[1] < count:
             sys = self.sys
             free = self._free_rows(window)
@@ -376,15 +405,21 @@ class ContextStepper:
         parts = [p.to(self.device) if torch.is_tensor(p) else p for p in parts]
         st = concat(parts, self.typed)
         m = int(st["pos"].shape[0])
-        parking = bool(self._free_rows(window))
         # without free rows (one slab) the window is the whole scene: no padding
+        parking = bool(self._free_rows(window, (0, self.sys.gy)))
         want = int(m * (1.0 + self.SPARE)) + 64 if parking else m
+        room = len(self._free_rows(window)) * self.sys.gx if self.sim is not None else 0
         if self.sim is None or m + (1 if parking else 0) > self.capacity or \
-                (not parking and m != self.capacity):
+                (not parking and m != self.capacity) or \
+                (parking and self.capacity - m > room):
             if self.sim is not None:
                 self.sim.close()
             self.capacity = want
-            self.sim = Simulation(self.sys, capacity=self.capacity, flags=self.flags)
+            # rows for four times the first window's parked particles
+            self.rows = self._context_rows(window, 4 * (want - m) if parking else 0)
+            whole = self.rows == (0, self.sys.gy)
+            self.sim = Simulation(self.sys, capacity=self.capacity, flags=self.flags,
+                                  rows=None if whole else self.rows)
         if parking:
             st = concat([st, self._parked(self.capacity - m, window)], self.typed)
         self.gid = st["id"]

@@ -187,6 +187,22 @@ typedef struct DemContext DemContext;
                                  as one thread-block cluster (see dem_step) */
 
 int dem_create(const DemSystem* sys, uint32_t capacity, uint32_t flags, DemContext** out);
+/* A context over the cell rows [rowFirst, rowFirst + rowCount) of sys's grid
+ * (rowCount a power of two, at most gridSize[1]; rowFirst < gridSize[1]):
+ * what a slab of a row decomposition steps.  Cells, keys and the sort span
+ * only those rows, so a window of a tall scene sorts and scans its own cells,
+ * not the scene's.  Positions give the scene's rows bit for bit (same box,
+ * grid and walls); a row r then has the cell row (r - rowFirst) mod rowCount,
+ * so the particles of rows [rowFirst, rowFirst + rowCount) are stepped
+ * exactly as by a context over the whole grid (their neighbour rows must be
+ * within the window too), while a particle outside them shares cells with
+ * distant rows and misses its true neighbours, as one beyond a slab's edge
+ * does.
+ * dem_row_slots takes the scene's rows.  The cluster form of DEM_CTX_RESIDENT
+ * and the adjoint take whole grids only.  rowFirst 0 and rowCount gridSize[1]
+ * is dem_create.  No reference counterpart. */
+int dem_create_rows(const DemSystem* sys, uint32_t capacity, uint32_t flags, uint32_t rowFirst,
+                    uint32_t rowCount, DemContext** out);
 int dem_destroy(DemContext* ctx);
 /* Runtime parameter change (gravity, dt, materials; grid size and particle
  * count fixed): the reference's set_gravity (functions.cu:663-668) generalised. */
@@ -361,7 +377,8 @@ int dem_debug_sort_hold(DemContext* ctx, uint32_t holdTile, uint32_t spinLimit);
 /* The slots [*first, *first + *count) of the current state whose cell (the
  * sort key of the last step's sort, which ordered the state) lies in grid
  * rows [rowLo, rowHi): one contiguous range, since keys are numbered row by
- * row.  A slab decomposition cuts its bands and its own rows this way.  Needs
+ * row.  Rows are the scene's; a row window (dem_create_rows) takes rows
+ * within its own.  A slab decomposition cuts its bands and own rows this way.  Needs
  * a step since the last dem_set_state / dem_adopt_state; single scenes only;
  * synchronises `stream`.  No reference counterpart. */
 int dem_row_slots(DemContext* ctx, uint32_t rowLo, uint32_t rowHi, uint32_t* first,

@@ -118,14 +118,15 @@ def gpu_stages(sys: System, st: dict) -> dict:
     return out
 
 
-def gpu_run(sys: System, st: dict, steps: int, flags=None, chunks=None) -> dict:
-    """`steps` full steps through the context API (fused kernels, graphs)."""
+def gpu_run(sys: System, st: dict, steps: int, flags=None, chunks=None, rows=None) -> dict:
+    """`steps` full steps through the context API (fused kernels, graphs);
+    `rows` = (first, count) steps a row window (dem_create_rows)."""
     import torch
     import demso_b200 as D
     if flags is None:
         flags = D.CTX_PRESSURE | D.CTX_ACCEL
     n = st["pos"].shape[0]
-    sim = D.Simulation(sys, capacity=max(n, 1), flags=flags)
+    sim = D.Simulation(sys, capacity=max(n, 1), flags=flags, rows=rows)
     typed = st.get("type") is not None
     to = (lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int32).copy())
           if a.dtype == np.uint32 else torch.from_numpy(np.ascontiguousarray(a).copy()))
