@@ -1646,9 +1646,10 @@ extern "C" int dem_row_slots(DemContext* c, uint32_t rowLo, uint32_t rowHi, uint
     if (!c) return fail(DEM_ERR_INVALID_ARG, "context is NULL");
     if (c->nspec) return fail(DEM_ERR_INVALID_ARG, "dem_row_slots takes a single scene");
     if (!first || !count) return fail(DEM_ERR_INVALID_ARG, "dem_row_slots: NULL output");
-    // the scene's rows; a row window holds rows [rowFirst, rowFirst + rows)
-    const uint32_t gx = c->sys.gridSize[0];
-    const uint32_t lo0 = c->rowFirst, hi0 = c->rowFirst + (c->rows ? c->rows : c->sys.gridSize[1]);
+    // the scene's rows; a row window holds rows [rowFirst, rowFirst + rows),
+    // of which those past the grid's last row do not exist
+    const uint32_t gx = c->sys.gridSize[0], gy = c->sys.gridSize[1];
+    const uint32_t lo0 = c->rowFirst, hi0 = std::min(c->rowFirst + (c->rows ? c->rows : gy), gy);
     if (rowLo > rowHi || rowLo < lo0 || rowHi > hi0)
         return fail(DEM_ERR_INVALID_ARG, "rows [%u, %u) outside the context's rows [%u, %u)",
                     rowLo, rowHi, lo0, hi0);

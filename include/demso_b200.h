@@ -378,7 +378,8 @@ int dem_debug_sort_hold(DemContext* ctx, uint32_t holdTile, uint32_t spinLimit);
  * sort key of the last step's sort, which ordered the state) lies in grid
  * rows [rowLo, rowHi): one contiguous range, since keys are numbered row by
  * row.  Rows are the scene's; a row window (dem_create_rows) takes rows
- * within its own.  A slab decomposition cuts its bands and own rows this way.  Needs
+ * within its own block and the grid.  A slab decomposition cuts its bands and
+ * own rows this way.  Needs
  * a step since the last dem_set_state / dem_adopt_state; single scenes only;
  * synchronises `stream`.  No reference counterpart. */
 int dem_row_slots(DemContext* ctx, uint32_t rowLo, uint32_t rowHi, uint32_t* first,

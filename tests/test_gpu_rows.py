@@ -113,6 +113,25 @@ def test_row_slots_take_the_scenes_rows():
         win.close()
 
 
+def test_row_slots_stop_at_the_grids_last_row():
+    """A block of rows that runs past the grid's top (rows 96..159 of 128):
+    dem_row_slots takes rows up to 128, not beyond."""
+    import torch
+    from demso_b200 import DemError
+    sys, st = _band()
+    win = _sim(sys, st, (96, 64))
+    try:
+        win.step(2)
+        torch.cuda.synchronize()
+        first, count = _row_slots(win, 96, 128)
+        assert first + count <= st["pos"].shape[0]
+        for lo, hi in [(96, 129), (95, 100), (120, 160)]:
+            with pytest.raises(DemError):
+                _row_slots(win, lo, hi)
+    finally:
+        win.close()
+
+
 @pytest.mark.parametrize("first,count", [(0, 48), (0, 256), (128, 32), (10, 0)])
 def test_bad_row_windows_are_refused(first, count):
     import demso_b200 as D
