@@ -511,6 +511,8 @@ MoverSinkArgs sink_of(DemContext* c) {
     m.movers = c->inc.movers;
     m.ctrl = c->inc.ctrl;
     m.moverCap = c->inc.moverCap;
+    m.tileShift = c->inc.tileShift;
+    m.dirty = c->inc.dirty;
     return m;
 }
 
@@ -530,14 +532,15 @@ cudaError_t enqueue_full_sort(DemContext* c, int a, cudaStream_t st, int* launch
 
 cudaError_t enqueue_inc_tail(DemContext* c, int a, cudaStream_t st, int* launches) {
     const int b = a ^ 1;
-    return enqueue_incremental_tail(c->inc, c->n, c->keys, c->skey[a], c->cells[a], c->skey[b],
-                                    c->cells[b], c->first[b], sort_move(c, a), st, launches,
-                                    c->moverStream, c->moverForkEv, c->moverJoinEv);
+    return enqueue_incremental_tail(c->inc, c->n, c->keys, c->skey[a], c->cells[a], c->first[a],
+                                    c->skey[b], c->cells[b], c->first[b], sort_move(c, a), st,
+                                    launches, c->moverStream, c->moverForkEv, c->moverJoinEv);
 }
 
 // The incremental sort launched directly (the host chose it).
 cudaError_t enqueue_inc_sort(DemContext* c, int a, cudaStream_t st, int* launches) {
-    cudaError_t e = enqueue_incremental_head(c->inc, c->cells[a], 0, false, st, launches);
+    cudaError_t e = enqueue_incremental_head(c->inc, c->cells[a], c->first[a], 0, false, st,
+                                             launches);
     return e == cudaSuccess ? enqueue_inc_tail(c, a, st, launches) : e;
 }
 
@@ -596,7 +599,8 @@ cudaError_t enqueue_sort_phase(DemContext* c, int kind, cudaStream_t st, int* la
     if (status != cudaStreamCaptureStatusActive) return cudaErrorStreamCaptureUnsupported;
     cudaGraphConditionalHandle hFull;
     e = cudaGraphConditionalHandleCreate(&hFull, g, 0, cudaGraphCondAssignDefault);
-    if (e == cudaSuccess) e = enqueue_incremental_head(c->inc, c->cells[a], hFull, true, st, launches);
+    if (e == cudaSuccess)
+        e = enqueue_incremental_head(c->inc, c->cells[a], c->first[a], hFull, true, st, launches);
     if (e != cudaSuccess) return e;
     e = cudaEventRecord(c->forkEv, st);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(c->forkStream, c->forkEv, 0);

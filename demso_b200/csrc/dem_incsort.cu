@@ -25,6 +25,11 @@ inline size_t cell_blocks(uint32_t numCells) {
     return (numCells + chunk - 1) / chunk;
 }
 inline unsigned blocks_for(size_t n, int t) { return (unsigned)((n + (size_t)t - 1) / (size_t)t); }
+inline uint32_t log2_of(uint32_t pow2) {
+    uint32_t k = 0;
+    while ((1u << k) < pow2) ++k;
+    return k;
+}
 inline size_t al256(size_t b) { return (b + 255u) & ~(size_t)255u; }
 
 __global__ void fill_u32_kernel(uint32_t* __restrict__ p, uint32_t value, size_t count) {
@@ -82,14 +87,20 @@ __device__ __forceinline__ unsigned long long cell_counts(const uint2* __restric
     return (unsigned long long)cnt | ((unsigned long long)ac << 32);
 }
 
+// Whether no mover left or entered scan tile `tile` (its bit is clear).
+__device__ __forceinline__ bool tile_clean(const uint32_t* __restrict__ dirty, uint32_t tile) {
+    return dirty != nullptr && ((dirty[tile >> 5] >> (tile & 31u)) & 1u) == 0u;
+}
+
 // Every kernel of the incremental path returns at once when the last step
 // asked for the full path.  The first one reads that request
 // (ctrl[kCtrlNeedFull]), keeps it for the others in ctrl[kCtrlPath] (the full
 // path, which may run beside them, clears the request) and passes it to the
 // graph's conditional node that runs the full path.
 __global__ void __launch_bounds__(kThreads)
-cells_reduce_kernel(const uint2* __restrict__ prevCells, const uint32_t* __restrict__ leavers,
-                    const uint32_t* __restrict__ arrCnt, uint32_t numCells, uint32_t items,
+cells_reduce_kernel(const uint2* __restrict__ prevCells, const uint32_t* __restrict__ prevFirst,
+                    const uint32_t* __restrict__ leavers, const uint32_t* __restrict__ arrCnt,
+                    const uint32_t* __restrict__ dirty, uint32_t numCells, uint32_t items,
                     unsigned long long* __restrict__ partials, uint32_t* __restrict__ ctrl,
                     const uint32_t* __restrict__ errFlag, cudaGraphConditionalHandle full,
                     int setFull) {
@@ -105,8 +116,16 @@ cells_reduce_kernel(const uint2* __restrict__ prevCells, const uint32_t* __restr
         if (setFull) cudaGraphSetConditional(full, needFull ? 1u : 0u);
     }
     if (needFull) return;
-    __shared__ unsigned long long warpTot[kThreads / 32];
     const size_t base = (size_t)blockIdx.x * kThreads * items;
+    if (tile_clean(dirty, blockIdx.x)) {
+        // no leavers or arrivals: the tile keeps its particle count
+        if (threadIdx.x == 0) {
+            const size_t end = min(base + (size_t)kThreads * items, (size_t)numCells);
+            partials[blockIdx.x] = (unsigned long long)(prevFirst[end] - prevFirst[base]);
+        }
+        return;
+    }
+    __shared__ unsigned long long warpTot[kThreads / 32];
     unsigned long long s = 0;
 #pragma unroll 2
     for (uint32_t k = 0; k < items; ++k) {
@@ -144,8 +163,9 @@ cells_top_kernel(unsigned long long* __restrict__ partials, uint32_t np,
 // cells, processed in `items` block-wide slabs so every access is coalesced; the
 // per-cell counters are cleared for the next step.
 __global__ void __launch_bounds__(kThreads)
-cells_apply_kernel(const uint2* __restrict__ prevCells, uint32_t* __restrict__ leavers,
-                   uint32_t* __restrict__ arrCnt, uint32_t* __restrict__ arrLo,
+cells_apply_kernel(const uint2* __restrict__ prevCells, const uint32_t* __restrict__ prevFirst,
+                   uint32_t* __restrict__ leavers, uint32_t* __restrict__ arrCnt,
+                   uint32_t* __restrict__ arrLo, uint32_t* __restrict__ dirty,
                    uint32_t numCells, uint32_t items,
                    const unsigned long long* __restrict__ partials,
                    uint2* __restrict__ newCells, uint32_t* __restrict__ newFirst,
@@ -155,6 +175,23 @@ cells_apply_kernel(const uint2* __restrict__ prevCells, uint32_t* __restrict__ l
     __shared__ unsigned long long warpTot[kThreads / 32];
     const size_t base = (size_t)blockIdx.x * kThreads * items;
     unsigned long long carry = partials[blockIdx.x];
+    if (tile_clean(dirty, blockIdx.x)) {
+        // no leavers or arrivals: every cell keeps its particles, shifted by
+        // the movers of the tiles below; no counter to clear
+        const uint32_t start0 = (uint32_t)carry, f0 = prevFirst[base];
+#pragma unroll 1
+        for (uint32_t k = 0; k < items; ++k) {
+            const size_t c = base + (size_t)k * kThreads + threadIdx.x;
+            if (c >= numCells) break;
+            const uint32_t a = prevFirst[c], cnt = prevFirst[c + 1] - a;
+            const uint32_t start = start0 + (a - f0);
+            newCells[c] = cnt ? make_uint2(start, start + cnt) : make_uint2(kEmptyCell, kEmptyCell);
+            newFirst[c] = start;
+            if (c == numCells - 1) newFirst[numCells] = start + cnt;
+            stayBase[c] = start;
+        }
+        return;
+    }
 #pragma unroll 1
     for (uint32_t k = 0; k < items; ++k) {
         const size_t c = base + (size_t)k * kThreads + threadIdx.x;
@@ -186,6 +223,8 @@ cells_apply_kernel(const uint2* __restrict__ prevCells, uint32_t* __restrict__ l
         carry += total;
         __syncthreads();  // warpTot is reused by the next slab
     }
+    // every thread read the tile's bit before the first slab's barrier
+    if (dirty && threadIdx.x == 0) atomicAnd(dirty + (blockIdx.x >> 5), ~(1u << (blockIdx.x & 31u)));
 }
 
 __global__ void arrivals_scatter_kernel(const uint4* __restrict__ movers,
@@ -315,7 +354,7 @@ size_t incsort_bytes(uint32_t n, uint32_t numCells, uint32_t* moverCapOut) {
     const size_t cells = al256(4ull * numCells);
     const size_t np = cell_blocks(numCells);
     return 4 * cells + al256(8ull * numCells) + al256(16ull * cap) + al256(4ull * cap) +
-           al256(8ull * std::max<size_t>(np, 1)) + 256;
+           al256(8ull * std::max<size_t>(np, 1)) + al256(4ull * ((np + 31) / 32 + 1)) + 256;
 }
 
 IncSort carve_incsort(void* base, uint32_t n, uint32_t numCells) {
@@ -333,26 +372,29 @@ IncSort carve_incsort(void* base, uint32_t n, uint32_t numCells) {
     s.movers = reinterpret_cast<uint4*>(p); p += al256(16ull * s.moverCap);
     s.arrSlots = reinterpret_cast<uint32_t*>(p); p += al256(4ull * s.moverCap);
     s.partials = reinterpret_cast<unsigned long long*>(p); p += al256(8ull * std::max<size_t>(np, 1));
+    s.dirty = reinterpret_cast<uint32_t*>(p); p += al256(4ull * ((np + 31) / 32 + 1));
+    s.tileShift = log2_of(kThreads * cell_items(numCells));
     s.ctrl = reinterpret_cast<uint32_t*>(p);
     return s;
 }
 
 cudaError_t enqueue_incremental_head(const IncSort& s, const uint2* prevCells,
-                                     cudaGraphConditionalHandle full, bool setFull,
-                                     cudaStream_t st, int* launches) {
+                                     const uint32_t* prevFirst, cudaGraphConditionalHandle full,
+                                     bool setFull, cudaStream_t st, int* launches) {
     const uint32_t C = s.numCells;
     const size_t nb = cell_blocks(C);
     if (nb > kMaxScanBlocks) return cudaErrorInvalidValue;
-    cells_reduce_kernel<<<(unsigned)nb, kThreads, 0, st>>>(prevCells, s.leavers, s.arrCnt, C,
-                                                           cell_items(C), s.partials, s.ctrl,
-                                                           s.errFlag, full, setFull ? 1 : 0);
+    cells_reduce_kernel<<<(unsigned)nb, kThreads, 0, st>>>(prevCells, prevFirst, s.leavers,
+                                                           s.arrCnt, s.dirty, C, cell_items(C),
+                                                           s.partials, s.ctrl, s.errFlag, full,
+                                                           setFull ? 1 : 0);
     if (launches) ++*launches;
     return cudaGetLastError();
 }
 
 cudaError_t enqueue_incremental_tail(const IncSort& s, uint32_t n, const uint32_t* keys,
                                      const uint32_t* prevSortedKey, const uint2* prevCells,
-                                     uint32_t* newSortedKey, uint2* newCells, uint32_t* newFirst,
+                                     const uint32_t* prevFirst, uint32_t* newSortedKey, uint2* newCells, uint32_t* newFirst,
                                      const SortMove& mv, cudaStream_t st, int* launches,
                                      cudaStream_t side, cudaEvent_t forkEv, cudaEvent_t joinEv) {
     const uint32_t C = s.numCells;
@@ -360,10 +402,10 @@ cudaError_t enqueue_incremental_tail(const IncSort& s, uint32_t n, const uint32_
     const size_t nb = cell_blocks(C);
     if (nb > kMaxScanBlocks) return cudaErrorInvalidValue;
     cells_top_kernel<<<1, kTopThreads, 0, st>>>(s.partials, (uint32_t)nb, s.ctrl);
-    cells_apply_kernel<<<(unsigned)nb, kThreads, 0, st>>>(prevCells, s.leavers, s.arrCnt, s.arrLo,
-                                                          C, items, s.partials, newCells,
-                                                          newFirst, s.stayBase, s.arrInfo,
-                                                          s.ctrl);
+    cells_apply_kernel<<<(unsigned)nb, kThreads, 0, st>>>(prevCells, prevFirst, s.leavers,
+                                                          s.arrCnt, s.arrLo, s.dirty, C, items,
+                                                          s.partials, newCells, newFirst,
+                                                          s.stayBase, s.arrInfo, s.ctrl);
     // the movers (two small kernels) on `side` when given, beside the
     // stayers: both only read what cells_apply wrote, and write disjoint slots
     const bool fork = side && forkEv && joinEv;

@@ -63,6 +63,13 @@ struct IncSort {
     uint4* movers = nullptr;       // moverCap records (index, new cell, old cell, arrival slot)
     uint32_t* arrSlots = nullptr;  // moverCap
     unsigned long long* partials = nullptr;  // scan partials
+    // A bit per scan tile (the 2^tileShift cells a block of the cell scan
+    // takes) set by the step kernel for the old and the new cell of every
+    // mover; the cell scan takes a clean tile's ranges from the previous
+    // first-particle array, shifted, and clears the bits of the tiles it
+    // scanned.  A stale bit only sends a tile through the full scan.
+    uint32_t* dirty = nullptr;
+    uint32_t tileShift = 0;
     uint32_t* ctrl = nullptr;      // kCtrlNeedFull, kCtrlMovers, kCtrlPath
     // the context's error word: while a sort wait has given up
     // (kSortTimeoutBit), every step takes the full path, which needs no
@@ -74,17 +81,19 @@ size_t incsort_bytes(uint32_t n, uint32_t numCells, uint32_t* moverCapOut);
 IncSort carve_incsort(void* base, uint32_t n, uint32_t numCells);
 
 // Fast path: new cell ranges, sorted keys, moved state.  prev* describe the
-// order the step kernel just stepped; `keys` are the new keys.  `head` (the
+// order the step kernel just stepped (prevFirst: its first-particle array,
+// numCells + 1 entries); `keys` are the new keys.  `head` (the
 // first kernel) reads whether the full path is due, keeps the answer in
 // ctrl[kCtrlPath] for the kernels of `tail`, and with setFull passes it to
 // the graph conditional handle `full`.  With a `side` stream (and two events)
 // `tail` places the movers on it, beside the stayers on `st` -- the two write
 // disjoint slots -- and joins it back into `st` before returning.
 cudaError_t enqueue_incremental_head(const IncSort& s, const uint2* prevCells,
-                                     cudaGraphConditionalHandle full, bool setFull,
-                                     cudaStream_t st, int* launches);
+                                     const uint32_t* prevFirst, cudaGraphConditionalHandle full,
+                                     bool setFull, cudaStream_t st, int* launches);
 cudaError_t enqueue_incremental_tail(const IncSort& s, uint32_t n, const uint32_t* keys,
                                      const uint32_t* prevSortedKey, const uint2* prevCells,
+                                     const uint32_t* prevFirst,
                                      uint32_t* newSortedKey, uint2* newCells, uint32_t* newFirst,
                                      const SortMove& mv, cudaStream_t st, int* launches,
                                      cudaStream_t side = nullptr, cudaEvent_t forkEv = nullptr,

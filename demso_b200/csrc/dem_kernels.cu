@@ -488,6 +488,12 @@ __device__ __forceinline__ void finish_particle(
         if (m < sink.moverCap) sink.movers[m] = make_uint4(i, nk, key, slot);
         if (m >= sink.moverCap || slot >= kMaxGroup || own.y - own.x > kMaxGroup)
             atomicOr(sink.ctrl, 1u);
+        // the cell scan rescans the tiles of both cells
+        if (sink.dirty) {
+            const uint32_t t0 = key >> sink.tileShift, t1 = nk >> sink.tileShift;
+            atomicOr(sink.dirty + (t0 >> 5), 1u << (t0 & 31u));
+            if (t1 != t0) atomicOr(sink.dirty + (t1 >> 5), 1u << (t1 & 31u));
+        }
     }
 }
 

@@ -76,6 +76,8 @@ struct MoverSinkArgs {
     uint4* movers;
     uint32_t* ctrl;
     uint32_t moverCap;
+    uint32_t tileShift;  // cells per tile of the cell scan: 2^tileShift
+    uint32_t* dirty;     // a bit per tile holding a mover's old or new cell (may be null)
 };
 // The control ("big") particle of the reference built with USE_BIG_PARTICLE 1
 // (device memory, read by the step kernel and moved by control_move_kernel).
