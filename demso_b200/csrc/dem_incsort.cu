@@ -8,12 +8,12 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr uint32_t kMinCellItems = 2;
-constexpr int kTopThreads = 1024;
-constexpr int kTopItems = 8;
-constexpr uint32_t kMaxScanBlocks = kTopThreads * kTopItems;
+// scan blocks at most: a block of cells_apply sums the totals of the blocks
+// below it, at most kMaxScanBlocks / kThreads loads a thread
+constexpr uint32_t kMaxScanBlocks = 8192;
 
 // Cells per thread of the cell scan: 2, or the smallest power of two that
-// keeps the number of scan blocks within what cells_top_kernel scans.
+// keeps the number of scan blocks within kMaxScanBlocks.
 inline uint32_t cell_items(uint32_t numCells) {
     uint32_t items = kMinCellItems;
     while ((size_t)numCells > (size_t)kMaxScanBlocks * kThreads * items && items < (1u << 20))
@@ -75,6 +75,22 @@ __device__ __forceinline__ unsigned long long block_excl_scan64(unsigned long lo
     return (warp > 0 ? warpTot[warp - 1] : 0ull) + x - v;
 }
 
+// Sum of one 64-bit value per thread over the block, returned to every
+// thread; warpTot is free again when it returns.
+template <int THREADS>
+__device__ __forceinline__ unsigned long long block_sum64(unsigned long long v,
+                                                          unsigned long long* warpTot) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) warpTot[threadIdx.x >> 5] = v;
+    __syncthreads();
+    unsigned long long t = 0;
+#pragma unroll
+    for (int w = 0; w < THREADS / 32; ++w) t += warpTot[w];
+    __syncthreads();
+    return t;
+}
+
 // New particle count and arrival count of a cell, packed (count | arrivals << 32).
 __device__ __forceinline__ unsigned long long cell_counts(const uint2* __restrict__ prevCells,
                                                           const uint32_t* __restrict__ leavers,
@@ -132,31 +148,8 @@ cells_reduce_kernel(const uint2* __restrict__ prevCells, const uint32_t* __restr
         const size_t c = base + (size_t)k * kThreads + threadIdx.x;
         if (c < numCells) s += cell_counts(prevCells, leavers, arrCnt, (uint32_t)c);
     }
-    unsigned long long total;
-    (void)block_excl_scan64<kThreads>(s, warpTot, total);
+    const unsigned long long total = block_sum64<kThreads>(s, warpTot);
     if (threadIdx.x == 0) partials[blockIdx.x] = total;
-}
-
-__global__ void __launch_bounds__(kTopThreads)
-cells_top_kernel(unsigned long long* __restrict__ partials, uint32_t np,
-                 const uint32_t* __restrict__ ctrl) {
-    if (ctrl[kCtrlPath]) return;
-    __shared__ unsigned long long warpTot[kTopThreads / 32];
-    unsigned long long v[kTopItems];
-    unsigned long long s = 0;
-    const uint32_t b = threadIdx.x * kTopItems;
-#pragma unroll
-    for (int k = 0; k < kTopItems; ++k) {
-        v[k] = (b + k < np) ? partials[b + k] : 0ull;
-        s += v[k];
-    }
-    unsigned long long total;
-    unsigned long long run = block_excl_scan64<kTopThreads>(s, warpTot, total);
-#pragma unroll
-    for (int k = 0; k < kTopItems; ++k) {
-        if (b + k < np) partials[b + k] = run;
-        run += v[k];
-    }
 }
 
 // New ranges, stayer bases and arrival bases of a tile of kThreads * items
@@ -174,7 +167,10 @@ cells_apply_kernel(const uint2* __restrict__ prevCells, const uint32_t* __restri
     if (ctrl[kCtrlPath]) return;
     __shared__ unsigned long long warpTot[kThreads / 32];
     const size_t base = (size_t)blockIdx.x * kThreads * items;
-    unsigned long long carry = partials[blockIdx.x];
+    // the tile's first slot and first arrival: the totals of the tiles below
+    unsigned long long below = 0;
+    for (uint32_t j = threadIdx.x; j < blockIdx.x; j += kThreads) below += partials[j];
+    unsigned long long carry = block_sum64<kThreads>(below, warpTot);
     if (tile_clean(dirty, blockIdx.x)) {
         // no leavers or arrivals: every cell keeps its particles, shifted by
         // the movers of the tiles below; no counter to clear
@@ -401,7 +397,6 @@ cudaError_t enqueue_incremental_tail(const IncSort& s, uint32_t n, const uint32_
     const uint32_t items = cell_items(C);
     const size_t nb = cell_blocks(C);
     if (nb > kMaxScanBlocks) return cudaErrorInvalidValue;
-    cells_top_kernel<<<1, kTopThreads, 0, st>>>(s.partials, (uint32_t)nb, s.ctrl);
     cells_apply_kernel<<<(unsigned)nb, kThreads, 0, st>>>(prevCells, prevFirst, s.leavers,
                                                           s.arrCnt, s.arrLo, s.dirty, C, items,
                                                           s.partials, newCells, newFirst,
@@ -425,7 +420,7 @@ cudaError_t enqueue_incremental_tail(const IncSort& s, uint32_t n, const uint32_
         place_stayers_kernel<<<blocks_for(n, kThreads), kThreads, 0, st>>>(
             n, keys, prevSortedKey, prevCells, s.stayBase, newSortedKey, mv, s.ctrl);
     }
-    if (launches) *launches += 5;
+    if (launches) *launches += 4;
     cudaError_t e = cudaGetLastError();
     if (fork) {
         // join the movers' branch even after an error
