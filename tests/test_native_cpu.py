@@ -111,6 +111,25 @@ def test_bad_arguments_are_status_codes_not_crashes():
     assert lib.dem_calc_hash(s, None, None, None, 0, None) == 0
 
 
+def test_row_windows_check_their_rows():
+    """dem_create_rows refuses a bad block of rows before any CUDA call."""
+    lib = _lib.load()
+    sys_ = _sys()
+    s = sys_.to_c()
+    gy = sys_.gy
+    h = C.c_void_p()
+    assert gy >= 4 and gy & (gy - 1) == 0
+    assert lib.dem_create_rows(s, 10, 0, 0, 3, C.byref(h)) == 1       # not a power of two
+    assert lib.dem_create_rows(s, 10, 0, 0, 0, C.byref(h)) == 1
+    assert lib.dem_create_rows(s, 10, 0, 0, 2 * gy, C.byref(h)) == 1  # more rows than the grid
+    assert lib.dem_create_rows(s, 10, 0, gy, 2, C.byref(h)) == 1      # first row outside it
+    assert lib.dem_create_rows(s, 0, 0, 0, 2, C.byref(h)) == 1        # no capacity
+    assert lib.dem_create_rows(None, 10, 0, 0, 2, C.byref(h)) == 1
+    assert lib.dem_create_rows(s, 10, 0, 0, 2, None) == 1
+    assert lib.dem_row_slots(None, 0, 1, None, None, None) == 1
+    assert not h.value
+
+
 def test_python_errors_raise():
     with pytest.raises(D.DemError):
         _lib.check(1)
